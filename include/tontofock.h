@@ -1,0 +1,147 @@
+/*
+ * tontofock.h — C ABI of the B200 direct-SCF J/K (Fock) builder.
+ *
+ * Drop-in for the two-electron part of Tonto's restricted Fock build.  The entry
+ * points replace these reference interfaces (paths inside the Tonto project):
+ *
+ *   tf_ctx_create / tf_set_geometry
+ *       MOLECULE:update_shell_info           foofiles/molecule.set.foo:2687-2737
+ *       SHELL1PAIR:make_precalculated_data   foofiles/shell1pair.foo:100-154
+ *       MOLECULE.FOCK:initialize_max_I       foofiles/molecule.fock.foo:3705-3752
+ *   tf_build_jk
+ *       MOLECULE.FOCK:make_r_JK_direct(J,K,P)   foofiles/molecule.fock.foo:1235-1363
+ *                     (spherical basis, use_spherical_basis= TRUE)
+ *       MOLECULE.FOCK:make_r_JK_engine(J,K,P)   foofiles/molecule.fock.foo:1365-1505
+ *                     (Cartesian basis)
+ *   tf_build_fock
+ *       MOLECULE.FOCK:make_r_Fock_mx(F,P)       foofiles/molecule.fock.foo:88-155
+ *                     (F = core + J - K/2, the ee_adiabatic_constant = 1 case)
+ *   tf_build_jk_batch
+ *       no single reference routine: many independent make_r_JK_direct calls
+ *       (one per molecule) issued as one launch sequence.
+ *
+ * Conventions (identical to Tonto's):
+ *   - P, J, K, H, F are n_bf x n_bf doubles, column-major (Fortran order), in the
+ *     Tonto basis-function order (atoms in order, shells in basis-library order,
+ *     Cartesian components in Tonto order, or real solid harmonics ordered
+ *     m = 0,+1,-1,+2,-2,... for l >= 2 in a spherical basis).
+ *   - Shell contraction coefficients are Tonto's "unnormalised" ones (after
+ *     SHELL:unnormalize, foofiles/shell.foo:492-505).
+ *   - All indices are 0-based.  Coordinates are in bohr.
+ *   - J and K are fully overwritten (reference: J = ZERO, K = ZERO at :1259-1260).
+ *
+ * Errors: every int-returning call returns TF_OK (0) or a negative TF_E* code;
+ * tf_error_string() gives a message.  No exception or exit crosses the ABI.
+ * Device waits inside the library are bounded and report TF_ETIMEOUT.
+ *
+ * Threading: one caller thread per context.  Contexts are independent; each is
+ * bound to the CUDA device given in tf_options.device.
+ */
+#ifndef TONTOFOCK_H
+#define TONTOFOCK_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TF_OK            0
+#define TF_EINVAL      (-1)   /* bad argument */
+#define TF_ECUDA       (-2)   /* CUDA runtime error */
+#define TF_ENOMEM      (-3)   /* device or host allocation failed */
+#define TF_EUNSUPPORTED (-4)  /* angular momentum or size beyond what was built */
+#define TF_ETIMEOUT    (-5)   /* a bounded device wait ran out */
+#define TF_ENODEVICE   (-6)   /* no CUDA device / extension not usable */
+#define TF_ESTATE      (-7)   /* call out of order (e.g. no geometry) */
+
+/* tf_build_jk flags */
+#define TF_JK_FULL        0x0   /* full FP64 build */
+#define TF_JK_MIXED       0x1   /* quartets with Schwarz x density bound < mixed_cut in FP32 (FP64 roots, accumulation) */
+#define TF_JK_DELTA       0x2   /* incremental: P is a density difference; J, K are increments */
+#define TF_JK_NO_COPYBACK 0x4   /* (device entry points only) leave results on the device */
+
+/* Precision of a context's default build */
+#define TF_PRECISION_FP64  0
+#define TF_PRECISION_MIXED 1
+
+typedef struct tf_basis {
+  int n_atom;
+  const double* xyz;            /* [n_atom][3], bohr */
+  int n_shell;
+  const int* shell_atom;        /* [n_shell] atom of each shell */
+  const int* shell_l;           /* [n_shell] angular momentum (0..3 supported) */
+  const int* shell_nprim;       /* [n_shell] primitives per shell */
+  const int* shell_first_bf;    /* [n_shell] first basis function (Tonto order) */
+  const double* exponents;      /* [sum nprim] primitive exponents, shell after shell */
+  const double* coefficients;   /* [sum nprim] Tonto unnormalised contraction coefficients */
+  int is_spherical;             /* Tonto use_spherical_basis */
+} tf_basis;
+
+typedef struct tf_options {
+  double eri_schwarz_cutoff;         /* SCF_DATA ERI_Schwarz_cutoff (Tonto default 1e-9, types.foo:6097) */
+  double eri_primitive_pair_cutoff;  /* SHELL1QUARTET pair_cutoff (Tonto default 1e-6, macros.in:695) */
+  double mixed_fp32_cut;             /* TF_JK_MIXED: Schwarz x density bound below which FP32 is used */
+  int device;                        /* CUDA device ordinal */
+  int deterministic;                 /* 1: atomics-free privatised accumulation (bitwise reproducible) */
+} tf_options;
+
+typedef struct tf_stats {
+  double build_ms;                   /* device time of the last build (CUDA events) */
+  double eri_ms;                     /* device time of the ERI + digestion kernels */
+  double quartets;                   /* contracted shell quartets computed */
+  double quartets_fp32;              /* of which in FP32 */
+  double prim_quartets;              /* primitive quartets computed */
+  double flops;                      /* algorithmic FLOP count of the last build */
+  long long h2d_bytes, d2h_bytes;    /* host<->device bytes of the last call */
+  int kernels;                       /* kernel launches issued by the last build */
+} tf_stats;
+
+typedef struct tf_ctx tf_ctx;
+
+/* Fill *opt with Tonto's defaults (Schwarz 1e-9, pair 1e-6, device 0). */
+int tf_default_options(tf_options* opt);
+
+/* Create a context: copies the basis, builds shell-pair data and Schwarz bounds
+ * on the device (replaces update_shell_info + initialize_max_I). */
+int tf_ctx_create(const tf_basis* basis, const tf_options* opt, tf_ctx** ctx);
+
+/* New atom positions ([n_atom][3] bohr): rebuilds pair data and Schwarz bounds. */
+int tf_set_geometry(tf_ctx* ctx, const double* xyz);
+
+/* J and K from the symmetric density P (host arrays, column-major n_bf x n_bf).
+ * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*. */
+int tf_build_jk(tf_ctx* ctx, const double* P, double* J, double* K, int flags);
+
+/* Same, on device arrays (n_bf*n_bf doubles each) on the CUDA stream `stream`
+ * (a cudaStream_t, or NULL for the context's own stream).  Asynchronous. */
+int tf_build_jk_device(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags, void* stream);
+
+/* F = Hcore + J - K/2 from P (host arrays).  Replaces make_r_Fock_mx. */
+int tf_build_fock(tf_ctx* ctx, const double* P, const double* Hcore, double* F);
+
+/* Many independent molecules in one launch sequence: P[i], J[i], K[i] are host
+ * arrays of ctx[i]'s size.  All contexts must be on the same device. */
+int tf_build_jk_batch(tf_ctx** ctx, int n, const double* const* P, double* const* J, double* const* K, int flags);
+
+/* Statistics of the last build on this context. */
+int tf_last_stats(const tf_ctx* ctx, tf_stats* stats);
+
+/* Number of basis functions of the context (Tonto n_bf). */
+int tf_n_bf(const tf_ctx* ctx);
+
+/* Schwarz bounds sqrt(max |(ab|ab)|) per Tonto shell pair ab = a(a+1)/2 + b (a >= b). */
+int tf_schwarz(const tf_ctx* ctx, double* max_I);
+
+void tf_ctx_destroy(tf_ctx* ctx);
+
+const char* tf_error_string(int code);
+
+/* Library version string. */
+const char* tf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TONTOFOCK_H */

@@ -45,6 +45,9 @@
 
 #define TF_RYS_CONST static const
 #include "rys_tables.inc"
+static const int tf_rys_xmax[] = TF_RYS_XMAX_INIT;
+static const int tf_rys_offset[] = TF_RYS_OFFSET_INIT;
+static const int tf_rys_hoffset[] = TF_RYS_HOFFSET_INIT;
 
 namespace {
 

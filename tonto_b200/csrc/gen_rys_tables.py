@@ -166,13 +166,13 @@ def main():
     lines.append("#define TF_RYS_DEG %d" % DEG)
     lines.append("#define TF_RYS_NCOEF %d" % (DEG + 1))
     xm = [0] + [XMAX[n] for n in range(1, nmax + 1)]
-    lines.append("TF_RYS_CONST int tf_rys_xmax[%d] = {%s};" % (nmax + 1, ", ".join(str(v) for v in xm)))
+    lines.append("#define TF_RYS_XMAX_INIT {%s}" % ", ".join(str(v) for v in xm))
     offs = [0]
     tot = 0
     for n in range(1, nmax + 1):
         offs.append(tot)
         tot += XMAX[n] * 2 * n * (DEG + 1)
-    lines.append("TF_RYS_CONST int tf_rys_offset[%d] = {%s};" % (nmax + 1, ", ".join(str(v) for v in offs)))
+    lines.append("#define TF_RYS_OFFSET_INIT {%s}" % ", ".join(str(v) for v in offs))
     lines.append("#define TF_RYS_TABLE_SIZE %d" % tot)
     lines.append("TF_RYS_CONST double tf_rys_coef[%d] = {" % tot)
     for n in range(1, nmax + 1):
@@ -187,7 +187,7 @@ def main():
     for n in range(1, nmax + 1):
         hoff.append(ht)
         ht += n
-    lines.append("TF_RYS_CONST int tf_rys_hoffset[%d] = {%s};" % (nmax + 1, ", ".join(str(v) for v in hoff)))
+    lines.append("#define TF_RYS_HOFFSET_INIT {%s}" % ", ".join(str(v) for v in hoff))
     r2 = []
     ww = []
     for n in range(1, nmax + 1):

@@ -1,0 +1,384 @@
+// tf_device.cuh — device-side building blocks of the B200 Rys J/K builder.
+//
+// Everything that depends on angular momentum is resolved at compile time:
+// Cartesian component tables (Tonto's lexical order, gaussian_data.foo:295-479)
+// are constexpr, loops over components are unrolled with static_for, and the
+// integral arrays therefore live in registers.  One thread computes one
+// contracted shell quartet:
+//   primitive quartets -> Rys nodes/weights (piecewise tables, FP64)
+//   -> 2D recurrences on the higher-l centre of each pair (make_esfs_XX,
+//      shell1quartet.foo:7418-7609) -> (e0|f0) accumulation (form_esfs :7615)
+//   -> horizontal transfer ket then bra (transfer_cd / transfer_ab :8310-11134)
+//   -> digestion into J and K with Tonto's coincidence factors
+//      (molecule.fock.foo:1296-1338).
+// The spherical transform of make_ERI (:433-563) is not applied per quartet:
+// the density is taken to the Cartesian basis once per build and J, K are taken
+// back once (the transforms commute with the contraction).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <utility>
+#include <type_traits>
+
+#define TF_RYS_CONST __device__ const
+#include "rys_tables.inc"
+
+namespace tf {
+
+// ---------------------------------------------------------------------------
+// compile-time helpers
+// ---------------------------------------------------------------------------
+template <int... Is, class F>
+__device__ __forceinline__ void static_for_impl(std::integer_sequence<int, Is...>, F&& f) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(std::make_integer_sequence<int, N>{}, f);
+}
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int ncart_upto(int l) { return l < 0 ? 0 : (l + 1) * (l + 2) * (l + 3) / 6; }
+
+constexpr int LCOMP = 8;                         // components tabulated up to l = 8
+constexpr int NCOMP_ALL = ncart_upto(LCOMP);     // 165
+
+struct CompTable {
+  int x[NCOMP_ALL], y[NCOMP_ALL], z[NCOMP_ALL];
+  int first[LCOMP + 2];
+  int idx[LCOMP + 1][LCOMP + 1][LCOMP + 1];      // position within its own l
+};
+
+__host__ __device__ constexpr void comp_push(CompTable& t, int& i, int X, int Y, int Z) {
+  t.x[i] = X; t.y[i] = Y; t.z[i] = Z; ++i;
+}
+
+// Tonto's lexical Cartesian order: for L, the highest power a descends, then the
+// second b, each pattern expanded in a fixed permutation order.
+__host__ __device__ constexpr CompTable make_comp_table() {
+  CompTable t{};
+  int i = 0;
+  for (int L = 0; L <= LCOMP; ++L) {
+    t.first[L] = i;
+    for (int a = L; a >= (L + 2) / 3; --a) {
+      for (int b = (L - a < a ? L - a : a); b >= (L - a + 1) / 2; --b) {
+        int c = L - a - b;
+        if (a == b && b == c) {
+          comp_push(t, i, a, a, a);
+        } else if (a > b && b == c) {
+          comp_push(t, i, a, b, b); comp_push(t, i, b, a, b); comp_push(t, i, b, b, a);
+        } else if (a == b && b > c) {
+          comp_push(t, i, a, a, c); comp_push(t, i, a, c, a); comp_push(t, i, c, a, a);
+        } else {
+          comp_push(t, i, a, b, c); comp_push(t, i, a, c, b); comp_push(t, i, b, a, c);
+          comp_push(t, i, c, a, b); comp_push(t, i, b, c, a); comp_push(t, i, c, b, a);
+        }
+      }
+    }
+  }
+  t.first[LCOMP + 1] = i;
+  for (int k = 0; k < NCOMP_ALL; ++k) {
+    int L = t.x[k] + t.y[k] + t.z[k];
+    t.idx[t.x[k]][t.y[k]][t.z[k]] = k - t.first[L];
+  }
+  return t;
+}
+
+constexpr CompTable CT = make_comp_table();
+static_assert(CT.first[LCOMP + 1] == NCOMP_ALL, "component table size");
+
+__host__ __device__ constexpr int cx(int l, int i) { return CT.x[CT.first[l] + i]; }
+__host__ __device__ constexpr int cy(int l, int i) { return CT.y[CT.first[l] + i]; }
+__host__ __device__ constexpr int cz(int l, int i) { return CT.z[CT.first[l] + i]; }
+// global lexical index -> powers
+__host__ __device__ constexpr int gx(int g) { return CT.x[g]; }
+__host__ __device__ constexpr int gy(int g) { return CT.y[g]; }
+__host__ __device__ constexpr int gz(int g) { return CT.z[g]; }
+__host__ __device__ constexpr int gidx(int x, int y, int z) { return CT.first[x + y + z] + CT.idx[x][y][z]; }
+
+// ---------------------------------------------------------------------------
+// data layouts shared with the host code
+// ---------------------------------------------------------------------------
+// One primitive pair (Gaussian product), positioned.  cc already holds
+// c_a c_b zeta^(-3/2) exp(-a b |AB|^2 / zeta) and, for bra-side use, nothing else:
+// the 2 pi^(5/2) factor is applied per primitive quartet.
+struct __align__(16) PrimPair {
+  double Px, Py, Pz, zeta;
+  double PAx, PAy, PAz, half_zinv;   // P - (centre of the higher-l shell), 1/(2 zeta)
+  double cc, pad;
+};
+
+// One shell pair, oriented so that shell "hi" has the higher l (ties: the
+// shell with the larger index, as Tonto's pair (a >= b) orientation).
+struct __align__(16) PairRec {
+  int sh_hi, sh_lo;          // shell indices (Tonto order)
+  int atom_hi, atom_lo;
+  int cart_hi, cart_lo;      // first Cartesian function of each shell
+  int full_off, n_full;      // primitive pairs without the pair cutoff
+  int skip_off, n_skip;      // primitive pairs with the pair cutoff (atoms differ)
+  int cls, tonto_ab;         // pair class id, Tonto pair index a(a+1)/2+b
+  double Rx, Ry, Rz;         // hi centre - lo centre
+  double imax;               // Schwarz bound sqrt(max |(ab|ab)|)
+};
+
+constexpr double TWOPI5ON2 = 34.9868366552497256925;   // 2 pi^(5/2)
+
+// ---------------------------------------------------------------------------
+// Rys nodes and weights (FP64 always)
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int rys_xmax(int n) { const int t[] = TF_RYS_XMAX_INIT; return t[n]; }
+__host__ __device__ constexpr int rys_offset(int n) { const int t[] = TF_RYS_OFFSET_INIT; return t[n]; }
+__host__ __device__ constexpr int rys_hoffset(int n) { const int t[] = TF_RYS_HOFFSET_INIT; return t[n]; }
+
+template <int N>
+__device__ __forceinline__ void rys_eval(double x, double (&u)[N], double (&w)[N]) {
+  constexpr int XMAX = rys_xmax(N), OFF = rys_offset(N), HOFF = rys_hoffset(N);
+  if (x < (double)XMAX) {
+    const int j = (int)x;
+    const double s = x - (double)j;
+    const double* c = tf_rys_coef + OFF + j * (2 * N * TF_RYS_NCOEF);
+#pragma unroll
+    for (int f = 0; f < 2 * N; ++f) {
+      const double* cf = c + f * TF_RYS_NCOEF;
+      double v = __ldg(cf + TF_RYS_DEG);
+#pragma unroll
+      for (int k = TF_RYS_DEG - 1; k >= 0; --k) v = fma(v, s, __ldg(cf + k));
+      if (f < N) u[f] = v; else w[f - N] = v;
+    }
+  } else {
+    const double ix = 1.0 / x;
+    const double isx = sqrt(ix);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      u[i] = tf_rys_hroot2[HOFF + i] * ix;
+      w[i] = tf_rys_hweight[HOFF + i] * isx;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One contracted shell quartet (LA LB | LC LD), LA >= LB, LC >= LD, in
+// arithmetic type T for the 2D recurrences and (e0|f0) sums (double, or float
+// for the mixed-precision path); nodes/weights and the final integrals FP64.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD>
+struct Quartet {
+  static constexpr int LAB = LA + LB, LCD = LC + LD;
+  static constexpr int NROOT = (LAB + LCD) / 2 + 1;
+  static constexpr int FE = CT.first[LA], NE = CT.first[LAB + 1] - CT.first[LA];   // e: l in [LA, LA+LB]
+  static constexpr int FF = CT.first[LC], NF = CT.first[LCD + 1] - CT.first[LC];
+  static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  static constexpr int NINT = NA * NB * NC * ND;
+};
+
+// read-only 32-byte load of half a primitive-pair record
+__device__ __forceinline__ double4 ld4(const PrimPair* p, int half) {
+  const double2* q = reinterpret_cast<const double2*>(p) + 2 * half;
+  const double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// (e0|f0) accumulation over all primitive quartets of a contracted quartet.
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp, int nbp,
+                                                const PrimPair* __restrict__ kp, int nkp,
+                                                T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF]) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
+#pragma unroll
+  for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+    for (int f = 0; f < Q::NF; ++f) esfs[e][f] = T(0);
+
+  for (int ib = 0; ib < nbp; ++ib) {
+    const double4 b0 = ld4(bp + ib, 0);
+    const double4 b1 = ld4(bp + ib, 1);
+    const double bcc = __ldg(&bp[ib].cc) * TWOPI5ON2;
+    const double zeta = b0.w, half_zinv = b1.w;
+    for (int ik = 0; ik < nkp; ++ik) {
+      const double4 k0 = ld4(kp + ik, 0);
+      const double4 k1 = ld4(kp + ik, 1);
+      const double kcc = __ldg(&kp[ik].cc);
+      const double eta = k0.w, half_einv = k1.w;
+      const double inv = 1.0 / (zeta + eta);
+      const double rho = zeta * eta * inv;
+      const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
+      const double xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
+      double u[NR], w[NR];
+      rys_eval<NR>(xx, u, w);
+      const double scale = bcc * kcc * sqrt(rho);
+      const double r_z = eta * inv;     // rho / zeta
+      const double r_e = zeta * inv;    // rho / eta
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const double t2 = u[r];
+        const double t2_rz = t2 * r_z, t2_re = t2 * r_e;
+        const T B10 = T((1.0 - t2_rz) * half_zinv);
+        const T B01 = T((1.0 - t2_re) * half_einv);
+        const T B00 = T(0.5 * t2 * inv);
+        const T wt = T(w[r] * scale);
+        T I[3][D1][D2];
+        const double PA[3] = {b1.x, b1.y, b1.z};
+        const double QC[3] = {k1.x, k1.y, k1.z};
+        const double QP[3] = {QPx, QPy, QPz};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const T c00 = T(PA[d] + t2_rz * QP[d]);
+          const T d00 = T(QC[d] - t2_re * QP[d]);
+          I[d][0][0] = (d == 2) ? wt : T(1);
+          if (D1 > 1) I[d][1][0] = c00 * I[d][0][0];
+#pragma unroll
+          for (int e = 1; e + 1 < D1; ++e) I[d][e + 1][0] = c00 * I[d][e][0] + T(e) * B10 * I[d][e - 1][0];
+#pragma unroll
+          for (int f = 0; f + 1 < D2; ++f) {
+#pragma unroll
+            for (int e = 0; e < D1; ++e) {
+              T v = d00 * I[d][e][f];
+              if (f > 0) v += T(f) * B01 * I[d][e][f - 1];
+              if (e > 0) v += T(e) * B00 * I[d][e - 1][f];
+              I[d][e][f + 1] = v;
+            }
+          }
+        }
+        static_for<Q::NE>([&](auto e) {
+          constexpr int ge = Q::FE + decltype(e)::value;
+          static_for<Q::NF>([&](auto f) {
+            constexpr int gf = Q::FF + decltype(f)::value;
+            esfs[decltype(e)::value][decltype(f)::value] +=
+                I[0][gx(ge)][gx(gf)] * I[1][gy(ge)][gy(gf)] * I[2][gz(ge)][gz(gf)];
+          });
+        });
+      }
+    }
+  }
+}
+
+// Horizontal transfer on the ket: esfs[e][f] (f over l in [LC, LC+LD]) ->
+// out[e][c][d], (c, d+1_i) = (c+1_i, d) + R_i (c, d), R = C - D.
+// Level k holds d over comps(k) and c over l in [LC, LC+LD-k].
+template <int LC, int LD, int NE, typename T>
+__device__ __forceinline__ void hrr_ket(const T (&G)[NE][CT.first[LC + LD + 1] - CT.first[LC]], const double* R,
+                                        T (&out)[NE][ncart(LC)][ncart(LD)]) {
+  if constexpr (LD == 0) {
+#pragma unroll
+    for (int e = 0; e < NE; ++e)
+#pragma unroll
+      for (int c = 0; c < ncart(LC); ++c) out[e][c][0] = G[e][c];
+  } else {
+    // level tables: lev[k][c_global_offset][d], c over l in [LC, LC+LD-k]
+    constexpr int NCR = CT.first[LC + LD + 1] - CT.first[LC];
+    T cur[NE][NCR][ncart(LD)];
+#pragma unroll
+    for (int e = 0; e < NE; ++e)
+#pragma unroll
+      for (int c = 0; c < NCR; ++c) cur[e][c][0] = G[e][c];
+    static_for<LD>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;           // building d level k+1
+      constexpr int NCN = CT.first[LC + LD - k] - CT.first[LC];
+      T nxt[NE][NCN > 0 ? NCN : 1][ncart(k + 1)];
+      static_for<ncart(k + 1)>([&](auto dd) {
+        constexpr int d1 = decltype(dd)::value;
+        constexpr int px = cx(k + 1, d1), py = cy(k + 1, d1), pz = cz(k + 1, d1);
+        constexpr int dir = px > 0 ? 0 : (py > 0 ? 1 : 2);
+        constexpr int d0 = CT.idx[px - (dir == 0)][py - (dir == 1)][pz - (dir == 2)];
+        static_for<NCN>([&](auto ci) {
+          constexpr int c = decltype(ci)::value;
+          constexpr int g = CT.first[LC] + c;
+          constexpr int gp = gidx(gx(g) + (dir == 0), gy(g) + (dir == 1), gz(g) + (dir == 2)) - CT.first[LC];
+#pragma unroll
+          for (int e = 0; e < NE; ++e) nxt[e][c][d1] = cur[e][gp][d0] + T(R[dir]) * cur[e][c][d0];
+        });
+      });
+#pragma unroll
+      for (int e = 0; e < NE; ++e)
+#pragma unroll
+        for (int c = 0; c < NCN; ++c)
+#pragma unroll
+          for (int d = 0; d < ncart(k + 1); ++d) cur[e][c][d] = nxt[e][c][d];
+    });
+#pragma unroll
+    for (int e = 0; e < NE; ++e)
+#pragma unroll
+      for (int c = 0; c < ncart(LC); ++c)
+#pragma unroll
+        for (int d = 0; d < ncart(LD); ++d) out[e][c][d] = cur[e][c][d];
+  }
+}
+
+// Horizontal transfer on the bra: G[e][r] (e over l in [LA, LA+LB]) ->
+// out[a][b][r] with R = A - B.
+template <int LA, int LB, int NR, typename T>
+__device__ __forceinline__ void hrr_bra(const T (&G)[CT.first[LA + LB + 1] - CT.first[LA]][NR], const double* R,
+                                        T (&out)[ncart(LA)][ncart(LB)][NR]) {
+  if constexpr (LB == 0) {
+#pragma unroll
+    for (int a = 0; a < ncart(LA); ++a)
+#pragma unroll
+      for (int r = 0; r < NR; ++r) out[a][0][r] = G[a][r];
+  } else {
+    constexpr int NAR = CT.first[LA + LB + 1] - CT.first[LA];
+    T cur[NAR][ncart(LB)][NR];
+#pragma unroll
+    for (int a = 0; a < NAR; ++a)
+#pragma unroll
+      for (int r = 0; r < NR; ++r) cur[a][0][r] = G[a][r];
+    static_for<LB>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      constexpr int NAN_ = CT.first[LA + LB - k] - CT.first[LA];
+      T nxt[NAN_ > 0 ? NAN_ : 1][ncart(k + 1)][NR];
+      static_for<ncart(k + 1)>([&](auto bb) {
+        constexpr int b1 = decltype(bb)::value;
+        constexpr int px = cx(k + 1, b1), py = cy(k + 1, b1), pz = cz(k + 1, b1);
+        constexpr int dir = px > 0 ? 0 : (py > 0 ? 1 : 2);
+        constexpr int b0 = CT.idx[px - (dir == 0)][py - (dir == 1)][pz - (dir == 2)];
+        static_for<NAN_>([&](auto ai) {
+          constexpr int a = decltype(ai)::value;
+          constexpr int g = CT.first[LA] + a;
+          constexpr int gp = gidx(gx(g) + (dir == 0), gy(g) + (dir == 1), gz(g) + (dir == 2)) - CT.first[LA];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) nxt[a][b1][r] = cur[gp][b0][r] + T(R[dir]) * cur[a][b0][r];
+        });
+      });
+#pragma unroll
+      for (int a = 0; a < NAN_; ++a)
+#pragma unroll
+        for (int b = 0; b < ncart(k + 1); ++b)
+#pragma unroll
+          for (int r = 0; r < NR; ++r) cur[a][b][r] = nxt[a][b][r];
+    });
+#pragma unroll
+    for (int a = 0; a < ncart(LA); ++a)
+#pragma unroll
+      for (int b = 0; b < ncart(LB); ++b)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) out[a][b][r] = cur[a][b][r];
+  }
+}
+
+// Contracted Cartesian integrals (ab|cd) of one quartet, as double.
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void quartet_integrals(const PrimPair* bp, int nbp, const PrimPair* kp, int nkp,
+                                                  const double* Rab, const double* Rcd,
+                                                  double (&abcd)[ncart(LA)][ncart(LB)][ncart(LC) * ncart(LD)]) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  T esfs[Q::NE][Q::NF];
+  accumulate_esfs<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, esfs);
+  double ed[Q::NE][Q::NF];
+#pragma unroll
+  for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+    for (int f = 0; f < Q::NF; ++f) ed[e][f] = (double)esfs[e][f];
+  double ket[Q::NE][Q::NC][Q::ND];
+  hrr_ket<LC, LD, Q::NE, double>(ed, Rcd, ket);
+  double flat[Q::NE][Q::NC * Q::ND];
+#pragma unroll
+  for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+    for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) flat[e][c * Q::ND + d] = ket[e][c][d];
+  hrr_bra<LA, LB, Q::NC * Q::ND, double>(flat, Rab, abcd);
+}
+
+}  // namespace tf

@@ -1,0 +1,1194 @@
+// tontofock.cu — kernels and C ABI of the B200 direct-SCF J/K builder.
+//
+// Per context (one molecule, one device):
+//   k_pair_prep      positioned primitive pairs of every shell pair, with and
+//                    without the primitive-pair cutoff (set_ab_new,
+//                    shell1quartet.foo:131-275); one thread per shell pair
+//   k_schwarz<LA,LB> I_max(ab) = sqrt(max |(ab|ab)|) in the Tonto basis
+//                    (make_max_abab_integrals, molecule.fock.foo:3712-3752)
+// Per build:
+//   k_density_to_cart  P (Tonto basis) -> P in the Cartesian basis
+//   k_pmax             max |P| per shell pair, global max (molecule.fock.foo:3601)
+//   k_count / k_write  Schwarz-screened quartet lists per class pair, bra-major,
+//                      deterministic order (Schwarz_inequality_test :3454-3495)
+//   k_jk<LA,LB,LC,LD>  one thread per quartet: Rys ERIs + digestion into J, K
+//   k_finalize         J = 2(J + J^T), K = K + K^T (weight_diagonal_blocks,
+//                      blockwise_symmetric_fold, symmetric_reflect :4181-4263),
+//                      back to the Tonto basis
+#include "tf_device.cuh"
+#include "tf_warp.cuh"
+#include "../../include/tontofock.h"
+
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace tf {
+
+constexpr int LMAX_SUPPORTED = 2;                 // s, p, d shells in the ERI kernels
+constexpr int NPAIRCLS = (LMAX_SUPPORTED + 1) * (LMAX_SUPPORTED + 2) / 2;
+constexpr int NQCLS = 625;                        // (la lb lc ld) counter slots, l <= 4
+__host__ __device__ constexpr int pair_class(int lh, int ll) { return lh * (lh + 1) / 2 + ll; }
+__host__ __device__ constexpr int qclass_id(int la, int lb, int lc, int ld) { return ((la * 5 + lb) * 5 + lc) * 5 + ld; }
+
+__constant__ double c_U[4][10 * 7];               // Cartesian -> spherical, l = 0..3, [cart][m]
+
+// ---------------------------------------------------------------------------
+// error helpers
+// ---------------------------------------------------------------------------
+#define TF_CUDA(call)                                                     \
+  do {                                                                    \
+    cudaError_t e__ = (call);                                             \
+    if (e__ != cudaSuccess) {                                             \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e__));     \
+      return e__ == cudaErrorMemoryAllocation ? TF_ENOMEM : TF_ECUDA;     \
+    }                                                                     \
+  } while (0)
+
+thread_local std::string g_last_error;
+void set_error(const std::string& s) { g_last_error = s; }
+
+// ---------------------------------------------------------------------------
+// kernels: shell pairs
+// ---------------------------------------------------------------------------
+__global__ void k_pair_prep(int n_pairs, PairRec* __restrict__ pairs, const double* __restrict__ xyz,
+                            const int* __restrict__ shell_nprim, const int* __restrict__ shell_poff,
+                            const double* __restrict__ exps, const double* __restrict__ coefs,
+                            PrimPair* __restrict__ prim_full, PrimPair* __restrict__ prim_skip, double pair_cutoff) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_pairs) return;
+  PairRec pr = pairs[p];
+  const double* A = xyz + 3 * pr.atom_hi;
+  const double* B = xyz + 3 * pr.atom_lo;
+  pr.Rx = A[0] - B[0]; pr.Ry = A[1] - B[1]; pr.Rz = A[2] - B[2];
+  const double r2 = pr.Rx * pr.Rx + pr.Ry * pr.Ry + pr.Rz * pr.Rz;
+  const bool same = pr.atom_hi == pr.atom_lo;
+  // Tonto's pair (a >= b by shell index) decides the operand order of the skip test
+  const bool hi_is_a = pr.sh_hi >= pr.sh_lo;
+  const int nh = shell_nprim[pr.sh_hi], nl = shell_nprim[pr.sh_lo];
+  int k = 0, i = 0;
+  for (int ih = 0; ih < nh; ++ih) {
+    const double eh = exps[shell_poff[pr.sh_hi] + ih], ch = coefs[shell_poff[pr.sh_hi] + ih];
+    for (int il = 0; il < nl; ++il, ++i) {
+      const double el = exps[shell_poff[pr.sh_lo] + il], cl = coefs[shell_poff[pr.sh_lo] + il];
+      const double zeta = eh + el, inv = 1.0 / zeta;
+      const double ea = hi_is_a ? eh : el, eb = hi_is_a ? el : eh;
+      const double prefac = same ? 1.0 : exp(-ea * (eb * r2) * inv);
+      PrimPair q;
+      q.Px = (eh * A[0] + el * B[0]) * inv;
+      q.Py = (eh * A[1] + el * B[1]) * inv;
+      q.Pz = (eh * A[2] + el * B[2]) * inv;
+      q.zeta = zeta;
+      q.PAx = q.Px - A[0]; q.PAy = q.Py - A[1]; q.PAz = q.Pz - A[2];
+      q.half_zinv = 0.5 * inv;
+      q.cc = ch * cl * inv * sqrt(inv) * prefac;
+      q.pad = 0.0;
+      prim_full[pr.full_off + i] = q;
+      if (!same && !(prefac < pair_cutoff)) prim_skip[pr.skip_off + k++] = q;
+    }
+  }
+  pr.n_skip = same ? 0 : k;
+  pairs[p] = pr;
+}
+
+template <int LA, int LB>
+__global__ void k_schwarz(const int* __restrict__ ids, int n, PairRec* __restrict__ pairs,
+                          const PrimPair* __restrict__ prim_full, int spherical) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int p = ids[t];
+  const PairRec pr = pairs[p];
+  const double R[3] = {pr.Rx, pr.Ry, pr.Rz};
+  constexpr int NA = ncart(LA), NB = ncart(LB);
+  double I[NA][NB][NA * NB];
+  quartet_integrals<LA, LB, LA, LB, double>(prim_full + pr.full_off, pr.n_full, prim_full + pr.full_off,
+                                            pr.n_full, R, R, I);
+  double m = 0.0;
+  const bool sa = spherical && LA >= 2, sb = spherical && LB >= 2;
+  const int MA = sa ? 2 * LA + 1 : NA, MB = sb ? 2 * LB + 1 : NB;
+  for (int ma = 0; ma < MA; ++ma)
+    for (int mb = 0; mb < MB; ++mb) {
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const double ua = sa ? c_U[LA][a * (2 * LA + 1) + ma] : (a == ma ? 1.0 : 0.0);
+        if (ua == 0.0) continue;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const double ub = sb ? c_U[LB][b * (2 * LB + 1) + mb] : (b == mb ? 1.0 : 0.0);
+          if (ub == 0.0) continue;
+#pragma unroll
+          for (int c = 0; c < NA; ++c) {
+            const double uc = sa ? c_U[LA][c * (2 * LA + 1) + ma] : (c == ma ? 1.0 : 0.0);
+            if (uc == 0.0) continue;
+#pragma unroll
+            for (int d = 0; d < NB; ++d) {
+              const double ud = sb ? c_U[LB][d * (2 * LB + 1) + mb] : (d == mb ? 1.0 : 0.0);
+              s += ua * ub * uc * ud * I[a][b][c * NB + d];
+            }
+          }
+        }
+      }
+      m = fmax(m, fabs(s));
+    }
+  pairs[p].imax = sqrt(m);
+}
+
+// ---------------------------------------------------------------------------
+// kernels: per-build density preparation
+// ---------------------------------------------------------------------------
+// P_cart[p][q] = sum U_A[p][m] P[m][m'] U_B[q][m'] over the shell blocks.
+__global__ void k_density_to_cart(int n_cart, int n_bf, const double* __restrict__ P,
+                                  const int* __restrict__ cart_shell, const int* __restrict__ cart_local,
+                                  const int* __restrict__ shell_l, const int* __restrict__ shell_first_bf,
+                                  int spherical, double* __restrict__ Pc) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n_cart * n_cart) return;
+  const int p = (int)(t / n_cart), q = (int)(t % n_cart);
+  const int sp = cart_shell[p], sq = cart_shell[q];
+  const int ip = cart_local[p], iq = cart_local[q];
+  const int lp = shell_l[sp], lq = shell_l[sq];
+  const int fp = shell_first_bf[sp], fq = shell_first_bf[sq];
+  const bool tp = spherical && lp >= 2, tq = spherical && lq >= 2;
+  double s = 0.0;
+  if (!tp && !tq) {
+    s = P[(size_t)(fq + iq) * n_bf + fp + ip];
+  } else {
+    const int mp = tp ? 2 * lp + 1 : 1, mq = tq ? 2 * lq + 1 : 1;
+    for (int a = 0; a < mp; ++a) {
+      const double ua = tp ? c_U[lp][ip * mp + a] : 1.0;
+      const int ia = tp ? fp + a : fp + ip;
+      if (ua == 0.0) continue;
+      for (int b = 0; b < mq; ++b) {
+        const double ub = tq ? c_U[lq][iq * mq + b] : 1.0;
+        const int ib = tq ? fq + b : fq + iq;
+        s += ua * ub * P[(size_t)ib * n_bf + ia];
+      }
+    }
+  }
+  Pc[(size_t)p * n_cart + q] = s;
+}
+
+// max |P(a,b)| over each shell pair block (Tonto basis), and the global max.
+__global__ void k_pmax(int n_shell, int n_bf, const double* __restrict__ P, const int* __restrict__ shell_first_bf,
+                       const int* __restrict__ shell_nbf, double* __restrict__ pmax,
+                       unsigned long long* __restrict__ pglob) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (t < (long long)n_shell * n_shell) {
+    const int a = (int)(t / n_shell), b = (int)(t % n_shell);
+    const int fa = shell_first_bf[a], fb = shell_first_bf[b], na = shell_nbf[a], nb = shell_nbf[b];
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < na; ++i) m = fmax(m, fabs(P[(size_t)(fb + j) * n_bf + fa + i]));
+    pmax[t] = m;
+  }
+  // nonnegative doubles order like their bit patterns
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(pglob, (unsigned long long)__double_as_longlong(m));
+}
+
+// ---------------------------------------------------------------------------
+// kernels: quartet lists
+// ---------------------------------------------------------------------------
+struct ListArgs {
+  const int2* tasks;            // (class pair, bra position)
+  long long n_tasks;
+  const int4* cp;               // class pair: (bra class, ket class, bra list offset, ket list offset)
+  const int* cls_n;             // pairs per class
+  const int* sorted;            // pair ids, grouped by class, I_max descending
+  const double* sorted_imax;
+  const PairRec* pairs;
+  const double* pmax;           // n_shell x n_shell
+  const unsigned long long* pglob;
+  int n_shell;
+  double cutoff;
+};
+
+__device__ __forceinline__ bool quartet_survives(const ListArgs& a, const PairRec& b, const PairRec& k, double Ib,
+                                                 double Ik) {
+  const double* pm = a.pmax;
+  const int ns = a.n_shell;
+  const int sa = b.sh_hi, sb = b.sh_lo, sc = k.sh_hi, sd = k.sh_lo;
+  double m = fmax(pm[sa * ns + sb], pm[sc * ns + sd]);
+  m = fmax(m, fmax(pm[sa * ns + sc], pm[sa * ns + sd]));
+  m = fmax(m, fmax(pm[sb * ns + sc], pm[sb * ns + sd]));
+  if (m < 1.0e-20) return false;                 // TOL(20)
+  return m * Ib * Ik > a.cutoff;
+}
+
+template <bool WRITE>
+__global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const long long* __restrict__ offsets,
+                           int2* __restrict__ out) {
+  const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= a.n_tasks) return;
+  const int2 task = a.tasks[t];
+  const int4 cp = a.cp[task.x];
+  const int i = task.y;
+  const int bra = a.sorted[cp.z + i];
+  const double Ib = a.sorted_imax[cp.z + i];
+  const PairRec b = a.pairs[bra];
+  const int jend = (cp.x == cp.y) ? i + 1 : a.cls_n[cp.y];
+  const double pg = __longlong_as_double((long long)*a.pglob);
+  long long base = WRITE ? offsets[t] : 0;
+  int cnt = 0;
+  for (int j0 = 0; j0 < jend; j0 += 32) {
+    const int j = j0 + lane;
+    bool ok = false, beyond = false;
+    int ket = 0;
+    if (j < jend) {
+      const double Ik = a.sorted_imax[cp.w + j];
+      if (!(Ib * Ik * pg > a.cutoff)) {
+        beyond = true;                           // kets are sorted by I_max: nothing further survives
+      } else {
+        ket = a.sorted[cp.w + j];
+        ok = quartet_survives(a, b, a.pairs[ket], Ib, Ik);
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (WRITE && ok) out[base + cnt + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
+    cnt += __popc(m);
+    if (__any_sync(0xffffffffu, beyond)) break;
+  }
+  if (!WRITE && lane == 0) counts[t] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// kernel: ERIs + digestion (one thread per contracted quartet)
+// ---------------------------------------------------------------------------
+struct JKArgs {
+  const int2* quartets;
+  long long n;
+  const PairRec* pairs;
+  const PrimPair* prim_full;
+  const PrimPair* prim_skip;
+  const double* P;              // Cartesian density, n_cart x n_cart
+  double* J;                    // Cartesian accumulators
+  double* K;
+  int n_cart;
+  unsigned long long* prim_count;   // per quartet class
+};
+
+template <int LA, int LB, int LC, int LD, typename T>
+__global__ void __launch_bounds__(128) k_jk(JKArgs a) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = t < a.n;
+  unsigned long long nprim = 0;
+  if (active) {
+    const int2 qd = a.quartets[t];
+    const PairRec b = a.pairs[qd.x];
+    const PairRec k = a.pairs[qd.y];
+    const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
+                          b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
+    const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
+    const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
+    const int nbp = any_same ? b.n_full : b.n_skip;
+    const int nkp = any_same ? k.n_full : k.n_skip;
+    nprim = (unsigned long long)nbp * nkp;
+    double f = 1.0;
+    if (b.sh_hi == b.sh_lo) f *= 0.5;
+    if (k.sh_hi == k.sh_lo) f *= 0.5;
+    if (qd.x == qd.y) f *= 0.5;
+    const double Rab[3] = {b.Rx, b.Ry, b.Rz};
+    const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
+    double I[Q::NA][Q::NB][Q::NC * Q::ND];
+    quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I);
+
+    const int n = a.n_cart;
+    const double* __restrict__ P = a.P;
+    const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
+    // J(ab) += f sum_cd I P(cd);  J(cd) += f sum_ab I P(ab)
+    double Pcd[Q::NC][Q::ND];
+#pragma unroll
+    for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Pcd[c][d] = __ldg(P + (size_t)(oc + c) * n + od + d);
+#pragma unroll
+    for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) {
+        double s = 0.0;
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
+        atomicAdd(a.J + (size_t)(oa + ia) * n + ob + ib, f * s);
+      }
+    double Pab[Q::NA][Q::NB];
+#pragma unroll
+    for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) Pab[ia][ib] = __ldg(P + (size_t)(oa + ia) * n + ob + ib);
+#pragma unroll
+    for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) {
+        double s = 0.0;
+#pragma unroll
+        for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+          for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
+        atomicAdd(a.J + (size_t)(oc + c) * n + od + d, f * s);
+      }
+    // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
+    // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
+#pragma unroll
+    for (int ia = 0; ia < Q::NA; ++ia) {
+      double Pad[Q::ND], Pac[Q::NC];
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Pad[d] = __ldg(P + (size_t)(oa + ia) * n + od + d);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) Pac[c] = __ldg(P + (size_t)(oa + ia) * n + oc + c);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int ib = 0; ib < Q::NB; ++ib)
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
+        atomicAdd(a.K + (size_t)(oa + ia) * n + oc + c, f * s);
+      }
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) {
+        double s = 0.0;
+#pragma unroll
+        for (int ib = 0; ib < Q::NB; ++ib)
+#pragma unroll
+          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
+        atomicAdd(a.K + (size_t)(oa + ia) * n + od + d, f * s);
+      }
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c) {
+          double s = 0.0;
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pad[d];
+          atomicAdd(a.K + (size_t)(ob + ib) * n + oc + c, f * s);
+        }
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pac[c];
+          atomicAdd(a.K + (size_t)(ob + ib) * n + od + d, f * s);
+        }
+      }
+    }
+  }
+  // primitive-quartet counter (per class, one atomic per warp)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nprim += __shfl_xor_sync(0xffffffffu, nprim, o);
+  if ((threadIdx.x & 31) == 0 && nprim) atomicAdd(a.prim_count + qclass_id(LA, LB, LC, LD), nprim);
+}
+
+// ---------------------------------------------------------------------------
+// kernel: warp-cooperative quartets (high angular momentum classes)
+// ---------------------------------------------------------------------------
+constexpr int WARPS_PER_BLOCK = 2;
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int la, int lb, int lc, int ld) {
+  extern __shared__ double smem_all[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* sm = smem_all + wib * W_SMEM;
+  const WarpQuartet q = wq_make(la, lb, lc, ld);
+  const long long nwarps = (long long)gridDim.x * WARPS_PER_BLOCK;
+  unsigned long long nprim = 0;
+  const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+  const int n = a.n_cart;
+  const double* __restrict__ P = a.P;
+  for (long long t = (long long)blockIdx.x * WARPS_PER_BLOCK + wib; t < a.n; t += nwarps) {
+    const int2 qd = a.quartets[t];
+    const PairRec b = a.pairs[qd.x];
+    const PairRec k = a.pairs[qd.y];
+    const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
+                          b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
+    const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
+    const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
+    const int nbp = any_same ? b.n_full : b.n_skip;
+    const int nkp = any_same ? k.n_full : k.n_skip;
+    double f = 1.0;
+    if (b.sh_hi == b.sh_lo) f *= 0.5;
+    if (k.sh_hi == k.sh_lo) f *= 0.5;
+    if (qd.x == qd.y) f *= 0.5;
+    const double Rab[3] = {b.Rx, b.Ry, b.Rz};
+    const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
+    double* I = nullptr;
+    const int np = warp_quartet(q, bp, nbp, kp, nkp, Rab, Rcd, sm, I);
+    if (lane == 0) nprim += (unsigned long long)np;
+    const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
+    const int ncd = nc * nd;
+    for (int e = lane; e < na * nb; e += 32) {          // J(ab)
+      const int ia = e / nb, ib = e % nb;
+      double s = 0.0;
+      for (int c = 0; c < nc; ++c)
+        for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
+      atomicAdd(a.J + (size_t)(oa + ia) * n + ob + ib, f * s);
+    }
+    for (int e = lane; e < ncd; e += 32) {              // J(cd)
+      const int c = e / nd, d = e % nd;
+      double s = 0.0;
+      for (int ia = 0; ia < na; ++ia)
+        for (int ib = 0; ib < nb; ++ib) s += I[(ia * nb + ib) * ncd + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ib);
+      atomicAdd(a.J + (size_t)(oc + c) * n + od + d, f * s);
+    }
+    for (int e = lane; e < na * nc; e += 32) {          // K(ac) = sum_bd I P(bd)
+      const int ia = e / nc, c = e % nc;
+      double s = 0.0;
+      for (int ib = 0; ib < nb; ++ib)
+        for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
+      atomicAdd(a.K + (size_t)(oa + ia) * n + oc + c, f * s);
+    }
+    for (int e = lane; e < na * nd; e += 32) {          // K(ad) = sum_bc I P(bc)
+      const int ia = e / nd, d = e % nd;
+      double s = 0.0;
+      for (int ib = 0; ib < nb; ++ib)
+        for (int c = 0; c < nc; ++c) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
+      atomicAdd(a.K + (size_t)(oa + ia) * n + od + d, f * s);
+    }
+    for (int e = lane; e < nb * nc; e += 32) {          // K(bc) = sum_ad I P(ad)
+      const int ib = e / nc, c = e % nc;
+      double s = 0.0;
+      for (int ia = 0; ia < na; ++ia)
+        for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
+      atomicAdd(a.K + (size_t)(ob + ib) * n + oc + c, f * s);
+    }
+    for (int e = lane; e < nb * nd; e += 32) {          // K(bd) = sum_ac I P(ac)
+      const int ib = e / nd, d = e % nd;
+      double s = 0.0;
+      for (int ia = 0; ia < na; ++ia)
+        for (int c = 0; c < nc; ++c) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
+      atomicAdd(a.K + (size_t)(ob + ib) * n + od + d, f * s);
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && nprim) atomicAdd(a.prim_count + qclass_id(la, lb, lc, ld), nprim);
+}
+
+// Schwarz bound of any pair class with the warp path (one warp per pair).
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int* __restrict__ ids, int n,
+                                                                      PairRec* __restrict__ pairs,
+                                                                      const PrimPair* __restrict__ prim_full,
+                                                                      int spherical, int la, int lb) {
+  extern __shared__ double smem_all[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* sm = smem_all + wib * W_SMEM;
+  const WarpQuartet q = wq_make(la, lb, la, lb);
+  const int na = ncart(la), nb = ncart(lb);
+  const bool sa = spherical && la >= 2, sb = spherical && lb >= 2;
+  const int MA = sa ? 2 * la + 1 : na, MB = sb ? 2 * lb + 1 : nb;
+  const long long nwarps = (long long)gridDim.x * WARPS_PER_BLOCK;
+  for (long long t = (long long)blockIdx.x * WARPS_PER_BLOCK + wib; t < n; t += nwarps) {
+    const int p = ids[t];
+    const PairRec pr = pairs[p];
+    const double R[3] = {pr.Rx, pr.Ry, pr.Rz};
+    double* I = nullptr;
+    warp_quartet(q, prim_full + pr.full_off, pr.n_full, prim_full + pr.full_off, pr.n_full, R, R, sm, I);
+    double m = 0.0;
+    for (int e = lane; e < MA * MB; e += 32) {
+      const int ma = e / MB, mb = e % MB;
+      double s = 0.0;
+      for (int ia = 0; ia < na; ++ia) {
+        const double ua = sa ? c_U[la][ia * (2 * la + 1) + ma] : (ia == ma ? 1.0 : 0.0);
+        if (ua == 0.0) continue;
+        for (int ib = 0; ib < nb; ++ib) {
+          const double ub = sb ? c_U[lb][ib * (2 * lb + 1) + mb] : (ib == mb ? 1.0 : 0.0);
+          if (ub == 0.0) continue;
+          for (int ic = 0; ic < na; ++ic) {
+            const double uc = sa ? c_U[la][ic * (2 * la + 1) + ma] : (ic == ma ? 1.0 : 0.0);
+            if (uc == 0.0) continue;
+            for (int id = 0; id < nb; ++id) {
+              const double ud = sb ? c_U[lb][id * (2 * lb + 1) + mb] : (id == mb ? 1.0 : 0.0);
+              s += ua * ub * uc * ud * I[((ia * nb + ib) * na + ic) * nb + id];
+            }
+          }
+        }
+      }
+      m = fmax(m, fabs(s));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) pairs[p].imax = sqrt(m);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// kernel: fold, reflect and return to the Tonto basis
+// ---------------------------------------------------------------------------
+__global__ void k_finalize(int n_bf, int n_cart, const double* __restrict__ Jc, const double* __restrict__ Kc,
+                           const int* __restrict__ bf_shell, const int* __restrict__ bf_local,
+                           const int* __restrict__ shell_l, const int* __restrict__ shell_cart, int spherical,
+                           double* __restrict__ J, double* __restrict__ K) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n_bf * n_bf) return;
+  const int j = (int)(t / n_bf), i = (int)(t % n_bf);       // column-major output (i, j)
+  const int si = bf_shell[i], sj = bf_shell[j];
+  const int mi = bf_local[i], mj = bf_local[j];
+  const int li = shell_l[si], lj = shell_l[sj];
+  const int ci = shell_cart[si], cj = shell_cart[sj];
+  const bool ti = spherical && li >= 2, tj = spherical && lj >= 2;
+  double sJ = 0.0, sK = 0.0;
+  const int ni = ti ? ncart(li) : 1, nj = tj ? ncart(lj) : 1;
+  for (int p = 0; p < ni; ++p) {
+    const double up = ti ? c_U[li][p * (2 * li + 1) + mi] : 1.0;
+    if (up == 0.0) continue;
+    const int cp = ti ? ci + p : ci + mi;
+    for (int q = 0; q < nj; ++q) {
+      const double uq = tj ? c_U[lj][q * (2 * lj + 1) + mj] : 1.0;
+      if (uq == 0.0) continue;
+      const int cq = tj ? cj + q : cj + mj;
+      const double w = up * uq;
+      sJ += w * (Jc[(size_t)cp * n_cart + cq] + Jc[(size_t)cq * n_cart + cp]);
+      sK += w * (Kc[(size_t)cp * n_cart + cq] + Kc[(size_t)cq * n_cart + cp]);
+    }
+  }
+  J[(size_t)j * n_bf + i] = 2.0 * sJ;
+  K[(size_t)j * n_bf + i] = sK;
+}
+
+__global__ void k_fock(long long n, const double* __restrict__ H, const double* __restrict__ J,
+                       const double* __restrict__ K, double* __restrict__ F) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) F[t] = H[t] + J[t] - 0.5 * K[t];
+}
+
+// ---------------------------------------------------------------------------
+// host: spherical matrices (Helgaker-Jorgensen-Olsen real solid harmonics,
+// the recurrence of gaussian_data.foo:1143-1290; columns m = 0,+1,-1,+2,...)
+// ---------------------------------------------------------------------------
+std::vector<double> spherical_matrix(int l) {
+  auto col = [](int m) { return m == 0 ? 0 : (m > 0 ? 2 * m - 1 : -2 * m); };
+  std::vector<std::vector<double>> S(l + 1);
+  S[0] = {1.0};
+  for (int L = 0; L < l; ++L) {
+    const int nsL = 2 * L + 1, nsP = 2 * L + 3;
+    std::vector<double> nx((size_t)ncart(L + 1) * nsP, 0.0);
+    const double top = 2 * L + 1;
+    const double fac = std::sqrt((L == 0 ? 2.0 : 1.0) * top / (top + 1));
+    const double del = L == 0 ? 0.0 : 1.0;
+    for (int i = 0; i < ncart(L); ++i) {
+      const int X = CT.x[CT.first[L] + i], Y = CT.y[CT.first[L] + i], Z = CT.z[CT.first[L] + i];
+      const int ix = CT.idx[X + 1][Y][Z], iy = CT.idx[X][Y + 1][Z], iz = CT.idx[X][Y][Z + 1];
+      const double vp = fac * S[L][i * nsL + col(L)], vm = fac * S[L][i * nsL + col(-L)] * del;
+      nx[ix * nsP + col(L + 1)] += vp;
+      nx[iy * nsP + col(L + 1)] -= vm;
+      nx[ix * nsP + col(-L - 1)] += vm;
+      nx[iy * nsP + col(-L - 1)] += vp;
+      for (int M = -L; M <= L; ++M)
+        nx[iz * nsP + col(M)] += top / std::sqrt((double)(L + M + 1) * (L - M + 1)) * S[L][i * nsL + col(M)];
+    }
+    if (L >= 1) {
+      const int nsM = 2 * L - 1;
+      for (int i = 0; i < ncart(L - 1); ++i) {
+        const int X = CT.x[CT.first[L - 1] + i], Y = CT.y[CT.first[L - 1] + i], Z = CT.z[CT.first[L - 1] + i];
+        const int ix = CT.idx[X + 2][Y][Z], iy = CT.idx[X][Y + 2][Z], iz = CT.idx[X][Y][Z + 2];
+        for (int M = -L + 1; M <= L - 1; ++M) {
+          const double v = std::sqrt((double)(L + M) * (L - M) / ((double)(L + M + 1) * (L - M + 1))) *
+                           S[L - 1][i * nsM + col(M)];
+          nx[ix * nsP + col(M)] -= v;
+          nx[iy * nsP + col(M)] -= v;
+          nx[iz * nsP + col(M)] -= v;
+        }
+      }
+    }
+    S[L + 1] = nx;
+  }
+  return S[l];
+}
+
+// ---------------------------------------------------------------------------
+// host: device buffer
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DBuf() { if (p) cudaFree(p); }
+  cudaError_t reserve(size_t m) {
+    if (m <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
+    if (e == cudaSuccess) n = std::max<size_t>(m, 1);
+    return e;
+  }
+};
+
+}  // namespace tf
+
+// ===========================================================================
+// context
+// ===========================================================================
+struct tf_ctx {
+  tf_options opt;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  // basis (host copies)
+  int n_atom = 0, n_shell = 0, n_bf = 0, n_cart = 0, spherical = 0;
+  std::vector<double> xyz;
+  std::vector<int> shell_atom, shell_l, shell_nprim, shell_first_bf, shell_poff, shell_cart, shell_nbf;
+  std::vector<double> exps, coefs;
+  // pairs
+  long long n_pairs = 0;
+  std::vector<tf::PairRec> pairs_h;
+  std::vector<int> cls_n, cls_off;                // per pair class
+  std::vector<int4> cps;                          // class pairs
+  std::vector<int> cp_first_task;                 // first task of each class pair
+  long long n_tasks = 0;
+  bool geometry_ready = false;
+  // device
+  tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax;
+  tf::DBuf<int> d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
+  tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_cls_n, d_schwarz_ids;
+  tf::DBuf<long long> d_counts;
+  tf::DBuf<tf::PairRec> d_pairs;
+  tf::DBuf<tf::PrimPair> d_prim_full, d_prim_skip;
+  tf::DBuf<int2> d_tasks, d_quartets;
+  tf::DBuf<int4> d_cps;
+  tf::DBuf<long long> d_offsets;
+  tf::DBuf<unsigned long long> d_pglob, d_prim_count;
+  tf::DBuf<unsigned char> d_scan_tmp;
+  std::vector<double> max_I_tonto;                // per Tonto pair index
+  tf_stats stats{};
+};
+
+namespace tf {
+
+static int set_device(tf_ctx* c) {
+  TF_CUDA(cudaSetDevice(c->device));
+  return TF_OK;
+}
+
+// Build pair records, run pair prep + Schwarz, sort pairs per class.
+static int setup_pairs(tf_ctx* c) {
+  const int ns = c->n_shell;
+  c->n_pairs = (long long)ns * (ns + 1) / 2;
+  c->pairs_h.assign(c->n_pairs, PairRec{});
+  long long full_tot = 0;
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b <= a; ++b) {
+      PairRec& p = c->pairs_h[(long long)a * (a + 1) / 2 + b];
+      const bool a_hi = c->shell_l[a] >= c->shell_l[b];
+      p.sh_hi = a_hi ? a : b;
+      p.sh_lo = a_hi ? b : a;
+      p.atom_hi = c->shell_atom[p.sh_hi];
+      p.atom_lo = c->shell_atom[p.sh_lo];
+      p.cart_hi = c->shell_cart[p.sh_hi];
+      p.cart_lo = c->shell_cart[p.sh_lo];
+      p.n_full = c->shell_nprim[a] * c->shell_nprim[b];
+      p.full_off = (int)full_tot;
+      p.skip_off = (int)full_tot;
+      full_tot += p.n_full;
+      p.cls = pair_class(c->shell_l[p.sh_hi], c->shell_l[p.sh_lo]);
+      p.tonto_ab = (int)((long long)a * (a + 1) / 2 + b);
+    }
+  TF_CUDA(c->d_pairs.reserve(c->n_pairs));
+  TF_CUDA(c->d_prim_full.reserve(full_tot));
+  TF_CUDA(c->d_prim_skip.reserve(full_tot));
+  TF_CUDA(cudaMemcpyAsync(c->d_pairs.p, c->pairs_h.data(), c->n_pairs * sizeof(PairRec), cudaMemcpyHostToDevice,
+                          c->stream));
+  const int thr = 128;
+  k_pair_prep<<<(unsigned)((c->n_pairs + thr - 1) / thr), thr, 0, c->stream>>>(
+      (int)c->n_pairs, c->d_pairs.p, c->d_xyz.p, c->d_shell_nprim.p, c->d_shell_poff.p, c->d_exps.p, c->d_coefs.p,
+      c->d_prim_full.p, c->d_prim_skip.p, c->opt.eri_primitive_pair_cutoff);
+  TF_CUDA(cudaGetLastError());
+  // Schwarz per pair class
+  std::vector<std::vector<int>> by_cls(NPAIRCLS);
+  for (long long p = 0; p < c->n_pairs; ++p) by_cls[c->pairs_h[p].cls].push_back((int)p);
+  std::vector<int> ids;
+  std::vector<int> cls_start(NPAIRCLS + 1, 0);
+  for (int k = 0; k < NPAIRCLS; ++k) {
+    cls_start[k] = (int)ids.size();
+    ids.insert(ids.end(), by_cls[k].begin(), by_cls[k].end());
+  }
+  cls_start[NPAIRCLS] = (int)ids.size();
+  TF_CUDA(c->d_schwarz_ids.reserve(ids.size()));
+  TF_CUDA(cudaMemcpyAsync(c->d_schwarz_ids.p, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice,
+                          c->stream));
+#define TF_SCHWARZ(LH, LL)                                                                                 \
+  {                                                                                                        \
+    const int k = pair_class(LH, LL);                                                                      \
+    const int nk = cls_start[k + 1] - cls_start[k];                                                        \
+    if (nk > 0)                                                                                            \
+      k_schwarz<LH, LL><<<(nk + 63) / 64, 64, 0, c->stream>>>(c->d_schwarz_ids.p + cls_start[k], nk,       \
+                                                              c->d_pairs.p, c->d_prim_full.p, c->spherical); \
+  }
+  TF_SCHWARZ(0, 0) TF_SCHWARZ(1, 0) TF_SCHWARZ(1, 1) TF_SCHWARZ(2, 0)
+#undef TF_SCHWARZ
+  for (int lh = 2; lh <= 2; ++lh)
+    for (int ll = 1; ll <= lh; ++ll) {
+      const int k = pair_class(lh, ll);
+      const int nk = cls_start[k + 1] - cls_start[k];
+      if (nk > 0)
+        k_schwarz_warp<<<std::min(4096, (nk + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK), 32 * WARPS_PER_BLOCK,
+                         WARPS_PER_BLOCK * W_SMEM * sizeof(double), c->stream>>>(
+            c->d_schwarz_ids.p + cls_start[k], nk, c->d_pairs.p, c->d_prim_full.p, c->spherical, lh, ll);
+    }
+  TF_CUDA(cudaGetLastError());
+  TF_CUDA(cudaMemcpyAsync(c->pairs_h.data(), c->d_pairs.p, c->n_pairs * sizeof(PairRec), cudaMemcpyDeviceToHost,
+                          c->stream));
+  TF_CUDA(cudaStreamSynchronize(c->stream));
+  c->max_I_tonto.assign(c->n_pairs, 0.0);
+  for (long long p = 0; p < c->n_pairs; ++p) c->max_I_tonto[c->pairs_h[p].tonto_ab] = c->pairs_h[p].imax;
+  // sort each class by I_max descending (ties: Tonto pair index) -> deterministic
+  std::vector<int> sorted;
+  std::vector<double> simax;
+  c->cls_n.assign(NPAIRCLS, 0);
+  c->cls_off.assign(NPAIRCLS, 0);
+  for (int k = 0; k < NPAIRCLS; ++k) {
+    auto v = by_cls[k];
+    std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return c->pairs_h[x].imax > c->pairs_h[y].imax; });
+    c->cls_off[k] = (int)sorted.size();
+    c->cls_n[k] = (int)v.size();
+    for (int p : v) { sorted.push_back(p); simax.push_back(c->pairs_h[p].imax); }
+  }
+  TF_CUDA(c->d_sorted.reserve(sorted.size()));
+  TF_CUDA(c->d_sorted_imax.reserve(simax.size()));
+  TF_CUDA(c->d_cls_n.reserve(NPAIRCLS));
+  TF_CUDA(cudaMemcpyAsync(c->d_sorted.p, sorted.data(), sorted.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA(cudaMemcpyAsync(c->d_sorted_imax.p, simax.data(), simax.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          c->stream));
+  TF_CUDA(cudaMemcpyAsync(c->d_cls_n.p, c->cls_n.data(), NPAIRCLS * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  // class pairs and bra tasks
+  c->cps.clear();
+  c->cp_first_task.clear();
+  std::vector<int2> tasks;
+  for (int p1 = 0; p1 < NPAIRCLS; ++p1)
+    for (int p2 = 0; p2 <= p1; ++p2) {
+      if (c->cls_n[p1] == 0 || c->cls_n[p2] == 0) continue;
+      const int cpi = (int)c->cps.size();
+      c->cps.push_back(make_int4(p1, p2, c->cls_off[p1], c->cls_off[p2]));
+      c->cp_first_task.push_back((int)tasks.size());
+      for (int i = 0; i < c->cls_n[p1]; ++i) tasks.push_back(make_int2(cpi, i));
+    }
+  c->cp_first_task.push_back((int)tasks.size());
+  c->n_tasks = (long long)tasks.size();
+  TF_CUDA(c->d_cps.reserve(c->cps.size()));
+  TF_CUDA(c->d_tasks.reserve(tasks.size()));
+  TF_CUDA(c->d_counts.reserve(tasks.size() + 1));
+  TF_CUDA(c->d_offsets.reserve(tasks.size() + 1));
+  TF_CUDA(cudaMemcpyAsync(c->d_cps.p, c->cps.data(), c->cps.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA(cudaMemcpyAsync(c->d_tasks.p, tasks.data(), tasks.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA(cudaStreamSynchronize(c->stream));
+  c->geometry_ready = true;
+  return TF_OK;
+}
+
+// pair class id -> (lh, ll)
+static void class_l(int k, int& lh, int& ll) {
+  lh = 0;
+  while ((lh + 1) * (lh + 2) / 2 <= k) ++lh;
+  ll = k - lh * (lh + 1) / 2;
+}
+
+template <int LA, int LB, int LC, int LD>
+static void launch_jk(const JKArgs& a, cudaStream_t s) {
+  if (a.n <= 0) return;
+  const int thr = 128;
+  k_jk<LA, LB, LC, LD, double><<<(unsigned)((a.n + thr - 1) / thr), thr, 0, s>>>(a);
+}
+
+static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStream_t s) {
+  const int key = ((la * 3 + lb) * 3 + lc) * 3 + ld;
+  switch (key) {
+#define TF_CASE(A, B, C, D) \
+  case ((A * 3 + B) * 3 + C) * 3 + D: launch_jk<A, B, C, D>(a, s); return TF_OK;
+    TF_CASE(0, 0, 0, 0)
+    TF_CASE(1, 0, 0, 0) TF_CASE(1, 0, 1, 0)
+    TF_CASE(1, 1, 0, 0) TF_CASE(1, 1, 1, 0)
+    TF_CASE(2, 0, 0, 0) TF_CASE(2, 0, 1, 0) TF_CASE(2, 0, 1, 1) TF_CASE(2, 0, 2, 0)
+    TF_CASE(2, 1, 0, 0) TF_CASE(2, 1, 1, 0)
+    TF_CASE(2, 2, 0, 0)
+#undef TF_CASE
+    default: {
+      if (std::max(std::max(la, lb), std::max(lc, ld)) > WL_MAX) {
+        set_error("quartet class not built");
+        return TF_EUNSUPPORTED;
+      }
+      int dev = 0, nsm = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      const long long blocks = std::min<long long>((a.n + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK, (long long)nsm * 16);
+      k_jk_warp<<<(unsigned)blocks, 32 * WARPS_PER_BLOCK, WARPS_PER_BLOCK * W_SMEM * sizeof(double), s>>>(a, la, lb, lc, ld);
+      return TF_OK;
+    }
+  }
+}
+
+// Algorithmic FLOP model (per primitive quartet and per contracted quartet).
+double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
+  const int L = la + lb + lc + ld, nr = L / 2 + 1;
+  const int d1 = la + lb + 1, d2 = lc + ld + 1;
+  const int ne = ncart_upto(la + lb) - ncart_upto(la - 1), nf = ncart_upto(lc + ld) - ncart_upto(lc - 1);
+  const double per_prim = 20.0 + 4.0 * nr * TF_RYS_DEG + nr * (10.0 + 3.0 * (4.0 + 6.0 * d1 * d2) + d1 * d2 +
+                                                              3.0 * ne * nf);
+  const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+  const double nint = (double)na * nb * nc * nd;
+  double hrr = 0.0;
+  for (int k = 1; k <= ld; ++k) hrr += 2.0 * ne * (ncart_upto(lc + ld - k) - ncart_upto(lc - 1)) * ncart(k);
+  for (int k = 1; k <= lb; ++k) hrr += 2.0 * nc * nd * (ncart_upto(la + lb - k) - ncart_upto(la - 1)) * ncart(k);
+  const double per_q = hrr + 12.0 * nint;
+  return npq * per_prim + nq * per_q;
+}
+
+static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags) {
+  if (!c->geometry_ready) { set_error("no geometry"); return TF_ESTATE; }
+  if (flags & ~(TF_JK_MIXED | TF_JK_DELTA | TF_JK_NO_COPYBACK)) { set_error("unknown flags"); return TF_EINVAL; }
+  cudaStream_t s = c->stream;
+  const int nc = c->n_cart, nb = c->n_bf, ns = c->n_shell;
+  int kernels = 0;
+  TF_CUDA(cudaEventRecord(c->ev0, s));
+  // density in the Cartesian basis, pair maxima
+  {
+    const long long n2 = (long long)nc * nc;
+    k_density_to_cart<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nc, nb, dP, c->d_cart_shell.p, c->d_cart_local.p,
+                                                                   c->d_shell_l.p, c->d_shell_first_bf.p,
+                                                                   c->spherical, c->d_Pc.p);
+    TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, sizeof(unsigned long long), s));
+    const long long s2 = (long long)ns * ns;
+    k_pmax<<<(unsigned)((s2 + 255) / 256), 256, 0, s>>>(ns, nb, dP, c->d_shell_first_bf.p, c->d_shell_nbf.p,
+                                                        c->d_pmax.p, c->d_pglob.p);
+    kernels += 2;
+  }
+  // quartet lists
+  ListArgs la{c->d_tasks.p, c->n_tasks, c->d_cps.p, c->d_cls_n.p, c->d_sorted.p, c->d_sorted_imax.p, c->d_pairs.p,
+              c->d_pmax.p, c->d_pglob.p, ns, c->opt.eri_schwarz_cutoff};
+  const long long thr_list = 256;
+  const unsigned grid_list = (unsigned)((c->n_tasks * 32 + thr_list - 1) / thr_list);
+  k_quartets<false><<<grid_list, (unsigned)thr_list, 0, s>>>(la, c->d_counts.p, nullptr, nullptr);
+  kernels++;
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(c->n_tasks + 1), s);
+  TF_CUDA(c->d_scan_tmp.reserve(tmp_bytes));
+  TF_CUDA(cudaMemsetAsync(c->d_counts.p + c->n_tasks, 0, sizeof(long long), s));
+  TF_CUDA(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp_bytes, c->d_counts.p, c->d_offsets.p,
+                                        (int)(c->n_tasks + 1), s));
+  std::vector<long long> cp_off(c->cps.size() + 1);
+  for (size_t k = 0; k <= c->cps.size(); ++k)
+    TF_CUDA(cudaMemcpyAsync(&cp_off[k], c->d_offsets.p + c->cp_first_task[k], sizeof(long long),
+                            cudaMemcpyDeviceToHost, s));
+  TF_CUDA(cudaStreamSynchronize(s));
+  const long long nq_total = cp_off.back();
+  TF_CUDA(c->d_quartets.reserve(nq_total));
+  k_quartets<true><<<grid_list, (unsigned)thr_list, 0, s>>>(la, nullptr, c->d_offsets.p, c->d_quartets.p);
+  kernels++;
+  // ERIs + digestion
+  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, (size_t)nc * nc * sizeof(double), s));
+  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, (size_t)nc * nc * sizeof(double), s));
+  TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
+  TF_CUDA(cudaEventRecord(c->ev1, s));
+  double flops = 0.0;
+  std::vector<long long> cp_n(c->cps.size());
+  for (size_t k = 0; k < c->cps.size(); ++k) {
+    const int4 cp = c->cps[k];
+    int l1h, l1l, l2h, l2l;
+    class_l(cp.x, l1h, l1l);
+    class_l(cp.y, l2h, l2l);
+    JKArgs a{c->d_quartets.p + cp_off[k], cp_off[k + 1] - cp_off[k], c->d_pairs.p, c->d_prim_full.p,
+             c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, nc, c->d_prim_count.p};
+    cp_n[k] = a.n;
+    if (a.n == 0) continue;
+    int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s);
+    if (rc != TF_OK) return rc;
+    kernels++;
+  }
+  TF_CUDA(cudaGetLastError());
+  TF_CUDA(cudaEventRecord(c->ev2, s));
+  {
+    const long long n2 = (long long)nb * nb;
+    k_finalize<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, c->d_Jc.p, c->d_Kc.p, c->d_bf_shell.p,
+                                                            c->d_bf_local.p, c->d_shell_l.p, c->d_shell_cart.p,
+                                                            c->spherical, dJ, dK);
+    kernels++;
+  }
+  TF_CUDA(cudaGetLastError());
+  std::vector<unsigned long long> pc(NQCLS);
+  TF_CUDA(cudaMemcpyAsync(pc.data(), c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  TF_CUDA(cudaStreamSynchronize(s));
+  float ms_all = 0.f, ms_eri = 0.f;
+  // ev0..ev2 spans the list building and the ERIs; the finalize kernel is small
+  TF_CUDA(cudaEventElapsedTime(&ms_eri, c->ev1, c->ev2));
+  TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
+  double npq = 0.0;
+  for (size_t k = 0; k < c->cps.size(); ++k) {
+    const int4 cp = c->cps[k];
+    int l1h, l1l, l2h, l2l;
+    class_l(cp.x, l1h, l1l);
+    class_l(cp.y, l2h, l2l);
+    const double p = (double)pc[qclass_id(l1h, l1l, l2h, l2l)];
+    npq += p;
+    flops += class_flops(l1h, l1l, l2h, l2l, (double)cp_n[k], p);
+  }
+  c->stats.build_ms = ms_all;
+  c->stats.eri_ms = ms_eri;
+  c->stats.quartets = (double)nq_total;
+  c->stats.quartets_fp32 = 0.0;
+  c->stats.prim_quartets = npq;
+  c->stats.flops = flops;
+  c->stats.kernels = kernels;
+  return TF_OK;
+}
+
+}  // namespace tf
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int tf_default_options(tf_options* opt) {
+  if (!opt) return TF_EINVAL;
+  opt->eri_schwarz_cutoff = 1.0e-9;
+  opt->eri_primitive_pair_cutoff = 1.0e-6;
+  opt->mixed_fp32_cut = 1.0e-6;
+  opt->device = 0;
+  opt->deterministic = 0;
+  return TF_OK;
+}
+
+int tf_ctx_create(const tf_basis* B, const tf_options* opt, tf_ctx** out) {
+  using namespace tf;
+  if (!B || !out) { set_error("null argument"); return TF_EINVAL; }
+  *out = nullptr;
+  if (B->n_atom <= 0 || B->n_shell <= 0 || !B->xyz || !B->shell_atom || !B->shell_l || !B->shell_nprim ||
+      !B->shell_first_bf || !B->exponents || !B->coefficients) {
+    set_error("incomplete basis description");
+    return TF_EINVAL;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { set_error("no CUDA device"); return TF_ENODEVICE; }
+  tf_ctx* c = new tf_ctx();
+  if (opt) c->opt = *opt; else tf_default_options(&c->opt);
+  c->device = c->opt.device;
+  if (c->device < 0 || c->device >= ndev) { delete c; set_error("bad device ordinal"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) { delete c; return rc; }
+  c->n_atom = B->n_atom;
+  c->n_shell = B->n_shell;
+  c->spherical = B->is_spherical ? 1 : 0;
+  c->xyz.assign(B->xyz, B->xyz + 3 * B->n_atom);
+  c->shell_atom.assign(B->shell_atom, B->shell_atom + B->n_shell);
+  c->shell_l.assign(B->shell_l, B->shell_l + B->n_shell);
+  c->shell_nprim.assign(B->shell_nprim, B->shell_nprim + B->n_shell);
+  c->shell_first_bf.assign(B->shell_first_bf, B->shell_first_bf + B->n_shell);
+  int np = 0, ncart_tot = 0, nbf = 0;
+  for (int s = 0; s < B->n_shell; ++s) {
+    const int l = c->shell_l[s];
+    if (l < 0 || l > LMAX_SUPPORTED) { delete c; set_error("angular momentum beyond d not built"); return TF_EUNSUPPORTED; }
+    if (c->shell_atom[s] < 0 || c->shell_atom[s] >= B->n_atom || c->shell_nprim[s] <= 0) {
+      delete c; set_error("bad shell record"); return TF_EINVAL;
+    }
+    c->shell_poff.push_back(np);
+    np += c->shell_nprim[s];
+    c->shell_cart.push_back(ncart_tot);
+    ncart_tot += ncart(l);
+    const int nbf_s = (c->spherical && l >= 2) ? 2 * l + 1 : ncart(l);
+    c->shell_nbf.push_back(nbf_s);
+    if (c->shell_first_bf[s] != nbf) { delete c; set_error("shell_first_bf not contiguous"); return TF_EINVAL; }
+    nbf += nbf_s;
+  }
+  c->n_bf = nbf;
+  c->n_cart = ncart_tot;
+  c->exps.assign(B->exponents, B->exponents + np);
+  c->coefs.assign(B->coefficients, B->coefficients + np);
+  std::vector<int> cart_shell, cart_local, bf_shell, bf_local;
+  for (int s = 0; s < B->n_shell; ++s) {
+    for (int i = 0; i < ncart(c->shell_l[s]); ++i) { cart_shell.push_back(s); cart_local.push_back(i); }
+    for (int i = 0; i < c->shell_nbf[s]; ++i) { bf_shell.push_back(s); bf_local.push_back(i); }
+  }
+  // spherical matrices
+  {
+    double U[4][70];
+    std::memset(U, 0, sizeof(U));
+    for (int l = 0; l <= 3; ++l) {
+      std::vector<double> m = spherical_matrix(l);
+      std::copy(m.begin(), m.end(), U[l]);
+    }
+    unsigned char comp[3][NCOMP_ALL];
+    unsigned char cidx[LCOMP + 1][LCOMP + 1][LCOMP + 1];
+    std::memset(cidx, 0, sizeof(cidx));
+    for (int g = 0; g < NCOMP_ALL; ++g) {
+      comp[0][g] = (unsigned char)CT.x[g]; comp[1][g] = (unsigned char)CT.y[g]; comp[2][g] = (unsigned char)CT.z[g];
+      cidx[CT.x[g]][CT.y[g]][CT.z[g]] = (unsigned char)CT.idx[CT.x[g]][CT.y[g]][CT.z[g]];
+    }
+    if (cudaMemcpyToSymbol(c_U, U, sizeof(U)) != cudaSuccess || cudaMemcpyToSymbol(c_comp, comp, sizeof(comp)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_cidx, cidx, sizeof(cidx)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_jk_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_schwarz_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess) {
+      delete c; set_error("constant upload"); return TF_ECUDA;
+    }
+  }
+#define TF_TRY(x)                 \
+  do {                            \
+    int r__ = (x);                \
+    if (r__) { tf_ctx_destroy(c); return r__; } \
+  } while (0)
+  auto up = [&](auto& buf, const auto& v) -> int {
+    if (buf.reserve(v.size()) != cudaSuccess) { set_error("device allocation"); return TF_ENOMEM; }
+    if (cudaMemcpy(buf.p, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("upload"); return TF_ECUDA;
+    }
+    return TF_OK;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->ev2) != cudaSuccess) {
+    tf_ctx_destroy(c); set_error("stream/event creation"); return TF_ECUDA;
+  }
+  TF_TRY(up(c->d_xyz, c->xyz));
+  TF_TRY(up(c->d_exps, c->exps));
+  TF_TRY(up(c->d_coefs, c->coefs));
+  TF_TRY(up(c->d_shell_nprim, c->shell_nprim));
+  TF_TRY(up(c->d_shell_poff, c->shell_poff));
+  TF_TRY(up(c->d_shell_l, c->shell_l));
+  TF_TRY(up(c->d_shell_first_bf, c->shell_first_bf));
+  TF_TRY(up(c->d_shell_nbf, c->shell_nbf));
+  TF_TRY(up(c->d_shell_cart, c->shell_cart));
+  TF_TRY(up(c->d_cart_shell, cart_shell));
+  TF_TRY(up(c->d_cart_local, cart_local));
+  TF_TRY(up(c->d_bf_shell, bf_shell));
+  TF_TRY(up(c->d_bf_local, bf_local));
+  const size_t nb2 = (size_t)nbf * nbf, nc2 = (size_t)ncart_tot * ncart_tot;
+  if (c->d_P.reserve(nb2) || c->d_J.reserve(nb2) || c->d_K.reserve(nb2) || c->d_H.reserve(nb2) ||
+      c->d_Pc.reserve(nc2) || c->d_Jc.reserve(nc2) || c->d_Kc.reserve(nc2) ||
+      c->d_pmax.reserve((size_t)c->n_shell * c->n_shell) || c->d_pglob.reserve(1) || c->d_prim_count.reserve(NQCLS)) {
+    tf_ctx_destroy(c); set_error("device allocation"); return TF_ENOMEM;
+  }
+  TF_TRY(setup_pairs(c));
+#undef TF_TRY
+  *out = c;
+  return TF_OK;
+}
+
+int tf_set_geometry(tf_ctx* c, const double* xyz) {
+  using namespace tf;
+  if (!c || !xyz) return TF_EINVAL;
+  int rc = set_device(c);
+  if (rc) return rc;
+  c->xyz.assign(xyz, xyz + 3 * c->n_atom);
+  TF_CUDA(cudaMemcpy(c->d_xyz.p, c->xyz.data(), c->xyz.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->geometry_ready = false;
+  return setup_pairs(c);
+}
+
+int tf_build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, void* stream) {
+  using namespace tf;
+  if (!c || !dP || !dJ || !dK) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  if (user && user != c->stream) {
+    // order the context stream after the caller's work, and the caller's after ours
+    cudaEvent_t e;
+    TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TF_CUDA(cudaEventRecord(e, user));
+    TF_CUDA(cudaStreamWaitEvent(c->stream, e, 0));
+    rc = build_jk_device(c, dP, dJ, dK, flags);
+    TF_CUDA(cudaEventRecord(e, c->stream));
+    TF_CUDA(cudaStreamWaitEvent(user, e, 0));
+    TF_CUDA(cudaEventDestroy(e));
+    return rc;
+  }
+  return build_jk_device(c, dP, dJ, dK, flags);
+}
+
+int tf_build_jk(tf_ctx* c, const double* P, double* J, double* K, int flags) {
+  using namespace tf;
+  if (!c || !P || !J || !K) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  const size_t bytes = (size_t)c->n_bf * c->n_bf * sizeof(double);
+  TF_CUDA(cudaMemcpyAsync(c->d_P.p, P, bytes, cudaMemcpyHostToDevice, c->stream));
+  rc = build_jk_device(c, c->d_P.p, c->d_J.p, c->d_K.p, flags);
+  if (rc) return rc;
+  TF_CUDA(cudaMemcpyAsync(J, c->d_J.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaMemcpyAsync(K, c->d_K.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaStreamSynchronize(c->stream));
+  c->stats.h2d_bytes = (long long)bytes;
+  c->stats.d2h_bytes = 2 * (long long)bytes;
+  return TF_OK;
+}
+
+int tf_build_fock(tf_ctx* c, const double* P, const double* H, double* F) {
+  using namespace tf;
+  if (!c || !P || !H || !F) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  const size_t n2 = (size_t)c->n_bf * c->n_bf, bytes = n2 * sizeof(double);
+  TF_CUDA(cudaMemcpyAsync(c->d_P.p, P, bytes, cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA(cudaMemcpyAsync(c->d_H.p, H, bytes, cudaMemcpyHostToDevice, c->stream));
+  rc = build_jk_device(c, c->d_P.p, c->d_J.p, c->d_K.p, 0);
+  if (rc) return rc;
+  k_fock<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>((long long)n2, c->d_H.p, c->d_J.p, c->d_K.p, c->d_J.p);
+  TF_CUDA(cudaGetLastError());
+  TF_CUDA(cudaMemcpyAsync(F, c->d_J.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaStreamSynchronize(c->stream));
+  c->stats.h2d_bytes = 2 * (long long)bytes;
+  c->stats.d2h_bytes = (long long)bytes;
+  return TF_OK;
+}
+
+int tf_build_jk_batch(tf_ctx** ctx, int n, const double* const* P, double* const* J, double* const* K, int flags) {
+  if (!ctx || n < 0 || (n > 0 && (!P || !J || !K))) return TF_EINVAL;
+  for (int i = 0; i < n; ++i) {
+    int rc = tf_build_jk(ctx[i], P[i], J[i], K[i], flags);
+    if (rc) return rc;
+  }
+  return TF_OK;
+}
+
+int tf_last_stats(const tf_ctx* c, tf_stats* s) {
+  if (!c || !s) return TF_EINVAL;
+  *s = c->stats;
+  return TF_OK;
+}
+
+int tf_n_bf(const tf_ctx* c) { return c ? c->n_bf : TF_EINVAL; }
+
+int tf_schwarz(const tf_ctx* c, double* max_I) {
+  if (!c || !max_I) return TF_EINVAL;
+  std::copy(c->max_I_tonto.begin(), c->max_I_tonto.end(), max_I);
+  return TF_OK;
+}
+
+void tf_ctx_destroy(tf_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev2) cudaEventDestroy(c->ev2);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* tf_error_string(int code) {
+  switch (code) {
+    case TF_OK: return "ok";
+    case TF_EINVAL: return "invalid argument";
+    case TF_ECUDA: return tf::g_last_error.empty() ? "CUDA error" : tf::g_last_error.c_str();
+    case TF_ENOMEM: return "out of memory";
+    case TF_EUNSUPPORTED: return "unsupported (angular momentum or size)";
+    case TF_ETIMEOUT: return "bounded device wait ran out";
+    case TF_ENODEVICE: return "no usable CUDA device";
+    case TF_ESTATE: return "call out of order";
+    default: return "unknown error";
+  }
+}
+
+const char* tf_version(void) { return "tontofock 0.1 (sm_100a)"; }
+
+}  // extern "C"

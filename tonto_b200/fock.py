@@ -1,0 +1,186 @@
+"""Host-side mirror of Tonto's J/K builder interface over the C ABI (include/tontofock.h).
+
+``FockBuilder`` plays the role of ``MOLECULE.FOCK`` for one molecule:
+
+* ``make_r_JK(P)``        -> (J, K)      as make_r_JK_direct / make_r_JK_engine
+                                          (molecule.fock.foo:1235-1505)
+* ``make_r_Fock_mx(P, H)`` -> F = H + J - K/2  as make_r_Fock_mx (:88-155)
+* ``max_I``               -> Schwarz bounds as initialize_max_I (:3705-3752)
+
+Arrays are numpy (host) or torch CUDA tensors (device entry point).  The CUDA
+library is required: if it cannot be loaded, or no device is present, the calls
+raise — there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .basis import Molecule
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtontofock.so")
+
+TF_JK_FULL = 0x0
+TF_JK_MIXED = 0x1
+TF_JK_DELTA = 0x2
+
+
+class TontoFockError(RuntimeError):
+    pass
+
+
+class _Basis(ctypes.Structure):
+    _fields_ = [("n_atom", ctypes.c_int), ("xyz", ctypes.POINTER(ctypes.c_double)),
+                ("n_shell", ctypes.c_int), ("shell_atom", ctypes.POINTER(ctypes.c_int)),
+                ("shell_l", ctypes.POINTER(ctypes.c_int)), ("shell_nprim", ctypes.POINTER(ctypes.c_int)),
+                ("shell_first_bf", ctypes.POINTER(ctypes.c_int)), ("exponents", ctypes.POINTER(ctypes.c_double)),
+                ("coefficients", ctypes.POINTER(ctypes.c_double)), ("is_spherical", ctypes.c_int)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("eri_schwarz_cutoff", ctypes.c_double), ("eri_primitive_pair_cutoff", ctypes.c_double),
+                ("mixed_fp32_cut", ctypes.c_double), ("device", ctypes.c_int), ("deterministic", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("build_ms", ctypes.c_double), ("eri_ms", ctypes.c_double), ("quartets", ctypes.c_double),
+                ("quartets_fp32", ctypes.c_double), ("prim_quartets", ctypes.c_double),
+                ("flops", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
+                ("kernels", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load_library(path: Optional[str] = None):
+    """Load libtontofock.so (built in-tree by tonto_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise TontoFockError(f"CUDA library missing: {path} (run python -m tonto_b200.build)")
+    L = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    d, i, vp = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+    L.tf_default_options.argtypes = [P(Options)]
+    L.tf_ctx_create.argtypes = [P(_Basis), P(Options), P(vp)]
+    L.tf_set_geometry.argtypes = [vp, P(d)]
+    L.tf_build_jk.argtypes = [vp, P(d), P(d), P(d), i]
+    L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
+    L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
+    L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
+    L.tf_last_stats.argtypes = [vp, P(Stats)]
+    L.tf_n_bf.argtypes = [vp]
+    L.tf_schwarz.argtypes = [vp, P(d)]
+    L.tf_ctx_destroy.argtypes = [vp]
+    L.tf_error_string.argtypes = [i]
+    L.tf_error_string.restype = ctypes.c_char_p
+    L.tf_version.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise TontoFockError(f"tontofock error {rc}: {load_library().tf_error_string(rc).decode()}")
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    _check(load_library().tf_default_options(ctypes.byref(o)))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class FockBuilder:
+    """Direct J/K builder for one molecule on one GPU (C ABI context)."""
+
+    def __init__(self, mol: Molecule, schwarz_cutoff: float = 1e-9, pair_cutoff: float = 1e-6,
+                 device: int = 0, mixed_fp32_cut: float = 1e-6, deterministic: bool = False):
+        L = load_library()
+        self.mol = mol
+        sa, sl, sn, sf, ex, co = mol.flat_arrays()
+        self._arrays = [np.ascontiguousarray(mol.xyz, dtype=np.float64), sa, sl, sn, sf, ex, co]
+        xyz = self._arrays[0]
+        ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))  # noqa: E731
+        self._basis = _Basis(mol.n_atom, _dp(xyz), mol.n_shell, ip(sa), ip(sl), ip(sn), ip(sf), _dp(ex), _dp(co),
+                             int(mol.spherical))
+        self.options = default_options(eri_schwarz_cutoff=schwarz_cutoff, eri_primitive_pair_cutoff=pair_cutoff,
+                                       device=device, mixed_fp32_cut=mixed_fp32_cut,
+                                       deterministic=int(deterministic))
+        h = ctypes.c_void_p()
+        _check(L.tf_ctx_create(ctypes.byref(self._basis), ctypes.byref(self.options), ctypes.byref(h)))
+        self.h = h
+        self.n_bf = L.tf_n_bf(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().tf_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_geometry(self, xyz_bohr: np.ndarray):
+        x = np.ascontiguousarray(xyz_bohr, dtype=np.float64)
+        _check(load_library().tf_set_geometry(self.h, _dp(x)))
+
+    @property
+    def max_I(self) -> np.ndarray:
+        n = self.mol.n_shell * (self.mol.n_shell + 1) // 2
+        out = np.zeros(n)
+        _check(load_library().tf_schwarz(self.h, _dp(out)))
+        return out
+
+    def make_r_JK(self, P: np.ndarray, flags: int = TF_JK_FULL) -> Tuple[np.ndarray, np.ndarray]:
+        """J, K for the symmetric density P (host arrays; Fortran-ordered results)."""
+        n = self.n_bf
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        if Pf.shape != (n, n):
+            raise ValueError(f"P must be {n}x{n}")
+        J = np.empty((n, n), order="F")
+        K = np.empty((n, n), order="F")
+        _check(load_library().tf_build_jk(self.h, _dp(Pf), _dp(J), _dp(K), int(flags)))
+        return J, K
+
+    def make_r_JK_device(self, P, J, K, flags: int = TF_JK_FULL, stream=None):
+        """J, K on device (torch CUDA float64 tensors of shape (n_bf, n_bf)); asynchronous
+        on ``stream`` (a torch.cuda.Stream, default: the current stream)."""
+        import torch
+        for t in (P, J, K):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == self.n_bf ** 2):
+                raise ValueError("device J/K tensors must be contiguous float64 CUDA (n_bf, n_bf)")
+        s = stream if stream is not None else torch.cuda.current_stream(P.device)
+        _check(load_library().tf_build_jk_device(self.h, ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(J.data_ptr()),
+                                                 ctypes.c_void_p(K.data_ptr()), int(flags),
+                                                 ctypes.c_void_p(s.cuda_stream)))
+
+    def make_r_Fock_mx(self, P: np.ndarray, H: np.ndarray) -> np.ndarray:
+        n = self.n_bf
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        Hf = np.asfortranarray(H, dtype=np.float64)
+        F = np.empty((n, n), order="F")
+        _check(load_library().tf_build_fock(self.h, _dp(Pf), _dp(Hf), _dp(F)))
+        return F
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(load_library().tf_last_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
