@@ -97,6 +97,14 @@ typedef struct tf_stats {
   int kernels;                       /* kernel launches issued by the last build */
 } tf_stats;
 
+/* Per quartet-class figures of the last build (one entry per (la lb|lc ld) launch). */
+typedef struct tf_class_stats {
+  int l[4];                          /* la >= lb, lc >= ld, pair class (la lb) >= (lc ld) */
+  double quartets, prim_quartets;    /* contracted and primitive quartets computed */
+  double flops;                      /* algorithmic FLOPs */
+  double ms;                         /* device time of the launch (CUDA events) */
+} tf_class_stats;
+
 typedef struct tf_ctx tf_ctx;
 
 /* Fill *opt with Tonto's defaults (Schwarz 1e-9, pair 1e-6, device 0). */
@@ -108,6 +116,13 @@ int tf_ctx_create(const tf_basis* basis, const tf_options* opt, tf_ctx** ctx);
 
 /* New atom positions ([n_atom][3] bohr): rebuilds pair data and Schwarz bounds. */
 int tf_set_geometry(tf_ctx* ctx, const double* xyz);
+
+/* Restrict this context's builds to shard `index` of `count`: every count-th bra
+ * shell-pair task, as one MPI rank of Tonto's round-robin parallel do
+ * (FooToFortran.java:2762-2783, molecule.fock.foo:1274).  The shards' J and K sum
+ * to the full J and K (the caller reduces them, e.g. one NCCL all-reduce, as
+ * PARALLEL_SYMMETRIC_SUM does at molecule.fock.foo:1355-1357). */
+int tf_set_shard(tf_ctx* ctx, int index, int count);
 
 /* J and K from the symmetric density P (host arrays, column-major n_bf x n_bf).
  * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*. */
@@ -124,8 +139,18 @@ int tf_build_fock(tf_ctx* ctx, const double* P, const double* Hcore, double* F);
  * arrays of ctx[i]'s size.  All contexts must be on the same device. */
 int tf_build_jk_batch(tf_ctx** ctx, int n, const double* const* P, double* const* J, double* const* K, int flags);
 
+/* One-electron integrals in the Tonto basis (column-major n_bf x n_bf): overlap S,
+ * kinetic T and nuclear attraction V for nuclear charges Z[n_atom].  Replaces
+ * MOLECULE.INTS:make_overlap_mx, make_kinetic_energy_mx, make_nuclear_attraction_mx
+ * (foofiles/molecule.ints.foo:34-420); H_core = T + V. */
+int tf_one_electron(tf_ctx* ctx, const double* Z, double* S, double* T, double* V);
+
 /* Statistics of the last build on this context. */
 int tf_last_stats(const tf_ctx* ctx, tf_stats* stats);
+
+/* Copies up to max per-class entries of the last build into out; returns the
+ * number of entries available (no reference counterpart: instrumentation). */
+int tf_last_class_stats(const tf_ctx* ctx, tf_class_stats* out, int max);
 
 /* Number of basis functions of the context (Tonto n_bf). */
 int tf_n_bf(const tf_ctx* ctx);

@@ -50,6 +50,8 @@ def lib():
                                            ctypes.c_int, dp]
         L.oracle_shell_quartet.restype = ctypes.c_int
         L.oracle_jk.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_long, ctypes.c_int]
+        L.oracle_jk_sample.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_long, ctypes.c_int, ctypes.c_long,
+                                       ctypes.c_long]
         L.oracle_counts.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.oracle_spherical_matrix.argtypes = [ctypes.c_int, dp]
         L.oracle_spherical_matrix.restype = ctypes.c_int
@@ -107,6 +109,15 @@ class Oracle:
         K = np.zeros((self.n_bf, self.n_bf), order="F")
         lib().oracle_jk(self.h, _dp(Pf), _dp(J), _dp(K), int(max_ab_pairs), int(n_threads))
         return np.ascontiguousarray(J), np.ascontiguousarray(K)
+
+    def jk_sample(self, P: np.ndarray, stride: int, offset: int = 0, n_threads: int = 0) -> float:
+        """Time the outer loop over ab = offset, offset+stride, ... (seconds)."""
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        J = np.zeros((self.n_bf, self.n_bf), order="F")
+        K = np.zeros((self.n_bf, self.n_bf), order="F")
+        t = time.perf_counter()
+        lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(stride), int(offset))
+        return time.perf_counter() - t
 
     def counts(self, reset: bool = False) -> np.ndarray:
         out = np.zeros(625 * 2)

@@ -559,7 +559,17 @@ int oracle_shell_quartet(OracleCtx* c, int a, int b, int cc, int d, int skip, do
 // make_r_JK_direct (:1235-1363).  P, J, K: column-major n_bf x n_bf.
 // max_ab_pairs < 0: all bra pairs; otherwise only the first max_ab_pairs bra
 // shell pairs (a bounded sample for CPU timing).  n_threads <= 0: all.
+void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long max_ab_pairs, int n_threads,
+                      long ab_stride, long ab_offset);
+
 void oracle_jk(OracleCtx* c, const double* P, double* J, double* K, long max_ab_pairs, int n_threads) {
+  oracle_jk_sample(c, P, J, K, max_ab_pairs, n_threads, 1, 0);
+}
+
+// The outer shell-pair loop restricted to ab = ab_offset, ab_offset + ab_stride, ...
+// (one "rank" of Tonto's round-robin parallel do); used to time a bounded sample.
+void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long max_ab_pairs, int n_threads,
+                      long ab_stride, long ab_offset) {
   Ctx* C = reinterpret_cast<Ctx*>(c);
   const Basis& B = C->B;
   const int n = B.n_bf;
@@ -592,8 +602,8 @@ void oracle_jk(OracleCtx* c, const double* P, double* J, double* K, long max_ab_
     Work W;
     Side s_ab_skip, s_ab_full, s_cd;
     // round-robin over ab, as Tonto's parallel do (FooToFortran.java:2762-2783)
-#pragma omp for schedule(static, 1)
-    for (long ab = 0; ab < nab; ++ab) {
+#pragma omp for schedule(dynamic, 1)
+    for (long ab = ab_offset; ab < nab; ab += ab_stride) {
       if (C->max_I[ab] * IP_max < cutoff) continue;
       const PairData& pab = C->pairs[ab];
       int aa = pab.a, bb = pab.b;

@@ -15,6 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtontofock.so")
+PEAK_LIB = os.path.join(HERE, "libtf_peak.so")
 
 SOURCES = ["tontofock.cu"]
 DEPS = ["tontofock.cu", "tf_device.cuh", "tf_warp.cuh", "rys_tables.inc", os.path.join("..", "..", "include",
@@ -40,7 +41,15 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(os.path.join(CSRC, d)) <= t for d in DEPS)
 
 
+def build_peak(force: bool = False) -> str:
+    src = os.path.join(CSRC, "fp64_peak.cu")
+    if force or not os.path.exists(PEAK_LIB) or os.path.getmtime(src) > os.path.getmtime(PEAK_LIB):
+        subprocess.run([nvcc()] + flags() + ["-o", PEAK_LIB, src], check=True, cwd=CSRC)
+    return PEAK_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_peak(force)
     if not force and up_to_date():
         return LIB
     cmd = [nvcc()] + flags() + ["-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]

@@ -562,6 +562,154 @@ __global__ void k_fock(long long n, const double* __restrict__ H, const double* 
 }
 
 // ---------------------------------------------------------------------------
+// kernel: one-electron integrals S, T, V (Cartesian blocks), one thread per
+// shell pair a >= b.  Overlap and kinetic by the Obara-Saika 1D recurrences,
+// nuclear attraction by Rys quadrature (molecule.ints.foo:34-420 in meaning).
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ void rys_eval_n(double x, double* u, double* w) {
+  double uu[N], ww[N];
+  rys_eval<N>(x, uu, ww);
+#pragma unroll
+  for (int i = 0; i < N; ++i) { u[i] = uu[i]; w[i] = ww[i]; }
+}
+
+__global__ void k_one_electron(int n_shell, int n_atom, const double* __restrict__ xyz, const double* __restrict__ Z,
+                               const int* __restrict__ shell_atom, const int* __restrict__ shell_l,
+                               const int* __restrict__ shell_nprim, const int* __restrict__ shell_poff,
+                               const int* __restrict__ shell_cart, const double* __restrict__ exps,
+                               const double* __restrict__ coefs, int n_cart, double* __restrict__ S,
+                               double* __restrict__ T, double* __restrict__ V) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n_shell * (n_shell + 1) / 2) return;
+  int sa = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
+  while ((long long)sa * (sa + 1) / 2 > t) --sa;
+  while ((long long)(sa + 1) * (sa + 2) / 2 <= t) ++sa;
+  const int sb = (int)(t - (long long)sa * (sa + 1) / 2);
+  const int la = shell_l[sa], lb = shell_l[sb];
+  const int na = ncart(la), nb = ncart(lb);
+  const double* A = xyz + 3 * shell_atom[sa];
+  const double* B = xyz + 3 * shell_atom[sb];
+  const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+  const double r2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+  double s_c[36], t_c[36], v_c[36];
+  for (int i = 0; i < na * nb; ++i) { s_c[i] = 0.0; t_c[i] = 0.0; v_c[i] = 0.0; }
+  constexpr int LD = 6;                    // 1D table edge (l <= 2: i <= 3, j <= 4)
+  const int nroot = (la + lb) / 2 + 1;
+  for (int ia = 0; ia < shell_nprim[sa]; ++ia)
+    for (int ib = 0; ib < shell_nprim[sb]; ++ib) {
+      const double a = exps[shell_poff[sa] + ia], ca = coefs[shell_poff[sa] + ia];
+      const double b = exps[shell_poff[sb] + ib], cb = coefs[shell_poff[sb] + ib];
+      const double z = a + b, oo2z = 0.5 / z;
+      const double Kab = exp(-a * b * r2 / z) * ca * cb;
+      double P[3], PA[3], PB[3];
+      for (int k = 0; k < 3; ++k) { P[k] = (a * A[k] + b * B[k]) / z; PA[k] = P[k] - A[k]; PB[k] = P[k] - B[k]; }
+      double s1[3][LD][LD];
+      for (int d = 0; d < 3; ++d) {
+        s1[d][0][0] = 1.0;
+        for (int i = 0; i <= la + 1; ++i)
+          for (int j = 0; j <= lb + 2; ++j) {
+            if (i == 0 && j == 0) continue;
+            double v;
+            if (i > 0) {
+              v = PA[d] * s1[d][i - 1][j];
+              if (i > 1) v += (i - 1) * oo2z * s1[d][i - 2][j];
+              if (j > 0) v += j * oo2z * s1[d][i - 1][j - 1];
+            } else {
+              v = PB[d] * s1[d][0][j - 1];
+              if (j > 1) v += (j - 1) * oo2z * s1[d][0][j - 2];
+            }
+            s1[d][i][j] = v;
+          }
+      }
+      const double pre = Kab * pow(M_PI / z, 1.5);
+      for (int i = 0; i < na; ++i) {
+        const int g = ncart_upto(la - 1) + i;
+        const int ix = c_comp[0][g], iy = c_comp[1][g], iz = c_comp[2][g];
+        for (int j = 0; j < nb; ++j) {
+          const int h = ncart_upto(lb - 1) + j;
+          const int jx = c_comp[0][h], jy = c_comp[1][h], jz = c_comp[2][h];
+          const double Sx = s1[0][ix][jx], Sy = s1[1][iy][jy], Sz = s1[2][iz][jz];
+          auto kin = [&](int d, int i1, int j1) {
+            double v = -2.0 * b * b * s1[d][i1][j1 + 2] + b * (2 * j1 + 1) * s1[d][i1][j1];
+            if (j1 >= 2) v += -0.5 * j1 * (j1 - 1) * s1[d][i1][j1 - 2];
+            return v;
+          };
+          s_c[i * nb + j] += pre * Sx * Sy * Sz;
+          t_c[i * nb + j] += pre * (kin(0, ix, jx) * Sy * Sz + Sx * kin(1, iy, jy) * Sz + Sx * Sy * kin(2, iz, jz));
+        }
+      }
+      for (int at = 0; at < n_atom; ++at) {
+        const double* C = xyz + 3 * at;
+        const double PC[3] = {P[0] - C[0], P[1] - C[1], P[2] - C[2]};
+        const double x = z * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
+        double u[3], w[3];
+        if (nroot == 1) rys_eval_n<1>(x, u, w);
+        else if (nroot == 2) rys_eval_n<2>(x, u, w);
+        else rys_eval_n<3>(x, u, w);
+        const double pv = -Z[at] * 2.0 * M_PI / z * Kab;
+        for (int r = 0; r < nroot; ++r) {
+          double tab[3][3][3];
+          for (int d = 0; d < 3; ++d) {
+            const double c0 = PA[d] - u[r] * PC[d], bb = (1.0 - u[r]) * oo2z;
+            double g[5], h[5][3];
+            g[0] = 1.0;
+            const int L = la + lb;
+            if (L >= 1) g[1] = c0;
+            for (int e = 1; e < L; ++e) g[e + 1] = c0 * g[e] + e * bb * g[e - 1];
+            for (int e = 0; e <= L; ++e) h[e][0] = g[e];
+            for (int j = 1; j <= lb; ++j)
+              for (int e = 0; e <= L - j; ++e) h[e][j] = h[e + 1][j - 1] + AB[d] * h[e][j - 1];
+            for (int i = 0; i <= la; ++i)
+              for (int j = 0; j <= lb; ++j) tab[d][i][j] = h[i][j];
+          }
+          const double wv = pv * w[r];
+          for (int i = 0; i < na; ++i) {
+            const int g2 = ncart_upto(la - 1) + i;
+            for (int j = 0; j < nb; ++j) {
+              const int h2 = ncart_upto(lb - 1) + j;
+              v_c[i * nb + j] += wv * tab[0][c_comp[0][g2]][c_comp[0][h2]] * tab[1][c_comp[1][g2]][c_comp[1][h2]] * tab[2][c_comp[2][g2]][c_comp[2][h2]];
+            }
+          }
+        }
+      }
+    }
+  const int oa = shell_cart[sa], ob = shell_cart[sb];
+  for (int i = 0; i < na; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const size_t p = (size_t)(oa + i) * n_cart + ob + j, q = (size_t)(ob + j) * n_cart + oa + i;
+      S[p] = S[q] = s_c[i * nb + j];
+      T[p] = T[q] = t_c[i * nb + j];
+      V[p] = V[q] = v_c[i * nb + j];
+    }
+}
+
+// Cartesian symmetric matrix -> Tonto basis (column-major), no folding.
+__global__ void k_cart_to_basis(int n_bf, int n_cart, const double* __restrict__ Xc, const int* __restrict__ bf_shell,
+                                const int* __restrict__ bf_local, const int* __restrict__ shell_l,
+                                const int* __restrict__ shell_cart, int spherical, double* __restrict__ X) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n_bf * n_bf) return;
+  const int j = (int)(t / n_bf), i = (int)(t % n_bf);
+  const int si = bf_shell[i], sj = bf_shell[j], mi = bf_local[i], mj = bf_local[j];
+  const int li = shell_l[si], lj = shell_l[sj], ci = shell_cart[si], cj = shell_cart[sj];
+  const bool ti = spherical && li >= 2, tj = spherical && lj >= 2;
+  const int ni = ti ? ncart(li) : 1, nj = tj ? ncart(lj) : 1;
+  double s = 0.0;
+  for (int p = 0; p < ni; ++p) {
+    const double up = ti ? c_U[li][p * (2 * li + 1) + mi] : 1.0;
+    if (up == 0.0) continue;
+    const int cp = ti ? ci + p : ci + mi;
+    for (int q = 0; q < nj; ++q) {
+      const double uq = tj ? c_U[lj][q * (2 * lj + 1) + mj] : 1.0;
+      if (uq == 0.0) continue;
+      s += up * uq * Xc[(size_t)cp * n_cart + (tj ? cj + q : cj + mj)];
+    }
+  }
+  X[(size_t)j * n_bf + i] = s;
+}
+
+// ---------------------------------------------------------------------------
 // host: spherical matrices (Helgaker-Jorgensen-Olsen real solid harmonics,
 // the recurrence of gaussian_data.foo:1143-1290; columns m = 0,+1,-1,+2,...)
 // ---------------------------------------------------------------------------
@@ -646,10 +794,11 @@ struct tf_ctx {
   std::vector<int4> cps;                          // class pairs
   std::vector<int> cp_first_task;                 // first task of each class pair
   long long n_tasks = 0;
+  int shard_index = 0, shard_count = 1;           // round-robin share of the bra tasks
   bool geometry_ready = false;
   // device
   tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax;
-  tf::DBuf<int> d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
+  tf::DBuf<int> d_shell_atom, d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
   tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_cls_n, d_schwarz_ids;
   tf::DBuf<long long> d_counts;
   tf::DBuf<tf::PairRec> d_pairs;
@@ -659,6 +808,8 @@ struct tf_ctx {
   tf::DBuf<long long> d_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
   tf::DBuf<unsigned char> d_scan_tmp;
+  std::vector<cudaEvent_t> cls_ev;                // one per class-pair launch boundary
+  std::vector<tf_class_stats> cls_stats;
   std::vector<double> max_I_tonto;                // per Tonto pair index
   tf_stats stats{};
 };
@@ -667,6 +818,36 @@ namespace tf {
 
 static int set_device(tf_ctx* c) {
   TF_CUDA(cudaSetDevice(c->device));
+  return TF_OK;
+}
+
+// Class pairs and bra tasks (class pair, bra position); with sharding, this
+// context keeps every shard_count-th task (Tonto's round-robin parallel do).
+static int build_tasks(tf_ctx* c) {
+  c->cps.clear();
+  c->cp_first_task.clear();
+  std::vector<int2> tasks;
+  long long g = 0;
+  for (int p1 = 0; p1 < NPAIRCLS; ++p1)
+    for (int p2 = 0; p2 <= p1; ++p2) {
+      if (c->cls_n[p1] == 0 || c->cls_n[p2] == 0) continue;
+      const int cpi = (int)c->cps.size();
+      c->cps.push_back(make_int4(p1, p2, c->cls_off[p1], c->cls_off[p2]));
+      c->cp_first_task.push_back((int)tasks.size());
+      for (int i = 0; i < c->cls_n[p1]; ++i, ++g)
+        if (g % c->shard_count == c->shard_index) tasks.push_back(make_int2(cpi, i));
+    }
+  c->cp_first_task.push_back((int)tasks.size());
+  c->n_tasks = (long long)tasks.size();
+  TF_CUDA(c->d_cps.reserve(std::max<size_t>(c->cps.size(), 1)));
+  TF_CUDA(c->d_tasks.reserve(std::max<size_t>(tasks.size(), 1)));
+  TF_CUDA(c->d_counts.reserve(tasks.size() + 1));
+  TF_CUDA(c->d_offsets.reserve(tasks.size() + 1));
+  if (!c->cps.empty())
+    TF_CUDA(cudaMemcpyAsync(c->d_cps.p, c->cps.data(), c->cps.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+  if (!tasks.empty())
+    TF_CUDA(cudaMemcpyAsync(c->d_tasks.p, tasks.data(), tasks.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA(cudaStreamSynchronize(c->stream));
   return TF_OK;
 }
 
@@ -760,27 +941,9 @@ static int setup_pairs(tf_ctx* c) {
   TF_CUDA(cudaMemcpyAsync(c->d_sorted_imax.p, simax.data(), simax.size() * sizeof(double), cudaMemcpyHostToDevice,
                           c->stream));
   TF_CUDA(cudaMemcpyAsync(c->d_cls_n.p, c->cls_n.data(), NPAIRCLS * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  // class pairs and bra tasks
-  c->cps.clear();
-  c->cp_first_task.clear();
-  std::vector<int2> tasks;
-  for (int p1 = 0; p1 < NPAIRCLS; ++p1)
-    for (int p2 = 0; p2 <= p1; ++p2) {
-      if (c->cls_n[p1] == 0 || c->cls_n[p2] == 0) continue;
-      const int cpi = (int)c->cps.size();
-      c->cps.push_back(make_int4(p1, p2, c->cls_off[p1], c->cls_off[p2]));
-      c->cp_first_task.push_back((int)tasks.size());
-      for (int i = 0; i < c->cls_n[p1]; ++i) tasks.push_back(make_int2(cpi, i));
-    }
-  c->cp_first_task.push_back((int)tasks.size());
-  c->n_tasks = (long long)tasks.size();
-  TF_CUDA(c->d_cps.reserve(c->cps.size()));
-  TF_CUDA(c->d_tasks.reserve(tasks.size()));
-  TF_CUDA(c->d_counts.reserve(tasks.size() + 1));
-  TF_CUDA(c->d_offsets.reserve(tasks.size() + 1));
-  TF_CUDA(cudaMemcpyAsync(c->d_cps.p, c->cps.data(), c->cps.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
-  TF_CUDA(cudaMemcpyAsync(c->d_tasks.p, tasks.data(), tasks.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(cudaStreamSynchronize(c->stream));
+  int rc = build_tasks(c);
+  if (rc) return rc;
   c->geometry_ready = true;
   return TF_OK;
 }
@@ -865,7 +1028,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   ListArgs la{c->d_tasks.p, c->n_tasks, c->d_cps.p, c->d_cls_n.p, c->d_sorted.p, c->d_sorted_imax.p, c->d_pairs.p,
               c->d_pmax.p, c->d_pglob.p, ns, c->opt.eri_schwarz_cutoff};
   const long long thr_list = 256;
-  const unsigned grid_list = (unsigned)((c->n_tasks * 32 + thr_list - 1) / thr_list);
+  const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   k_quartets<false><<<grid_list, (unsigned)thr_list, 0, s>>>(la, c->d_counts.p, nullptr, nullptr);
   kernels++;
   size_t tmp_bytes = 0;
@@ -890,6 +1053,12 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   TF_CUDA(cudaEventRecord(c->ev1, s));
   double flops = 0.0;
   std::vector<long long> cp_n(c->cps.size());
+  while (c->cls_ev.size() < c->cps.size() + 1) {
+    cudaEvent_t e;
+    TF_CUDA(cudaEventCreate(&e));
+    c->cls_ev.push_back(e);
+  }
+  TF_CUDA(cudaEventRecord(c->cls_ev[0], s));
   for (size_t k = 0; k < c->cps.size(); ++k) {
     const int4 cp = c->cps[k];
     int l1h, l1l, l2h, l2l;
@@ -898,10 +1067,12 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     JKArgs a{c->d_quartets.p + cp_off[k], cp_off[k + 1] - cp_off[k], c->d_pairs.p, c->d_prim_full.p,
              c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, nc, c->d_prim_count.p};
     cp_n[k] = a.n;
-    if (a.n == 0) continue;
-    int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s);
-    if (rc != TF_OK) return rc;
-    kernels++;
+    if (a.n > 0) {
+      int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s);
+      if (rc != TF_OK) return rc;
+      kernels++;
+    }
+    TF_CUDA(cudaEventRecord(c->cls_ev[k + 1], s));
   }
   TF_CUDA(cudaGetLastError());
   TF_CUDA(cudaEventRecord(c->ev2, s));
@@ -921,6 +1092,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   TF_CUDA(cudaEventElapsedTime(&ms_eri, c->ev1, c->ev2));
   TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
   double npq = 0.0;
+  c->cls_stats.clear();
   for (size_t k = 0; k < c->cps.size(); ++k) {
     const int4 cp = c->cps[k];
     int l1h, l1l, l2h, l2l;
@@ -928,7 +1100,17 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     class_l(cp.y, l2h, l2l);
     const double p = (double)pc[qclass_id(l1h, l1l, l2h, l2l)];
     npq += p;
-    flops += class_flops(l1h, l1l, l2h, l2l, (double)cp_n[k], p);
+    const double fl = class_flops(l1h, l1l, l2h, l2l, (double)cp_n[k], p);
+    flops += fl;
+    float ms = 0.f;
+    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[k], c->cls_ev[k + 1]));
+    tf_class_stats cs;
+    cs.l[0] = l1h; cs.l[1] = l1l; cs.l[2] = l2h; cs.l[3] = l2l;
+    cs.quartets = (double)cp_n[k];
+    cs.prim_quartets = p;
+    cs.flops = fl;
+    cs.ms = ms;
+    c->cls_stats.push_back(cs);
   }
   c->stats.build_ms = ms_all;
   c->stats.eri_ms = ms_eri;
@@ -1052,6 +1234,7 @@ int tf_ctx_create(const tf_basis* B, const tf_options* opt, tf_ctx** out) {
   TF_TRY(up(c->d_exps, c->exps));
   TF_TRY(up(c->d_coefs, c->coefs));
   TF_TRY(up(c->d_shell_nprim, c->shell_nprim));
+  TF_TRY(up(c->d_shell_atom, c->shell_atom));
   TF_TRY(up(c->d_shell_poff, c->shell_poff));
   TF_TRY(up(c->d_shell_l, c->shell_l));
   TF_TRY(up(c->d_shell_first_bf, c->shell_first_bf));
@@ -1082,6 +1265,16 @@ int tf_set_geometry(tf_ctx* c, const double* xyz) {
   TF_CUDA(cudaMemcpy(c->d_xyz.p, c->xyz.data(), c->xyz.size() * sizeof(double), cudaMemcpyHostToDevice));
   c->geometry_ready = false;
   return setup_pairs(c);
+}
+
+int tf_set_shard(tf_ctx* c, int index, int count) {
+  using namespace tf;
+  if (!c || count < 1 || index < 0 || index >= count) { set_error("bad shard"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  c->shard_index = index;
+  c->shard_count = count;
+  return c->geometry_ready ? build_tasks(c) : TF_OK;
 }
 
 int tf_build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, void* stream) {
@@ -1150,10 +1343,50 @@ int tf_build_jk_batch(tf_ctx** ctx, int n, const double* const* P, double* const
   return TF_OK;
 }
 
+int tf_one_electron(tf_ctx* c, const double* Z, double* S, double* T, double* V) {
+  using namespace tf;
+  if (!c || !Z || !S || !T || !V) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  const int nc = c->n_cart, nb = c->n_bf;
+  DBuf<double> dZ, dS, dT, dV;
+  TF_CUDA(dZ.reserve(c->n_atom));
+  TF_CUDA(cudaMemcpyAsync(dZ.p, Z, c->n_atom * sizeof(double), cudaMemcpyHostToDevice, s));
+  // Cartesian blocks into the (reused) Cartesian accumulators, then to the basis
+  double* Sc = c->d_Jc.p;
+  double* Tc = c->d_Kc.p;
+  double* Vc = c->d_Pc.p;
+  const long long npair = (long long)c->n_shell * (c->n_shell + 1) / 2;
+  k_one_electron<<<(unsigned)((npair + 127) / 128), 128, 0, s>>>(
+      c->n_shell, c->n_atom, c->d_xyz.p, dZ.p, c->d_shell_atom.p, c->d_shell_l.p, c->d_shell_nprim.p,
+      c->d_shell_poff.p, c->d_shell_cart.p, c->d_exps.p, c->d_coefs.p, nc, Sc, Tc, Vc);
+  TF_CUDA(cudaGetLastError());
+  const long long n2 = (long long)nb * nb;
+  double* outs[3] = {S, T, V};
+  double* ins[3] = {Sc, Tc, Vc};
+  for (int k = 0; k < 3; ++k) {
+    k_cart_to_basis<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, ins[k], c->d_bf_shell.p, c->d_bf_local.p,
+                                                                 c->d_shell_l.p, c->d_shell_cart.p, c->spherical,
+                                                                 c->d_J.p);
+    TF_CUDA(cudaMemcpyAsync(outs[k], c->d_J.p, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    TF_CUDA(cudaStreamSynchronize(s));
+  }
+  TF_CUDA(cudaGetLastError());
+  return TF_OK;
+}
+
 int tf_last_stats(const tf_ctx* c, tf_stats* s) {
   if (!c || !s) return TF_EINVAL;
   *s = c->stats;
   return TF_OK;
+}
+
+int tf_last_class_stats(const tf_ctx* c, tf_class_stats* out, int max) {
+  if (!c || (!out && max > 0)) return TF_EINVAL;
+  const int n = (int)c->cls_stats.size();
+  for (int i = 0; i < n && i < max; ++i) out[i] = c->cls_stats[i];
+  return n;
 }
 
 int tf_n_bf(const tf_ctx* c) { return c ? c->n_bf : TF_EINVAL; }
@@ -1171,6 +1404,7 @@ void tf_ctx_destroy(tf_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
+  for (cudaEvent_t e : c->cls_ev) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -57,6 +57,11 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ClassStats(ctypes.Structure):
+    _fields_ = [("l", ctypes.c_int * 4), ("quartets", ctypes.c_double), ("prim_quartets", ctypes.c_double),
+                ("flops", ctypes.c_double), ("ms", ctypes.c_double)]
+
+
 _lib = None
 
 
@@ -75,10 +80,13 @@ def load_library(path: Optional[str] = None):
     L.tf_ctx_create.argtypes = [P(_Basis), P(Options), P(vp)]
     L.tf_set_geometry.argtypes = [vp, P(d)]
     L.tf_build_jk.argtypes = [vp, P(d), P(d), P(d), i]
+    L.tf_set_shard.argtypes = [vp, i, i]
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
     L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
+    L.tf_one_electron.argtypes = [vp, P(d), P(d), P(d), P(d)]
     L.tf_last_stats.argtypes = [vp, P(Stats)]
+    L.tf_last_class_stats.argtypes = [vp, P(ClassStats), i]
     L.tf_n_bf.argtypes = [vp]
     L.tf_schwarz.argtypes = [vp, P(d)]
     L.tf_ctx_destroy.argtypes = [vp]
@@ -142,6 +150,11 @@ class FockBuilder:
         x = np.ascontiguousarray(xyz_bohr, dtype=np.float64)
         _check(load_library().tf_set_geometry(self.h, _dp(x)))
 
+    def set_shard(self, index: int, count: int):
+        """Build only shard ``index`` of ``count`` (round-robin bra tasks); the shards'
+        J and K sum to the full build."""
+        _check(load_library().tf_set_shard(self.h, int(index), int(count)))
+
     @property
     def max_I(self) -> np.ndarray:
         n = self.mol.n_shell * (self.mol.n_shell + 1) // 2
@@ -179,6 +192,31 @@ class FockBuilder:
         F = np.empty((n, n), order="F")
         _check(load_library().tf_build_fock(self.h, _dp(Pf), _dp(Hf), _dp(F)))
         return F
+
+    def class_stats(self) -> list:
+        """Per-class (la lb|lc ld) figures of the last build."""
+        L = load_library()
+        n = L.tf_last_class_stats(self.h, None, 0)
+        arr = (ClassStats * max(n, 1))()
+        L.tf_last_class_stats(self.h, arr, n)
+        sym = "spdfg"
+        out = []
+        for c in arr[:n]:
+            name = "(%s%s|%s%s)" % tuple(sym[v] for v in c.l)
+            out.append({"class": name, "quartets": c.quartets, "prim_quartets": c.prim_quartets,
+                        "flops": c.flops, "ms": c.ms})
+        return out
+
+    def one_electron(self):
+        """S, T, V in the Tonto basis (make_overlap_mx, make_kinetic_energy_mx,
+        make_nuclear_attraction_mx)."""
+        n = self.n_bf
+        Z = np.ascontiguousarray(self.mol.Z, dtype=np.float64)
+        S = np.empty((n, n), order="F")
+        T = np.empty((n, n), order="F")
+        V = np.empty((n, n), order="F")
+        _check(load_library().tf_one_electron(self.h, _dp(Z), _dp(S), _dp(T), _dp(V)))
+        return S, T, V
 
     def stats(self) -> dict:
         s = Stats()

@@ -1,0 +1,194 @@
+"""Restricted Hartree-Fock SCF driver on the GPU around the J/K builder.
+
+Host-side mirror of Tonto's ``MOLECULE.SCF:usual_SCF`` (molecule.scf.foo:1690-1727):
+
+    initialize_SCF   overlap, core Hamiltonian, initial density (core guess,
+                     make_core_mx_guess_MOs :4723, or a caller-supplied one)
+    loop             extrapolate_Fock_mx (DIIS on the commutator FPS - SPF, keep 8,
+                     :6717-6890) -> update_MOs (diagonalise in the S^-1/2 basis,
+                     MO_r_eigen_update :3797) -> make_SCF_density_mx
+                     (molecule.base.foo:318) -> make_scf_Fock_mx (:1562, the J/K
+                     build through the C ABI) -> energy and convergence
+                     (scf_data.foo:2283-2310: |delta E| and the DIIS error both below
+                     their tolerances)
+
+The J/K build runs on the device arrays (``tf_build_jk_device``); diagonalisation
+and DIIS use torch (cuSOLVER) on the same GPU and stream, so nothing returns to
+the host except two scalars per cycle.
+
+Optional modes (none changes the converged answer):
+* ``mixed``: quartets below the Schwarz x density cut in FP32 (FP64 roots,
+  weights and accumulation); the last ``fp64_final`` cycles rebuilt in FP64;
+* ``incremental``: Fock builds from the density change (F_n = F_{n-1} + G[dP]),
+  with a full rebuild every ``rebuild_every`` cycles and in the final cycles.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
+
+import numpy as np
+import torch
+
+from .basis import Molecule
+from .fock import TF_JK_DELTA, TF_JK_FULL, TF_JK_MIXED, FockBuilder
+
+
+@dataclass
+class SCFResult:
+    energy: float
+    converged: bool
+    iterations: int
+    builds: int
+    seconds: float
+    build_seconds: float
+    P: torch.Tensor
+    history: List[tuple] = field(default_factory=list)
+    guess: str = "core"
+    fell_back: bool = False
+
+
+class DIIS:
+    """Pulay DIIS on the commutator error (Tonto's DIIS, keep 8)."""
+
+    def __init__(self, keep: int = 8):
+        self.keep = keep
+        self.F: List[torch.Tensor] = []
+        self.E: List[torch.Tensor] = []
+
+    def reset(self):
+        self.F.clear()
+        self.E.clear()
+
+    def extrapolate(self, F: torch.Tensor, err: torch.Tensor) -> torch.Tensor:
+        self.F.append(F.clone())
+        self.E.append(err.clone())
+        if len(self.F) > self.keep:
+            self.F.pop(0)
+            self.E.pop(0)
+        m = len(self.F)
+        if m < 2:
+            return F
+        Es = torch.stack([e.reshape(-1) for e in self.E])
+        B = torch.zeros((m + 1, m + 1), dtype=F.dtype, device=F.device)
+        B[:m, :m] = Es @ Es.T
+        B[m, :m] = -1.0
+        B[:m, m] = -1.0
+        rhs = torch.zeros(m + 1, dtype=F.dtype, device=F.device)
+        rhs[m] = -1.0
+        c = torch.linalg.solve(B, rhs)[:m]
+        return torch.einsum("i,ijk->jk", c, torch.stack(self.F))
+
+
+class RHF:
+    def __init__(self, mol: Molecule, schwarz_cutoff: float = 1e-12, device: int = 0, diis_keep: int = 8,
+                 mixed_fp32_cut: float = 1e-6, builder: Optional[FockBuilder] = None):
+        self.mol = mol
+        self.dev = torch.device("cuda", device)
+        self.fb = builder or FockBuilder(mol, schwarz_cutoff=schwarz_cutoff, device=device,
+                                         mixed_fp32_cut=mixed_fp32_cut)
+        S, T, V = self.fb.one_electron()
+        self.S = torch.tensor(np.ascontiguousarray(S), dtype=torch.float64, device=self.dev)
+        self.T = torch.tensor(np.ascontiguousarray(T), dtype=torch.float64, device=self.dev)
+        self.V = torch.tensor(np.ascontiguousarray(V), dtype=torch.float64, device=self.dev)
+        self.H = self.T + self.V
+        e, U = torch.linalg.eigh(self.S)
+        self.X = (U / torch.sqrt(e)) @ U.T
+        self.n_occ = mol.n_electrons // 2
+        self.e_nuc = mol.nuclear_repulsion()
+        self.diis_keep = diis_keep
+        n = mol.n_bf
+        self._J = torch.empty((n, n), dtype=torch.float64, device=self.dev)
+        self._K = torch.empty((n, n), dtype=torch.float64, device=self.dev)
+
+    def density(self, F: torch.Tensor):
+        e, C = torch.linalg.eigh(self.X.T @ F @ self.X)
+        C = self.X @ C
+        Co = C[:, : self.n_occ]
+        return 2.0 * Co @ Co.T, e, C
+
+    def core_guess(self) -> torch.Tensor:
+        return self.density(self.H)[0]
+
+    def jk(self, P: torch.Tensor, flags: int = TF_JK_FULL):
+        Pc = P.contiguous()
+        self.fb.make_r_JK_device(Pc, self._J, self._K, flags)
+        return self._J, self._K
+
+    def run(self, P0: Optional[torch.Tensor] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
+            max_iter: int = 100, mixed: bool = False, fp64_final: int = 2, incremental: bool = False,
+            rebuild_every: int = 8, guess_name: str = "core",
+            fallback: Optional[Callable[[], torch.Tensor]] = None, fallback_after: int = 3,
+            verbose: bool = False) -> SCFResult:
+        torch.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        P = self.core_guess() if P0 is None else P0.to(self.dev, torch.float64).contiguous()
+        diis = DIIS(self.diis_keep)
+        hist = []
+        builds = 0
+        build_s = 0.0
+        E_old = None
+        F_prev = None
+        P_prev = None
+        fell_back = False
+        err_first = None
+        it = 0
+        converged = False
+        fp64_left = None          # cycles still to run in FP64 at the end
+        since_full = 0
+        while True:
+            # Fock build: mixed precision until close, incremental when allowed
+            near = E_old is not None and len(hist) >= 2 and abs(hist[-1][2]) < 1e3 * conv
+            use_mixed = mixed and not near and fp64_left is None
+            flags = TF_JK_MIXED if use_mixed else TF_JK_FULL
+            tb = time.perf_counter()
+            if incremental and F_prev is not None and since_full < rebuild_every and not near:
+                dP = (P - P_prev).contiguous()
+                J, K = self.jk(dP, flags | TF_JK_DELTA)
+                F = F_prev + J - 0.5 * K
+                since_full += 1
+            else:
+                J, K = self.jk(P, flags)
+                F = self.H + J - 0.5 * K
+                since_full = 0
+            builds += 1
+            E_t = 0.5 * torch.sum(P * (self.H + F)) + self.e_nuc
+            err = F @ P @ self.S - self.S @ P @ F
+            err_n_t = torch.linalg.norm(err)
+            E, err_n = float(E_t), float(err_n_t)            # the per-cycle host sync
+            build_s += time.perf_counter() - tb
+            dE = float("inf") if E_old is None else E - E_old
+            hist.append((it, E, dE, err_n, "mixed" if use_mixed else "fp64"))
+            if verbose:
+                print(f"scf {it:3d} E={E:.12f} dE={dE:.3e} err={err_n:.3e} {hist[-1][4]}")
+            if err_first is None:
+                err_first = err_n
+            # learned-guess fallback: DIIS error not falling within the first cycles
+            if fallback is not None and not fell_back and it == fallback_after and err_n >= err_first:
+                P = fallback().to(self.dev, torch.float64).contiguous()
+                diis.reset()
+                fell_back = True
+                E_old = None
+                F_prev = None
+                it += 1
+                continue
+            done = E_old is not None and abs(dE) < conv and err_n < diis_tol
+            if done and mixed and hist[-1][4] != "fp64":
+                done = False                                   # final answer must come from FP64 builds
+            if done and mixed:
+                n64 = sum(1 for h in hist[-fp64_final:] if h[4] == "fp64")
+                done = n64 >= min(fp64_final, len(hist))
+            if done or it >= max_iter:
+                converged = done
+                break
+            E_old = E
+            F_prev, P_prev = F, P
+            Fx = diis.extrapolate(F, err)
+            P, _, _ = self.density(Fx)
+            it += 1
+        torch.cuda.synchronize(self.dev)
+        return SCFResult(energy=E, converged=converged, iterations=it, builds=builds,
+                         seconds=time.perf_counter() - t0, build_seconds=build_s, P=P, history=hist,
+                         guess=guess_name, fell_back=fell_back)
