@@ -95,3 +95,37 @@ def test_fock_matches_j_minus_half_k(cuda_ok, oracle_mod):
     F = fb.make_r_Fock_mx(P, H)
     Jr, Kr = orc.jk(P)
     assert np.max(np.abs(F - (H + Jr - 0.5 * Kr))) <= TOL
+
+
+@pytest.mark.gpu
+def test_mixed_precision_build_error_is_bounded(cuda_ok, oracle_mod):
+    """TF_JK_MIXED: quartets with Schwarz x density bound < 1e-6 in FP32 (FP64 roots,
+    weights, transfers and accumulation).  Each FP32 quartet contributes at most ~1e-6
+    with a relative error ~1e-6, so J and K stay within 1e-9 of the FP64 oracle."""
+    from tonto_b200.fock import FockBuilder, TF_JK_MIXED
+    mol = water_cluster(4, seed=0)
+    orc = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
+    P = core_density(orc, oracle_mod, mol)
+    Jr, Kr = orc.jk(P)
+    fb = FockBuilder(mol, schwarz_cutoff=1e-12, mixed_fp32_cut=1e-6)
+    J, K = fb.make_r_JK(P, TF_JK_MIXED)
+    st = fb.stats()
+    assert st["quartets_fp32"] > 0.3 * st["quartets"]
+    assert np.max(np.abs(J - Jr)) < 1e-9 and np.max(np.abs(K - Kr)) < 1e-9
+
+
+@pytest.mark.gpu
+def test_delta_build_is_linear(cuda_ok, oracle_mod):
+    """TF_JK_DELTA: J, K of a density difference; G[P1] = G[P0] + G[P1 - P0]."""
+    from tonto_b200.fock import FockBuilder, TF_JK_DELTA
+    mol = water_cluster(2, seed=8)
+    orc = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
+    P0 = core_density(orc, oracle_mod, mol)
+    rng = np.random.default_rng(2)
+    A = rng.normal(size=P0.shape) * 1e-3
+    P1 = P0 + A + A.T
+    fb = FockBuilder(mol, schwarz_cutoff=1e-12)
+    J0, K0 = fb.make_r_JK(P0)
+    dJ, dK = fb.make_r_JK(P1 - P0, TF_JK_DELTA)
+    J1r, K1r = orc.jk(P1)
+    assert np.max(np.abs(J0 + dJ - J1r)) < 1e-10 and np.max(np.abs(K0 + dK - K1r)) < 1e-10

@@ -157,6 +157,45 @@ __device__ __forceinline__ void rys_eval(double x, double (&u)[N], double (&w)[N
   }
 }
 
+// The same tables staged in shared memory, transposed to [coef][function][interval]
+// so that lanes evaluating different intervals hit different banks.
+template <int N>
+struct RysSmem {
+  static constexpr int NI = rys_xmax(N);              // intervals
+  static constexpr int SIZE = TF_RYS_NCOEF * 2 * N * NI;
+  static __device__ __forceinline__ void load(double* t) {
+    constexpr int OFF = rys_offset(N);
+    for (int q = threadIdx.x; q < SIZE; q += blockDim.x) {
+      // q = (k * 2N + f) * NI + j
+      const int j = q % NI, kf = q / NI, f = kf % (2 * N), k = kf / (2 * N);
+      t[q] = tf_rys_coef[OFF + j * (2 * N * TF_RYS_NCOEF) + f * TF_RYS_NCOEF + k];
+    }
+  }
+  static __device__ __forceinline__ void eval(const double* __restrict__ t, double x, double (&u)[N], double (&w)[N]) {
+    if (x < (double)NI) {
+      const int j = (int)x;
+      const double s = x - (double)j;
+      const double* c = t + j;
+#pragma unroll
+      for (int f = 0; f < 2 * N; ++f) {
+        double v = c[(TF_RYS_DEG * 2 * N + f) * NI];
+#pragma unroll
+        for (int k = TF_RYS_DEG - 1; k >= 0; --k) v = fma(v, s, c[(k * 2 * N + f) * NI]);
+        if (f < N) u[f] = v; else w[f - N] = v;
+      }
+    } else {
+      constexpr int HOFF = rys_hoffset(N);
+      const double ix = 1.0 / x;
+      const double isx = sqrt(ix);
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        u[i] = tf_rys_hroot2[HOFF + i] * ix;
+        w[i] = tf_rys_hweight[HOFF + i] * isx;
+      }
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // One contracted shell quartet (LA LB | LC LD), LA >= LB, LC >= LD, in
 // arithmetic type T for the 2D recurrences and (e0|f0) sums (double, or float
@@ -183,7 +222,8 @@ __device__ __forceinline__ double4 ld4(const PrimPair* p, int half) {
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp, int nbp,
                                                 const PrimPair* __restrict__ kp, int nkp,
-                                                T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF]) {
+                                                T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
+                                                const double* __restrict__ rys_smem = nullptr) {
   using Q = Quartet<LA, LB, LC, LD>;
   constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
 #pragma unroll
@@ -206,7 +246,8 @@ __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp,
       const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
       const double xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
       double u[NR], w[NR];
-      rys_eval<NR>(xx, u, w);
+      if (rys_smem) RysSmem<NR>::eval(rys_smem, xx, u, w);
+      else rys_eval<NR>(xx, u, w);
       const double scale = bcc * kcc * sqrt(rho);
       const double r_z = eta * inv;     // rho / zeta
       const double r_e = zeta * inv;    // rho / eta
@@ -360,10 +401,11 @@ __device__ __forceinline__ void hrr_bra(const T (&G)[CT.first[LA + LB + 1] - CT.
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void quartet_integrals(const PrimPair* bp, int nbp, const PrimPair* kp, int nkp,
                                                   const double* Rab, const double* Rcd,
-                                                  double (&abcd)[ncart(LA)][ncart(LB)][ncart(LC) * ncart(LD)]) {
+                                                  double (&abcd)[ncart(LA)][ncart(LB)][ncart(LC) * ncart(LD)],
+                                                  const double* __restrict__ rys_smem = nullptr) {
   using Q = Quartet<LA, LB, LC, LD>;
   T esfs[Q::NE][Q::NF];
-  accumulate_esfs<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, esfs);
+  accumulate_esfs<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, esfs, rys_smem);
   double ed[Q::NE][Q::NF];
 #pragma unroll
   for (int e = 0; e < Q::NE; ++e)

@@ -17,6 +17,7 @@
 //                      back to the Tonto basis
 #include "tf_device.cuh"
 #include "tf_warp.cuh"
+#include "tf_group.cuh"
 #include "../../include/tontofock.h"
 
 #include <cub/cub.cuh>
@@ -197,10 +198,14 @@ __global__ void k_pmax(int n_shell, int n_bf, const double* __restrict__ P, cons
 // ---------------------------------------------------------------------------
 // kernels: quartet lists
 // ---------------------------------------------------------------------------
+constexpr int NCOST = 13;                  // log2 buckets of the primitive-quartet count
+constexpr int NBUCKET = 2 * NCOST;         // FP64 buckets, then FP32 buckets
+
 struct ListArgs {
   const int2* tasks;            // (class pair, bra position)
   long long n_tasks;
   const int4* cp;               // class pair: (bra class, ket class, bra list offset, ket list offset)
+  const int* cp_task0;          // first task of each class pair
   const int* cls_n;             // pairs per class
   const int* sorted;            // pair ids, grouped by class, I_max descending
   const double* sorted_imax;
@@ -209,18 +214,34 @@ struct ListArgs {
   const unsigned long long* pglob;
   int n_shell;
   double cutoff;
+  double fp32_cut;              // 0: no FP32 quartets
 };
 
-__device__ __forceinline__ bool quartet_survives(const ListArgs& a, const PairRec& b, const PairRec& k, double Ib,
-                                                 double Ik) {
+__device__ __forceinline__ double quartet_bound(const ListArgs& a, const PairRec& b, const PairRec& k, double Ib,
+                                                double Ik) {
   const double* pm = a.pmax;
   const int ns = a.n_shell;
   const int sa = b.sh_hi, sb = b.sh_lo, sc = k.sh_hi, sd = k.sh_lo;
   double m = fmax(pm[sa * ns + sb], pm[sc * ns + sd]);
   m = fmax(m, fmax(pm[sa * ns + sc], pm[sa * ns + sd]));
   m = fmax(m, fmax(pm[sb * ns + sc], pm[sb * ns + sd]));
-  if (m < 1.0e-20) return false;                 // TOL(20)
-  return m * Ib * Ik > a.cutoff;
+  if (m < 1.0e-20) return -1.0;                 // TOL(20): skipped
+  return m * Ib * Ik;
+}
+
+__device__ __forceinline__ int cost_bucket(const PairRec& b, const PairRec& k) {
+  const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
+                        b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
+  const int npq = any_same ? b.n_full * k.n_full : b.n_skip * k.n_skip;
+  const int lg = npq > 0 ? 31 - __clz(npq) : 0;
+  return lg < NCOST ? lg : NCOST - 1;
+}
+
+// Index of (task, bucket) in the count/offset arrays: class pair, then bucket,
+// then task -> each class pair's list is bucket-sorted and deterministic.
+__device__ __forceinline__ long long slot(const ListArgs& a, long long t, int cpi, int bucket) {
+  const long long t0 = a.cp_task0[cpi], nt = a.cp_task0[cpi + 1] - t0;
+  return t0 * NBUCKET + (long long)bucket * nt + (t - t0);
 }
 
 template <bool WRITE>
@@ -237,27 +258,37 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
   const PairRec b = a.pairs[bra];
   const int jend = (cp.x == cp.y) ? i + 1 : a.cls_n[cp.y];
   const double pg = __longlong_as_double((long long)*a.pglob);
-  long long base = WRITE ? offsets[t] : 0;
-  int cnt = 0;
+  int cnt[NBUCKET];
+#pragma unroll
+  for (int k = 0; k < NBUCKET; ++k) cnt[k] = 0;
   for (int j0 = 0; j0 < jend; j0 += 32) {
     const int j = j0 + lane;
     bool ok = false, beyond = false;
-    int ket = 0;
+    int ket = 0, bucket = 0;
     if (j < jend) {
       const double Ik = a.sorted_imax[cp.w + j];
       if (!(Ib * Ik * pg > a.cutoff)) {
         beyond = true;                           // kets are sorted by I_max: nothing further survives
       } else {
         ket = a.sorted[cp.w + j];
-        ok = quartet_survives(a, b, a.pairs[ket], Ib, Ik);
+        const PairRec k = a.pairs[ket];
+        const double bound = quartet_bound(a, b, k, Ib, Ik);
+        ok = bound > a.cutoff;
+        if (ok) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
       }
     }
-    const unsigned m = __ballot_sync(0xffffffffu, ok);
-    if (WRITE && ok) out[base + cnt + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
-    cnt += __popc(m);
+#pragma unroll
+    for (int k = 0; k < NBUCKET; ++k) {
+      const unsigned m = __ballot_sync(0xffffffffu, ok && bucket == k);
+      if (WRITE && ok && bucket == k)
+        out[offsets[slot(a, t, task.x, k)] + cnt[k] + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
+      cnt[k] += __popc(m);
+    }
     if (__any_sync(0xffffffffu, beyond)) break;
   }
-  if (!WRITE && lane == 0) counts[t] = cnt;
+  if (!WRITE && lane == 0)
+#pragma unroll
+    for (int k = 0; k < NBUCKET; ++k) counts[slot(a, t, task.x, k)] = cnt[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -279,9 +310,15 @@ struct JKArgs {
 template <int LA, int LB, int LC, int LD, typename T>
 __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
   using Q = Quartet<LA, LB, LC, LD>;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = t < a.n;
+  using RS = RysSmem<Q::NROOT>;
+  extern __shared__ double rys_tab[];
+  RS::load(rys_tab);
+  __syncthreads();
   unsigned long long nprim = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long n_pad = (a.n + 31) / 32 * 32;     // whole warps stay in the loop together
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n_pad; t += stride) {
+  const bool active = t < a.n;
   if (active) {
     const int2 qd = a.quartets[t];
     const PairRec b = a.pairs[qd.x];
@@ -292,7 +329,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
     const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
     const int nbp = any_same ? b.n_full : b.n_skip;
     const int nkp = any_same ? k.n_full : k.n_skip;
-    nprim = (unsigned long long)nbp * nkp;
+    nprim += (unsigned long long)nbp * nkp;
     double f = 1.0;
     if (b.sh_hi == b.sh_lo) f *= 0.5;
     if (k.sh_hi == k.sh_lo) f *= 0.5;
@@ -300,7 +337,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
     const double Rab[3] = {b.Rx, b.Ry, b.Rz};
     const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
     double I[Q::NA][Q::NB][Q::NC * Q::ND];
-    quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I);
+    quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I, rys_tab);
 
     const int n = a.n_cart;
     const double* __restrict__ P = a.P;
@@ -383,6 +420,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         }
       }
     }
+  }
   }
   // primitive-quartet counter (per class, one atomic per warp)
 #pragma unroll
@@ -804,6 +842,7 @@ struct tf_ctx {
   tf::DBuf<tf::PairRec> d_pairs;
   tf::DBuf<tf::PrimPair> d_prim_full, d_prim_skip;
   tf::DBuf<int2> d_tasks, d_quartets;
+  tf::DBuf<int> d_cp_task0;
   tf::DBuf<int4> d_cps;
   tf::DBuf<long long> d_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
@@ -841,8 +880,11 @@ static int build_tasks(tf_ctx* c) {
   c->n_tasks = (long long)tasks.size();
   TF_CUDA(c->d_cps.reserve(std::max<size_t>(c->cps.size(), 1)));
   TF_CUDA(c->d_tasks.reserve(std::max<size_t>(tasks.size(), 1)));
-  TF_CUDA(c->d_counts.reserve(tasks.size() + 1));
-  TF_CUDA(c->d_offsets.reserve(tasks.size() + 1));
+  TF_CUDA(c->d_counts.reserve(tasks.size() * NBUCKET + 1));
+  TF_CUDA(c->d_offsets.reserve(tasks.size() * NBUCKET + 1));
+  TF_CUDA(c->d_cp_task0.reserve(c->cp_first_task.size()));
+  TF_CUDA(cudaMemcpyAsync(c->d_cp_task0.p, c->cp_first_task.data(), c->cp_first_task.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, c->stream));
   if (!c->cps.empty())
     TF_CUDA(cudaMemcpyAsync(c->d_cps.p, c->cps.data(), c->cps.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
   if (!tasks.empty())
@@ -955,18 +997,62 @@ static void class_l(int k, int& lh, int& ll) {
   ll = k - lh * (lh + 1) / 2;
 }
 
-template <int LA, int LB, int LC, int LD>
-static void launch_jk(const JKArgs& a, cudaStream_t s) {
-  if (a.n <= 0) return;
+template <int LA, int LB, int LC, int LD, typename T>
+static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
+  constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
+  static int blocks_per_sm = -1;
+  if (blocks_per_sm < 0) {
+    cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T>, 128, smem);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int thr = 128;
-  k_jk<LA, LB, LC, LD, double><<<(unsigned)((a.n + thr - 1) / thr), thr, 0, s>>>(a);
+  const long long blocks = std::min<long long>((a.n + thr - 1) / thr, (long long)nsm * blocks_per_sm);
+  k_jk<LA, LB, LC, LD, T><<<(unsigned)blocks, thr, smem, s>>>(a);
 }
 
-static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStream_t s) {
+template <int LA, int LB, int LC, int LD>
+static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32) {
+  if (a.n <= 0) return;
+  if (fp32) launch_jk_t<LA, LB, LC, LD, float>(a, s);
+  else launch_jk_t<LA, LB, LC, LD, double>(a, s);
+}
+
+constexpr int GROUP_WPB = 4;
+
+template <int LA, int LB, int LC, int LD>
+static int launch_group(const JKArgs& a, cudaStream_t s) {
+  if (a.n <= 0) return TF_OK;
+  constexpr size_t smem = group_smem_bytes<LA, LB, LC, LD>(GROUP_WPB);
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_jk_group<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+      set_error("shared memory attribute");
+      return TF_ECUDA;
+    }
+    attr = true;
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  constexpr int QPB = GroupCfg<LA, LB, LC, LD>::QPW * GROUP_WPB;
+  const long long blocks = std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
+  GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.n_cart, a.prim_count};
+  k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
+  return TF_OK;
+}
+
+// fp32: evaluate the 2D recurrences and (e0|f0) sums in FP32 (thread-per-quartet
+// classes); roots, weights, transfers and the Fock accumulation stay FP64.
+static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStream_t s, bool fp32) {
   const int key = ((la * 3 + lb) * 3 + lc) * 3 + ld;
   switch (key) {
 #define TF_CASE(A, B, C, D) \
-  case ((A * 3 + B) * 3 + C) * 3 + D: launch_jk<A, B, C, D>(a, s); return TF_OK;
+  case ((A * 3 + B) * 3 + C) * 3 + D: launch_jk<A, B, C, D>(a, s, fp32); return TF_OK;
     TF_CASE(0, 0, 0, 0)
     TF_CASE(1, 0, 0, 0) TF_CASE(1, 0, 1, 0)
     TF_CASE(1, 1, 0, 0) TF_CASE(1, 1, 1, 0)
@@ -974,6 +1060,12 @@ static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStre
     TF_CASE(2, 1, 0, 0) TF_CASE(2, 1, 1, 0)
     TF_CASE(2, 2, 0, 0)
 #undef TF_CASE
+#define TF_GCASE(A, B, C, D) \
+  case ((A * 3 + B) * 3 + C) * 3 + D: return launch_group<A, B, C, D>(a, s);
+    TF_GCASE(1, 1, 1, 1)
+    TF_GCASE(2, 1, 1, 1) TF_GCASE(2, 1, 2, 0) TF_GCASE(2, 1, 2, 1)
+    TF_GCASE(2, 2, 1, 0) TF_GCASE(2, 2, 1, 1) TF_GCASE(2, 2, 2, 0) TF_GCASE(2, 2, 2, 1) TF_GCASE(2, 2, 2, 2)
+#undef TF_GCASE
     default: {
       if (std::max(std::max(la, lb), std::max(lc, ld)) > WL_MAX) {
         set_error("quartet class not built");
@@ -1024,23 +1116,33 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
                                                         c->d_pmax.p, c->d_pglob.p);
     kernels += 2;
   }
-  // quartet lists
-  ListArgs la{c->d_tasks.p, c->n_tasks, c->d_cps.p, c->d_cls_n.p, c->d_sorted.p, c->d_sorted_imax.p, c->d_pairs.p,
-              c->d_pmax.p, c->d_pglob.p, ns, c->opt.eri_schwarz_cutoff};
+  // quartet lists (bucket-sorted per class pair; FP32 buckets last when mixed)
+  const bool mixed = (flags & TF_JK_MIXED) != 0;
+  ListArgs la{c->d_tasks.p, c->n_tasks, c->d_cps.p, c->d_cp_task0.p, c->d_cls_n.p, c->d_sorted.p,
+              c->d_sorted_imax.p, c->d_pairs.p, c->d_pmax.p, c->d_pglob.p, ns, c->opt.eri_schwarz_cutoff,
+              mixed ? c->opt.mixed_fp32_cut : 0.0};
   const long long thr_list = 256;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
+  const long long nslots = c->n_tasks * NBUCKET;
   k_quartets<false><<<grid_list, (unsigned)thr_list, 0, s>>>(la, c->d_counts.p, nullptr, nullptr);
   kernels++;
   size_t tmp_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(c->n_tasks + 1), s);
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
   TF_CUDA(c->d_scan_tmp.reserve(tmp_bytes));
-  TF_CUDA(cudaMemsetAsync(c->d_counts.p + c->n_tasks, 0, sizeof(long long), s));
-  TF_CUDA(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp_bytes, c->d_counts.p, c->d_offsets.p,
-                                        (int)(c->n_tasks + 1), s));
-  std::vector<long long> cp_off(c->cps.size() + 1);
-  for (size_t k = 0; k <= c->cps.size(); ++k)
-    TF_CUDA(cudaMemcpyAsync(&cp_off[k], c->d_offsets.p + c->cp_first_task[k], sizeof(long long),
+  TF_CUDA(cudaMemsetAsync(c->d_counts.p + nslots, 0, sizeof(long long), s));
+  TF_CUDA(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1),
+                                        s));
+  // per class pair: start, FP32 start, end
+  const size_t ncp = c->cps.size();
+  std::vector<long long> cp_off(ncp + 1), cp_mid(ncp);
+  for (size_t k = 0; k <= ncp; ++k)
+    TF_CUDA(cudaMemcpyAsync(&cp_off[k], c->d_offsets.p + (long long)c->cp_first_task[k] * NBUCKET, sizeof(long long),
                             cudaMemcpyDeviceToHost, s));
+  for (size_t k = 0; k < ncp; ++k) {
+    const long long t0 = c->cp_first_task[k], nt = c->cp_first_task[k + 1] - t0;
+    TF_CUDA(cudaMemcpyAsync(&cp_mid[k], c->d_offsets.p + t0 * NBUCKET + (long long)NCOST * nt, sizeof(long long),
+                            cudaMemcpyDeviceToHost, s));
+  }
   TF_CUDA(cudaStreamSynchronize(s));
   const long long nq_total = cp_off.back();
   TF_CUDA(c->d_quartets.reserve(nq_total));
@@ -1052,6 +1154,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
   TF_CUDA(cudaEventRecord(c->ev1, s));
   double flops = 0.0;
+  long long n_fp32 = 0;
   std::vector<long long> cp_n(c->cps.size());
   while (c->cls_ev.size() < c->cps.size() + 1) {
     cudaEvent_t e;
@@ -1064,11 +1167,20 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     int l1h, l1l, l2h, l2l;
     class_l(cp.x, l1h, l1l);
     class_l(cp.y, l2h, l2l);
-    JKArgs a{c->d_quartets.p + cp_off[k], cp_off[k + 1] - cp_off[k], c->d_pairs.p, c->d_prim_full.p,
+    JKArgs a{c->d_quartets.p + cp_off[k], cp_mid[k] - cp_off[k], c->d_pairs.p, c->d_prim_full.p,
              c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, nc, c->d_prim_count.p};
-    cp_n[k] = a.n;
+    JKArgs a32 = a;
+    a32.quartets = c->d_quartets.p + cp_mid[k];
+    a32.n = cp_off[k + 1] - cp_mid[k];
+    cp_n[k] = a.n + a32.n;
+    n_fp32 += a32.n;
     if (a.n > 0) {
-      int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s);
+      int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
+      if (rc != TF_OK) return rc;
+      kernels++;
+    }
+    if (a32.n > 0) {
+      int rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
       if (rc != TF_OK) return rc;
       kernels++;
     }
@@ -1115,7 +1227,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   c->stats.build_ms = ms_all;
   c->stats.eri_ms = ms_eri;
   c->stats.quartets = (double)nq_total;
-  c->stats.quartets_fp32 = 0.0;
+  c->stats.quartets_fp32 = (double)n_fp32;
   c->stats.prim_quartets = npq;
   c->stats.flops = flops;
   c->stats.kernels = kernels;
@@ -1205,6 +1317,8 @@ int tf_ctx_create(const tf_basis* B, const tf_options* opt, tf_ctx** out) {
       cidx[CT.x[g]][CT.y[g]][CT.z[g]] = (unsigned char)CT.idx[CT.x[g]][CT.y[g]][CT.z[g]];
     }
     if (cudaMemcpyToSymbol(c_U, U, sizeof(U)) != cudaSuccess || cudaMemcpyToSymbol(c_comp, comp, sizeof(comp)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_gcomp, comp, sizeof(comp)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_gidx, cidx, sizeof(cidx)) != cudaSuccess ||
         cudaMemcpyToSymbol(c_cidx, cidx, sizeof(cidx)) != cudaSuccess ||
         cudaFuncSetAttribute(k_jk_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess ||
