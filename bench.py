@@ -250,10 +250,12 @@ def main():
             ev[k][1].record(stream)
             torch.cuda.synchronize(dev)
             for c in fb.class_stats():
-                a = cls_acc.setdefault(c["class"], [0.0, 0.0, 0])
+                a = cls_acc.setdefault(c["class"], [0.0, 0.0, 0, 0.0, 0.0])
                 a[0] += c["ms"]
                 a[1] += c["flops"]
                 a[2] += 1
+                a[3] = c["prim_quartets"]
+                a[4] = c["quartets"]
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_local = sum(step_ms)
     if world > 1:
@@ -265,7 +267,7 @@ def main():
     st = fb.stats()
 
     # dominant kernel by device time
-    dom_cls, (dom_ms, dom_flops, dom_n) = max(cls_acc.items(), key=lambda kv: kv[1][0])
+    dom_cls, (dom_ms, dom_flops, dom_n, _, _) = max(cls_acc.items(), key=lambda kv: kv[1][0])
     achieved = dom_flops / (dom_ms * 1e-3) / 1e12
     tkern, traffic = traffic_from_profile()
     roofline = {"bound": "fp64_pipe", "kernel": f"k_jk {dom_cls}", "achieved": achieved, "peak": peak,
@@ -296,7 +298,9 @@ def main():
             "e2e": e2e,
             "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"], "flops": st["flops"],
                       "eri_ms": st["eri_ms"], "build_ms": st["build_ms"]},
-            "classes_ms": {k: round(v[0] / v[2], 3) for k, v in sorted(cls_acc.items(), key=lambda kv: -kv[1][0])}}
+            "classes": {k: {"ms": round(v[0] / v[2], 3), "prim_quartets": v[3], "quartets": v[4],
+                            "tflops": round(v[1] / (v[0] * 1e-3) / 1e12, 3) if v[0] > 0 else None}
+                        for k, v in sorted(cls_acc.items(), key=lambda kv: -kv[1][0])}}
 
     if rank == 0 and world == 1 and not args.no_scf:
         from tonto_b200.scf import RHF

@@ -105,8 +105,8 @@ __host__ __device__ constexpr int gidx(int x, int y, int z) { return CT.first[x 
 // the 2 pi^(5/2) factor is applied per primitive quartet.
 struct __align__(16) PrimPair {
   double Px, Py, Pz, zeta;
-  double PAx, PAy, PAz, half_zinv;   // P - (centre of the higher-l shell), 1/(2 zeta)
-  double cc, pad;
+  double cc, half_zinv;              // prefactor, 1/(2 zeta)
+  double PAx, PAy, PAz, pad;         // P - (centre of the higher-l shell)
 };
 
 // One shell pair, oriented so that shell "hi" has the higher l (ties: the
@@ -163,11 +163,14 @@ template <int N>
 struct RysSmem {
   static constexpr int NI = rys_xmax(N);              // intervals
   static constexpr int SIZE = TF_RYS_NCOEF * 2 * N * NI;
+  // layout [k][j][i] with the pairs (u_i, w_i) adjacent: one 16-byte load per
+  // (coefficient, root)
   static __device__ __forceinline__ void load(double* t) {
     constexpr int OFF = rys_offset(N);
     for (int q = threadIdx.x; q < SIZE; q += blockDim.x) {
-      // q = (k * 2N + f) * NI + j
-      const int j = q % NI, kf = q / NI, f = kf % (2 * N), k = kf / (2 * N);
+      // q = ((k * NI + j) * N + i) * 2 + (0: node, 1: weight)
+      const int uw = q & 1, i = (q >> 1) % N, kj = (q >> 1) / N, j = kj % NI, k = kj / NI;
+      const int f = uw ? N + i : i;
       t[q] = tf_rys_coef[OFF + j * (2 * N * TF_RYS_NCOEF) + f * TF_RYS_NCOEF + k];
     }
   }
@@ -175,14 +178,22 @@ struct RysSmem {
     if (x < (double)NI) {
       const int j = (int)x;
       const double s = x - (double)j;
-      const double* c = t + j;
+      const double2* c = reinterpret_cast<const double2*>(t) + j * N;
+      constexpr int KS = NI * N;                     // stride between coefficients (double2)
 #pragma unroll
-      for (int f = 0; f < 2 * N; ++f) {
-        double v = c[(TF_RYS_DEG * 2 * N + f) * NI];
-#pragma unroll
-        for (int k = TF_RYS_DEG - 1; k >= 0; --k) v = fma(v, s, c[(k * 2 * N + f) * NI]);
-        if (f < N) u[f] = v; else w[f - N] = v;
+      for (int i = 0; i < N; ++i) {
+        const double2 v = c[TF_RYS_DEG * KS + i];
+        u[i] = v.x;
+        w[i] = v.y;
       }
+#pragma unroll
+      for (int k = TF_RYS_DEG - 1; k >= 0; --k)
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const double2 v = c[k * KS + i];
+          u[i] = fma(u[i], s, v.x);
+          w[i] = fma(w[i], s, v.y);
+        }
     } else {
       constexpr int HOFF = rys_hoffset(N);
       const double ix = 1.0 / x;
@@ -211,11 +222,16 @@ struct Quartet {
   static constexpr int NINT = NA * NB * NC * ND;
 };
 
-// read-only 32-byte load of half a primitive-pair record
+// read-only loads of a primitive-pair record: half 0 = (Px, Py, Pz, zeta),
+// half 1 = (PAx, PAy, PAz, 1/(2 zeta))
 __device__ __forceinline__ double4 ld4(const PrimPair* p, int half) {
-  const double2* q = reinterpret_cast<const double2*>(p) + 2 * half;
-  const double2 a = __ldg(q), b = __ldg(q + 1);
-  return make_double4(a.x, a.y, b.x, b.y);
+  const double2* q = reinterpret_cast<const double2*>(p);
+  if (half == 0) {
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+  }
+  const double2 c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
+  return make_double4(d.x, d.y, e.x, c.y);
 }
 
 // (e0|f0) accumulation over all primitive quartets of a contracted quartet.
@@ -231,15 +247,38 @@ __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp,
 #pragma unroll
     for (int f = 0; f < Q::NF; ++f) esfs[e][f] = T(0);
 
-  for (int ib = 0; ib < nbp; ++ib) {
-    const double4 b0 = ld4(bp + ib, 0);
-    const double4 b1 = ld4(bp + ib, 1);
-    const double bcc = __ldg(&bp[ib].cc) * TWOPI5ON2;
-    const double zeta = b0.w, half_zinv = b1.w;
-    for (int ik = 0; ik < nkp; ++ik) {
-      const double4 k0 = ld4(kp + ik, 0);
-      const double4 k1 = ld4(kp + ik, 1);
-      const double kcc = __ldg(&kp[ik].cc);
+  // one flat loop over the nbp x nkp primitive quartets: lanes with the same count
+  // but different (nbp, nkp) splits stay converged.  Kets are the outer index and
+  // bras the inner one: the lanes of a warp share the bra pair (bra-major lists),
+  // so the per-iteration bra loads are warp-wide broadcasts and each lane's ket
+  // record is read once per ket primitive.  P - A and 1/(2 zeta) only where needed.
+  const int npq = nbp * nkp;
+  int ib = 0, ik = 0;
+  const double2* bq = reinterpret_cast<const double2*>(bp);
+  const double2* kq = reinterpret_cast<const double2*>(kp);
+  constexpr int PPS = sizeof(PrimPair) / sizeof(double2);       // 5
+  double2 kP, kZ, kC, kA0 = make_double2(0.0, 0.0), kA1 = make_double2(0.0, 0.0);
+  auto load_ket = [&](int i) {
+    kP = __ldg(kq + i * PPS); kZ = __ldg(kq + i * PPS + 1); kC = __ldg(kq + i * PPS + 2);
+    if constexpr (Q::LCD > 0) { kA0 = __ldg(kq + i * PPS + 3); kA1 = __ldg(kq + i * PPS + 4); }
+  };
+  if (npq > 0) load_ket(0);
+  for (int p = 0; p < npq; ++p) {
+    {
+      const double2 bP = __ldg(bq + ib * PPS), bZ = __ldg(bq + ib * PPS + 1), bC = __ldg(bq + ib * PPS + 2);
+      double2 bA0 = make_double2(0.0, 0.0), bA1 = make_double2(0.0, 0.0);
+      if constexpr (Q::LAB > 0) { bA0 = __ldg(bq + ib * PPS + 3); bA1 = __ldg(bq + ib * PPS + 4); }
+      const double4 b0 = make_double4(bP.x, bP.y, bZ.x, bZ.y);
+      const double4 b1 = make_double4(bA0.x, bA0.y, bA1.x, bC.y);
+      const double4 k0 = make_double4(kP.x, kP.y, kZ.x, kZ.y);
+      const double4 k1 = make_double4(kA0.x, kA0.y, kA1.x, kC.y);
+      const double bcc = bC.x * TWOPI5ON2, kcc = kC.x;
+      const double zeta = b0.w, half_zinv = b1.w;
+      if (++ib == nbp) {
+        ib = 0;
+        ++ik;
+        if (ik < nkp) load_ket(ik);
+      }
       const double eta = k0.w, half_einv = k1.w;
       const double inv = 1.0 / (zeta + eta);
       const double rho = zeta * eta * inv;

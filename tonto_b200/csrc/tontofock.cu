@@ -91,6 +91,7 @@ __global__ void k_pair_prep(int n_pairs, PairRec* __restrict__ pairs, const doub
       q.half_zinv = 0.5 * inv;
       q.cc = ch * cl * inv * sqrt(inv) * prefac;
       q.pad = 0.0;
+      static_assert(sizeof(PrimPair) == 80, "primitive-pair record layout");
       prim_full[pr.full_off + i] = q;
       if (!same && !(prefac < pair_cutoff)) prim_skip[pr.skip_off + k++] = q;
     }
