@@ -145,6 +145,24 @@ int tf_build_jk_batch(tf_ctx** ctx, int n, const double* const* P, double* const
  * (foofiles/molecule.ints.foo:34-420); H_core = T + V. */
 int tf_one_electron(tf_ctx* ctx, const double* Z, double* S, double* T, double* V);
 
+/* One-electron integrals (S, T, V as tf_one_electron) without any device
+ * allocation, for callers that cannot call cudaMalloc where they need them: a
+ * program whose host framework owns the GPU memory, or code running where
+ * allocating would be forbidden or would stall the device.  No counterpart in
+ * the reference (Tonto allocates freely on the host); this is an addition.
+ *   basis: host arrays as for tf_ctx_create; Z: host nuclear charges;
+ *   dS, dT, dV: caller-owned DEVICE arrays of n_bf*n_bf doubles (column-major);
+ *   stream: cudaStream_t or NULL; the call is asynchronous on that stream.
+ * Limits: 256 atoms, 512 shells, 4096 primitives, 512 Cartesian functions
+ * (hence n_bf <= 512); larger inputs return TF_EUNSUPPORTED.  All scratch lives
+ * in one fixed array of about 6.4 MB in device memory, held by every GPU that
+ * loads this library until the process exits.  The first call on a device looks
+ * up that array's device address and uploads constant tables; make that first
+ * call before any stream capture.  Every call on a device reuses the same array,
+ * so calls whose work overlaps on the GPU (different streams, no ordering) race. */
+int tf_one_electron_noalloc(const tf_basis* basis, const double* Z, double* dS, double* dT, double* dV,
+                            void* stream);
+
 /* Statistics of the last build on this context. */
 int tf_last_stats(const tf_ctx* ctx, tf_stats* stats);
 

@@ -792,6 +792,26 @@ std::vector<double> spherical_matrix(int l) {
   return S[l];
 }
 
+// Host copies of the constant tables, built once when the library is loaded.
+struct HostTables {
+  double U[4][70];
+  unsigned char comp[3][NCOMP_ALL];
+  unsigned char cidx[LCOMP + 1][LCOMP + 1][LCOMP + 1];
+  HostTables() {
+    std::memset(U, 0, sizeof(U));
+    for (int l = 0; l <= 3; ++l) {
+      std::vector<double> m = spherical_matrix(l);
+      std::copy(m.begin(), m.end(), U[l]);
+    }
+    std::memset(cidx, 0, sizeof(cidx));
+    for (int g = 0; g < NCOMP_ALL; ++g) {
+      comp[0][g] = (unsigned char)CT.x[g]; comp[1][g] = (unsigned char)CT.y[g]; comp[2][g] = (unsigned char)CT.z[g];
+      cidx[CT.x[g]][CT.y[g]][CT.z[g]] = (unsigned char)CT.idx[CT.x[g]][CT.y[g]][CT.z[g]];
+    }
+  }
+};
+static const HostTables g_tables;
+
 // ---------------------------------------------------------------------------
 // host: device buffer
 // ---------------------------------------------------------------------------
@@ -1487,6 +1507,146 @@ int tf_one_electron(tf_ctx* c, const double* Z, double* S, double* T, double* V)
     TF_CUDA(cudaMemcpyAsync(outs[k], c->d_J.p, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     TF_CUDA(cudaStreamSynchronize(s));
   }
+  TF_CUDA(cudaGetLastError());
+  return TF_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// One-electron integrals with no device allocation.
+//
+// For callers that cannot call cudaMalloc at the point where they need the
+// integrals — code running inside a host framework that owns the device
+// allocator (an MPI rank driven by a Fortran program that pre-reserves the GPU
+// memory), or a context where allocation is forbidden or would serialize the
+// device.  The caller passes the basis (host arrays, as tf_basis) and three
+// device output arrays; everything else — the staged basis, the derived index
+// tables and the Cartesian S, T, V blocks — lives in one file-scope __device__
+// array of fixed size, held by every GPU that loads this library until exit.
+// ===========================================================================
+namespace tf {
+
+constexpr int NOALLOC_MAX_ATOM = 256;
+constexpr int NOALLOC_MAX_SHELL = 512;
+constexpr int NOALLOC_MAX_PRIM = 4096;
+constexpr int NOALLOC_MAX_CART = 512;      // also bounds n_bf
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+struct NoAllocScratch {
+  double S[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+  double T[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+  double V[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+  double xyz[3 * NOALLOC_MAX_ATOM];
+  double Z[NOALLOC_MAX_ATOM];
+  double exps[NOALLOC_MAX_PRIM];
+  double coefs[NOALLOC_MAX_PRIM];
+  int shell_atom[NOALLOC_MAX_SHELL];
+  int shell_l[NOALLOC_MAX_SHELL];
+  int shell_nprim[NOALLOC_MAX_SHELL];
+  int shell_poff[NOALLOC_MAX_SHELL];
+  int shell_cart[NOALLOC_MAX_SHELL];
+  int bf_shell[NOALLOC_MAX_CART];
+  int bf_local[NOALLOC_MAX_CART];
+};
+
+// The scratch array: about 6.4 MB, shared by every call on a device.
+static __device__ __align__(256) unsigned char tf_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Device addresses of the array, one per device, looked up on the first call on
+// that device (host code cannot use the symbol's host-side name as an address).
+static NoAllocScratch* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Derived index tables (first primitive, first Cartesian function per shell,
+// basis function -> shell and position) from shell_l / shell_nprim.
+__global__ void k_noalloc_index(int n_shell, int spherical, NoAllocScratch* sc) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int np = 0, nc = 0, nb = 0;
+  for (int s = 0; s < n_shell; ++s) {
+    const int l = sc->shell_l[s];
+    sc->shell_poff[s] = np;
+    sc->shell_cart[s] = nc;
+    np += sc->shell_nprim[s];
+    nc += ncart(l);
+    const int m = (spherical && l >= 2) ? 2 * l + 1 : ncart(l);
+    for (int i = 0; i < m; ++i) { sc->bf_shell[nb + i] = s; sc->bf_local[nb + i] = i; }
+    nb += m;
+  }
+}
+
+static int noalloc_setup(int dev, NoAllocScratch** out) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) { set_error("device ordinal beyond the no-allocation table"); return TF_EINVAL; }
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    TF_CUDA(cudaGetSymbolAddress(&ptr, tf_noalloc_scratch));
+    // constant tables (component order, spherical matrices) for this device
+    TF_CUDA(cudaMemcpyToSymbol(c_U, g_tables.U, sizeof(g_tables.U)));
+    TF_CUDA(cudaMemcpyToSymbol(c_comp, g_tables.comp, sizeof(g_tables.comp)));
+    g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(ptr);
+  }
+  *out = g_noalloc_ptr[dev];
+  return TF_OK;
+}
+
+}  // namespace tf
+
+extern "C" {
+
+int tf_one_electron_noalloc(const tf_basis* B, const double* Z, double* dS, double* dT, double* dV, void* stream) {
+  using namespace tf;
+  if (!B || !Z || !dS || !dT || !dV || !B->xyz || !B->shell_atom || !B->shell_l || !B->shell_nprim ||
+      !B->shell_first_bf || !B->exponents || !B->coefficients) {
+    set_error("null argument");
+    return TF_EINVAL;
+  }
+  if (B->n_atom <= 0 || B->n_atom > NOALLOC_MAX_ATOM || B->n_shell <= 0 || B->n_shell > NOALLOC_MAX_SHELL) {
+    set_error("tf_one_electron_noalloc: at most 256 atoms and 512 shells");
+    return TF_EUNSUPPORTED;
+  }
+  int np = 0, nc = 0, nb = 0;
+  for (int s = 0; s < B->n_shell; ++s) {
+    const int l = B->shell_l[s];
+    if (l < 0 || l > LMAX_SUPPORTED || B->shell_nprim[s] <= 0 || B->shell_atom[s] < 0 ||
+        B->shell_atom[s] >= B->n_atom || B->shell_first_bf[s] != nb) {
+      set_error("tf_one_electron_noalloc: bad shell record");
+      return TF_EINVAL;
+    }
+    np += B->shell_nprim[s];
+    nc += ncart(l);
+    nb += (B->is_spherical && l >= 2) ? 2 * l + 1 : ncart(l);
+  }
+  if (np > NOALLOC_MAX_PRIM || nc > NOALLOC_MAX_CART) {
+    set_error("tf_one_electron_noalloc: at most 4096 primitives and 512 Cartesian functions");
+    return TF_EUNSUPPORTED;
+  }
+  int dev = 0;
+  TF_CUDA(cudaGetDevice(&dev));
+  NoAllocScratch* sc = nullptr;
+  int rc = noalloc_setup(dev, &sc);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // stage the inputs in the scratch array (host arrays may be reused after return)
+  TF_CUDA(cudaMemcpyAsync(sc->xyz, B->xyz, 3 * B->n_atom * sizeof(double), cudaMemcpyHostToDevice, s));
+  TF_CUDA(cudaMemcpyAsync(sc->Z, Z, B->n_atom * sizeof(double), cudaMemcpyHostToDevice, s));
+  TF_CUDA(cudaMemcpyAsync(sc->exps, B->exponents, np * sizeof(double), cudaMemcpyHostToDevice, s));
+  TF_CUDA(cudaMemcpyAsync(sc->coefs, B->coefficients, np * sizeof(double), cudaMemcpyHostToDevice, s));
+  TF_CUDA(cudaMemcpyAsync(sc->shell_atom, B->shell_atom, B->n_shell * sizeof(int), cudaMemcpyHostToDevice, s));
+  TF_CUDA(cudaMemcpyAsync(sc->shell_l, B->shell_l, B->n_shell * sizeof(int), cudaMemcpyHostToDevice, s));
+  TF_CUDA(cudaMemcpyAsync(sc->shell_nprim, B->shell_nprim, B->n_shell * sizeof(int), cudaMemcpyHostToDevice, s));
+  k_noalloc_index<<<1, 1, 0, s>>>(B->n_shell, B->is_spherical ? 1 : 0, sc);
+  // every Cartesian element of S, T, V is written by the pair kernel (both
+  // triangles of every shell-pair block), so nothing needs clearing first
+  const long long npair = (long long)B->n_shell * (B->n_shell + 1) / 2;
+  k_one_electron<<<(unsigned)((npair + 127) / 128), 128, 0, s>>>(
+      B->n_shell, B->n_atom, sc->xyz, sc->Z, sc->shell_atom, sc->shell_l, sc->shell_nprim, sc->shell_poff,
+      sc->shell_cart, sc->exps, sc->coefs, nc, sc->S, sc->T, sc->V);
+  const long long n2 = (long long)nb * nb;
+  double* outs[3] = {dS, dT, dV};
+  double* ins[3] = {sc->S, sc->T, sc->V};
+  for (int k = 0; k < 3; ++k)
+    k_cart_to_basis<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, ins[k], sc->bf_shell, sc->bf_local,
+                                                                 sc->shell_l, sc->shell_cart,
+                                                                 B->is_spherical ? 1 : 0, outs[k]);
   TF_CUDA(cudaGetLastError());
   return TF_OK;
 }
