@@ -17,9 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtontofock.so")
 PEAK_LIB = os.path.join(HERE, "libtf_peak.so")
 
-SOURCES = ["tontofock.cu"]
-DEPS = ["tontofock.cu", "tf_device.cuh", "tf_warp.cuh", "rys_tables.inc", os.path.join("..", "..", "include",
-                                                                                          "tontofock.h")]
+SOURCES = ["tontofock.cu", "tf_mlp.cu"]
+DEPS = ["tontofock.cu", "tf_mlp.cu", "tf_device.cuh", "tf_warp.cuh", "tf_group.cuh", "rys_tables.inc",
+        os.path.join("..", "..", "include", "tontofock.h"), os.path.join("..", "..", "include", "tontofock_guess.h")]
 
 
 def nvcc() -> str:

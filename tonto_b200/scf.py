@@ -119,9 +119,22 @@ class RHF:
 
     def run(self, P0: Optional[torch.Tensor] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
             max_iter: int = 100, mixed: bool = False, fp64_final: int = 2, incremental: bool = False,
-            rebuild_every: int = 8, guess_name: str = "core",
+            rebuild_every: int = 8, guess_name: str = "core", mixed_until: float = 1e-6,
             fallback: Optional[Callable[[], torch.Tensor]] = None, fallback_after: int = 3,
             verbose: bool = False) -> SCFResult:
+        """Converge from P0 (default: core guess).
+
+        With ``mixed`` or ``incremental`` the SCF runs in two states.  "cheap": Fock
+        builds from the density change (incremental, a full rebuild every
+        ``rebuild_every`` cycles) and, while |dE| >= ``mixed_until``, with FP32
+        quartets below the Schwarz x density cut.  Once the convergence test passes
+        in the cheap state, the SCF continues with full FP64 builds and stops when the
+        test passes again after at least ``fp64_final`` of them, so the reported energy
+        comes from full FP64 Fock matrices.
+
+        ``fallback``: a callable giving a replacement density; used (once) if the DIIS
+        error after ``fallback_after`` cycles is not below the first cycle's.
+        """
         torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
         P = self.core_guess() if P0 is None else P0.to(self.dev, torch.float64).contiguous()
@@ -130,58 +143,62 @@ class RHF:
         builds = 0
         build_s = 0.0
         E_old = None
-        F_prev = None
-        P_prev = None
+        F_prev = P_prev = None
         fell_back = False
         err_first = None
         it = 0
         converged = False
-        fp64_left = None          # cycles still to run in FP64 at the end
+        state = "cheap" if (mixed or incremental) else "final"
+        n_final = 0
         since_full = 0
+        E = float("nan")
         while True:
-            # Fock build: mixed precision until close, incremental when allowed
-            near = E_old is not None and len(hist) >= 2 and abs(hist[-1][2]) < 1e3 * conv
-            use_mixed = mixed and not near and fp64_left is None
+            if state == "cheap":
+                use_mixed = mixed and not (E_old is not None and abs(hist[-1][2]) < mixed_until)
+                use_delta = incremental and F_prev is not None and since_full < rebuild_every
+            else:
+                use_mixed = use_delta = False
             flags = TF_JK_MIXED if use_mixed else TF_JK_FULL
             tb = time.perf_counter()
-            if incremental and F_prev is not None and since_full < rebuild_every and not near:
-                dP = (P - P_prev).contiguous()
-                J, K = self.jk(dP, flags | TF_JK_DELTA)
+            if use_delta:
+                J, K = self.jk((P - P_prev).contiguous(), flags | TF_JK_DELTA)
                 F = F_prev + J - 0.5 * K
                 since_full += 1
             else:
                 J, K = self.jk(P, flags)
                 F = self.H + J - 0.5 * K
                 since_full = 0
+            kind = ("mixed" if use_mixed else "fp64") + ("+delta" if use_delta else "")
             builds += 1
+            if state == "final":
+                n_final += 1
             E_t = 0.5 * torch.sum(P * (self.H + F)) + self.e_nuc
             err = F @ P @ self.S - self.S @ P @ F
             err_n_t = torch.linalg.norm(err)
             E, err_n = float(E_t), float(err_n_t)            # the per-cycle host sync
             build_s += time.perf_counter() - tb
             dE = float("inf") if E_old is None else E - E_old
-            hist.append((it, E, dE, err_n, "mixed" if use_mixed else "fp64"))
+            hist.append((it, E, dE, err_n, kind))
             if verbose:
-                print(f"scf {it:3d} E={E:.12f} dE={dE:.3e} err={err_n:.3e} {hist[-1][4]}")
+                print(f"scf {it:3d} E={E:.12f} dE={dE:.3e} err={err_n:.3e} {kind}")
             if err_first is None:
                 err_first = err_n
-            # learned-guess fallback: DIIS error not falling within the first cycles
             if fallback is not None and not fell_back and it == fallback_after and err_n >= err_first:
                 P = fallback().to(self.dev, torch.float64).contiguous()
                 diis.reset()
                 fell_back = True
                 E_old = None
-                F_prev = None
+                F_prev = P_prev = None
+                err_first = None
                 it += 1
                 continue
-            done = E_old is not None and abs(dE) < conv and err_n < diis_tol
-            if done and mixed and hist[-1][4] != "fp64":
-                done = False                                   # final answer must come from FP64 builds
-            if done and mixed:
-                n64 = sum(1 for h in hist[-fp64_final:] if h[4] == "fp64")
-                done = n64 >= min(fp64_final, len(hist))
-            if done or it >= max_iter:
-                converged = done
+            passed = E_old is not None and abs(dE) < conv and err_n < diis_tol
+            if state == "final" and passed and n_final >= min(fp64_final, it + 1):
+                converged = True
+                break
+            if state == "cheap" and passed:
+                state = "final"
+            if it >= max_iter:
                 break
             E_old = E
             F_prev, P_prev = F, P
