@@ -114,6 +114,19 @@ int tf_default_options(tf_options* opt);
  * on the device (replaces update_shell_info + initialize_max_I). */
 int tf_ctx_create(const tf_basis* basis, const tf_options* opt, tf_ctx** ctx);
 
+/* A context holding n independent molecules (same basis kind).  Every build then
+ * computes J and K of all of them with one launch per (la lb|lc ld) class: the
+ * many separate make_r_JK_direct calls of a set of SCFs, batched.  Device arrays
+ * for such a context are the molecules' n_bf x n_bf blocks concatenated in
+ * order; tf_batch_info gives the sizes. */
+int tf_ctx_create_batch(const tf_basis* bases, int n, const tf_options* opt, tf_ctx** ctx);
+
+/* Number of molecules of the context; fills n_bf_per_mol[n] if not NULL. */
+int tf_batch_info(const tf_ctx* ctx, int* n_bf_per_mol);
+
+/* J, K of every molecule of a batched context (host arrays per molecule). */
+int tf_build_jk_batched(tf_ctx* ctx, const double* const* P, double* const* J, double* const* K, int flags);
+
 /* New atom positions ([n_atom][3] bohr): rebuilds pair data and Schwarz bounds. */
 int tf_set_geometry(tf_ctx* ctx, const double* xyz);
 
@@ -170,10 +183,12 @@ int tf_last_stats(const tf_ctx* ctx, tf_stats* stats);
  * number of entries available (no reference counterpart: instrumentation). */
 int tf_last_class_stats(const tf_ctx* ctx, tf_class_stats* out, int max);
 
-/* Number of basis functions of the context (Tonto n_bf). */
+/* Number of basis functions of the context (Tonto n_bf; the sum over molecules
+ * for a batched context). */
 int tf_n_bf(const tf_ctx* ctx);
 
-/* Schwarz bounds sqrt(max |(ab|ab)|) per Tonto shell pair ab = a(a+1)/2 + b (a >= b). */
+/* Schwarz bounds sqrt(max |(ab|ab)|) per Tonto shell pair ab = a(a+1)/2 + b (a >= b);
+ * for a batched context, molecule after molecule. */
 int tf_schwarz(const tf_ctx* ctx, double* max_I);
 
 void tf_ctx_destroy(tf_ctx* ctx);

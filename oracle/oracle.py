@@ -119,6 +119,15 @@ class Oracle:
         lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(stride), int(offset))
         return time.perf_counter() - t
 
+    def jk_shard(self, P: np.ndarray, rank: int, n_ranks: int, n_threads: int = 0):
+        """Partial J, K of the bra pairs ab = rank, rank + n_ranks, ... (one rank of
+        Tonto's round-robin parallel do); the ranks' results sum to jk(P)."""
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        J = np.zeros((self.n_bf, self.n_bf), order="F")
+        K = np.zeros((self.n_bf, self.n_bf), order="F")
+        lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(n_ranks), int(rank))
+        return np.ascontiguousarray(J), np.ascontiguousarray(K)
+
     def counts(self, reset: bool = False) -> np.ndarray:
         out = np.zeros(625 * 2)
         lib().oracle_counts(self.h, _dp(out), int(reset))

@@ -52,3 +52,27 @@ def test_adam_reduces_loss(cuda_ok):
         m.adam(3e-3)
         first = float(loss) if first is None else first
     assert float(loss) < 0.2 * first
+
+
+@pytest.mark.gpu
+def test_trained_guess_cuts_scf_cycles_not_the_answer(cuda_ok):
+    """The committed network (tonto_b200/data/guess_mlp.npz) against the core guess on
+    held-out clusters (seeds outside the training range): fewer SCF cycles, the same
+    converged energy."""
+    import torch
+    from tonto_b200 import guess as G
+    from tonto_b200 import learned_guess as LG
+    from tonto_b200.molecules import water_cluster
+    from tonto_b200.scf import RHF
+    model = LG.MLP.load()
+    P_mono = model.extra["mono_P_local"]
+    for i, n in enumerate((8, 11)):
+        mol = water_cluster(n, seed=900000 + i)
+        rhf = RHF(mol, schwarz_cutoff=1e-12)
+        core = rhf.run(conv=1e-8, diis_tol=1e-5)
+        P_sup = torch.tensor(G.superposition_guess(mol, P_mono), device=rhf.dev)
+        P0 = torch.tensor(LG.learned_density(mol, model, P_mono), device=rhf.dev)
+        learned = rhf.run(P0=P0, conv=1e-8, diis_tol=1e-5, fallback=lambda: P_sup)
+        assert core.converged and learned.converged
+        assert learned.iterations <= 0.7 * core.iterations, (learned.iterations, core.iterations)
+        assert abs(learned.energy - core.energy) < 1e-8

@@ -117,10 +117,32 @@ struct __align__(16) PairRec {
   int cart_hi, cart_lo;      // first Cartesian function of each shell
   int full_off, n_full;      // primitive pairs without the pair cutoff
   int skip_off, n_skip;      // primitive pairs with the pair cutoff (atoms differ)
-  int cls, tonto_ab;         // pair class id, Tonto pair index a(a+1)/2+b
+  int mol, tonto_ab;         // molecule (batched contexts), Tonto pair index a(a+1)/2+b within it
   double Rx, Ry, Rz;         // hi centre - lo centre
   double imax;               // Schwarz bound sqrt(max |(ab|ab)|)
 };
+
+// One molecule of a (possibly batched) context: its shells are a contiguous
+// global range; its matrices sit at fixed offsets in the concatenated buffers.
+struct __align__(16) MolInfo {
+  int shell0, n_shell;       // global shell range
+  int cart0, bf0;            // first global Cartesian / basis function
+  int n_cart, n_bf;
+  int atom0, n_atom;         // global atom range
+  long long cmat;            // offset of its n_cart x n_cart Cartesian block
+  long long bmat;            // offset of its n_bf x n_bf Tonto-basis block
+  long long pmax;            // offset of its n_shell x n_shell pair-maximum block
+};
+
+// molecule owning element t of a concatenated buffer with offsets off[0..n_mol]
+__device__ __forceinline__ int find_mol(const long long* __restrict__ off, int n_mol, long long t) {
+  int lo = 0, hi = n_mol - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
 
 constexpr double TWOPI5ON2 = 34.9868366552497256925;   // 2 pi^(5/2)
 

@@ -120,7 +120,7 @@ struct GroupArgs {
   const double* P;
   double* J;
   double* K;
-  int n_cart;
+  const MolInfo* mols;
   unsigned long long* prim_count;
 };
 
@@ -151,8 +151,6 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
   const int fx = sc.x[gf], fy = sc.y[gf], fz = sc.z[gf];
   const long long nwarps = (long long)gridDim.x * wpb;
   unsigned long long nprim = 0;
-  const int n = a.n_cart;
-  const double* __restrict__ P = a.P;
   for (long long base = ((long long)blockIdx.x * wpb + warp) * QPW; base < a.n; base += nwarps * QPW) {
     const long long t = base + (in_group ? g : 0);
     const bool act = in_group && t < a.n;
@@ -256,6 +254,11 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
     // lanes outside every group start beyond all element loops (they only keep the warp in step)
     const double* I = group_hrr<LA, LB, LC, LD>(B0, B1, sc, Rab, Rcd, in_group ? gl : 0x40000000);
     if (act) {
+      const MolInfo mi = a.mols[b.mol];
+      const int n = mi.n_cart;
+      const double* __restrict__ P = a.P + mi.cmat;
+      double* __restrict__ Jm = a.J + mi.cmat;
+      double* __restrict__ Km = a.K + mi.cmat;
       double f = 1.0;
       if (b.sh_hi == b.sh_lo) f *= 0.5;
       if (k.sh_hi == k.sh_lo) f *= 0.5;
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         for (int c = 0; c < NC; ++c)
 #pragma unroll
           for (int d = 0; d < ND; ++d) s += I[e * NCD + c * ND + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
-        atomicAdd(a.J + (size_t)(oa + ia) * n + ob + ibb, f * s);
+        atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ibb, f * s);
       }
       for (int e = gl; e < NCD; e += G) {                // J(cd) = sum_ab I P(ab)
         const int c = e / ND, d = e - c * ND;
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
           for (int ibb = 0; ibb < NB; ++ibb) s += I[(ia * NB + ibb) * NCD + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ibb);
-        atomicAdd(a.J + (size_t)(oc + c) * n + od + d, f * s);
+        atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
       }
       for (int e = gl; e < NA * NC; e += G) {            // K(ac) = sum_bd I P(bd)
         const int ia = e / NC, c = e - ia * NC;
@@ -287,7 +290,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         for (int ibb = 0; ibb < NB; ++ibb)
 #pragma unroll
           for (int d = 0; d < ND; ++d) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + od + d);
-        atomicAdd(a.K + (size_t)(oa + ia) * n + oc + c, f * s);
+        atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
       }
       for (int e = gl; e < NA * ND; e += G) {            // K(ad) = sum_bc I P(bc)
         const int ia = e / ND, d = e - ia * ND;
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         for (int ibb = 0; ibb < NB; ++ibb)
 #pragma unroll
           for (int c = 0; c < NC; ++c) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + oc + c);
-        atomicAdd(a.K + (size_t)(oa + ia) * n + od + d, f * s);
+        atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
       }
       for (int e = gl; e < NB * NC; e += G) {            // K(bc) = sum_ad I P(ad)
         const int ibb = e / NC, c = e - ibb * NC;
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
           for (int d = 0; d < ND; ++d) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
-        atomicAdd(a.K + (size_t)(ob + ibb) * n + oc + c, f * s);
+        atomicAdd(Km + (size_t)(ob + ibb) * n + oc + c, f * s);
       }
       for (int e = gl; e < NB * ND; e += G) {            // K(bd) = sum_ac I P(ac)
         const int ibb = e / ND, d = e - ibb * ND;
@@ -314,7 +317,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
           for (int c = 0; c < NC; ++c) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
-        atomicAdd(a.K + (size_t)(ob + ibb) * n + od + d, f * s);
+        atomicAdd(Km + (size_t)(ob + ibb) * n + od + d, f * s);
       }
     }
     __syncwarp();

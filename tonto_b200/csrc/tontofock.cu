@@ -146,54 +146,84 @@ __global__ void k_schwarz(const int* __restrict__ ids, int n, PairRec* __restric
 // ---------------------------------------------------------------------------
 // kernels: per-build density preparation
 // ---------------------------------------------------------------------------
-// P_cart[p][q] = sum U_A[p][m] P[m][m'] U_B[q][m'] over the shell blocks.
-__global__ void k_density_to_cart(int n_cart, int n_bf, const double* __restrict__ P,
-                                  const int* __restrict__ cart_shell, const int* __restrict__ cart_local,
-                                  const int* __restrict__ shell_l, const int* __restrict__ shell_first_bf,
-                                  int spherical, double* __restrict__ Pc) {
+struct BatchArgs {
+  const MolInfo* mols;
+  int n_mol;
+  const long long* cmat_off;    // n_mol + 1 prefix offsets of the Cartesian blocks
+  const long long* bmat_off;    // ... of the Tonto-basis blocks
+  const long long* pmax_off;    // ... of the pair-maximum blocks
+  const int* cart_shell;        // global Cartesian function -> global shell
+  const int* cart_local;        // ... -> component within the shell
+  const int* bf_shell;          // global basis function -> global shell
+  const int* bf_local;
+  const int* shell_l;
+  const int* shell_first_bf;    // within the molecule
+  const int* shell_cart;        // within the molecule
+  const int* shell_nbf;
+  int spherical;
+};
+
+// P_cart[p][q] = sum U_A[p][m] P[m][m'] U_B[q][m'] over the shell blocks, for every
+// molecule of the batch (P, Pc: concatenated per-molecule blocks).
+__global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, double* __restrict__ Pc) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)n_cart * n_cart) return;
-  const int p = (int)(t / n_cart), q = (int)(t % n_cart);
-  const int sp = cart_shell[p], sq = cart_shell[q];
-  const int ip = cart_local[p], iq = cart_local[q];
-  const int lp = shell_l[sp], lq = shell_l[sq];
-  const int fp = shell_first_bf[sp], fq = shell_first_bf[sq];
-  const bool tp = spherical && lp >= 2, tq = spherical && lq >= 2;
+  if (t >= b.cmat_off[b.n_mol]) return;
+  const int m = find_mol(b.cmat_off, b.n_mol, t);
+  const MolInfo mi = b.mols[m];
+  const long long r = t - mi.cmat;
+  const int p = (int)(r / mi.n_cart), q = (int)(r % mi.n_cart);
+  const int sp = b.cart_shell[mi.cart0 + p], sq = b.cart_shell[mi.cart0 + q];
+  const int ip = b.cart_local[mi.cart0 + p], iq = b.cart_local[mi.cart0 + q];
+  const int lp = b.shell_l[sp], lq = b.shell_l[sq];
+  const int fp = b.shell_first_bf[sp], fq = b.shell_first_bf[sq];
+  const bool tp = b.spherical && lp >= 2, tq = b.spherical && lq >= 2;
+  const double* Pm = P + mi.bmat;
+  const int n_bf = mi.n_bf;
   double s = 0.0;
   if (!tp && !tq) {
-    s = P[(size_t)(fq + iq) * n_bf + fp + ip];
+    s = Pm[(size_t)(fq + iq) * n_bf + fp + ip];
   } else {
     const int mp = tp ? 2 * lp + 1 : 1, mq = tq ? 2 * lq + 1 : 1;
     for (int a = 0; a < mp; ++a) {
       const double ua = tp ? c_U[lp][ip * mp + a] : 1.0;
       const int ia = tp ? fp + a : fp + ip;
       if (ua == 0.0) continue;
-      for (int b = 0; b < mq; ++b) {
-        const double ub = tq ? c_U[lq][iq * mq + b] : 1.0;
-        const int ib = tq ? fq + b : fq + iq;
-        s += ua * ub * P[(size_t)ib * n_bf + ia];
+      for (int bb = 0; bb < mq; ++bb) {
+        const double ub = tq ? c_U[lq][iq * mq + bb] : 1.0;
+        const int ib = tq ? fq + bb : fq + iq;
+        s += ua * ub * Pm[(size_t)ib * n_bf + ia];
       }
     }
   }
-  Pc[(size_t)p * n_cart + q] = s;
+  Pc[t] = s;
 }
 
-// max |P(a,b)| over each shell pair block (Tonto basis), and the global max.
-__global__ void k_pmax(int n_shell, int n_bf, const double* __restrict__ P, const int* __restrict__ shell_first_bf,
-                       const int* __restrict__ shell_nbf, double* __restrict__ pmax,
+// max |P(a,b)| over each shell pair block (Tonto basis) and, per molecule, the
+// maximum over all pairs (an upper bound: the high word is rounded up).
+__global__ void k_pmax(BatchArgs b, const double* __restrict__ P, double* __restrict__ pmax,
                        unsigned long long* __restrict__ pglob) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double m = 0.0;
-  if (t < (long long)n_shell * n_shell) {
-    const int a = (int)(t / n_shell), b = (int)(t % n_shell);
-    const int fa = shell_first_bf[a], fb = shell_first_bf[b], na = shell_nbf[a], nb = shell_nbf[b];
+  const long long total = b.pmax_off[b.n_mol];
+  double mx = 0.0;
+  int m = 0;
+  if (t < total) {
+    m = find_mol(b.pmax_off, b.n_mol, t);
+    const MolInfo mi = b.mols[m];
+    const long long r = t - mi.pmax;
+    const int sa = mi.shell0 + (int)(r / mi.n_shell), sb = mi.shell0 + (int)(r % mi.n_shell);
+    const int fa = b.shell_first_bf[sa], fb = b.shell_first_bf[sb], na = b.shell_nbf[sa], nb = b.shell_nbf[sb];
+    const double* Pm = P + mi.bmat;
     for (int j = 0; j < nb; ++j)
-      for (int i = 0; i < na; ++i) m = fmax(m, fabs(P[(size_t)(fb + j) * n_bf + fa + i]));
-    pmax[t] = m;
+      for (int i = 0; i < na; ++i) mx = fmax(mx, fabs(Pm[(size_t)(fb + j) * mi.n_bf + fa + i]));
+    pmax[t] = mx;
   }
-  // nonnegative doubles order like their bit patterns
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(pglob, (unsigned long long)__double_as_longlong(m));
+  // nonnegative doubles order like their bit patterns; reduce the high words
+  // among the lanes of the same molecule, then one atomic per molecule and warp
+  const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(mx) >> 32);
+  const unsigned grp = __match_any_sync(0xffffffffu, t < total ? m : -1);
+  const unsigned mhi = __reduce_max_sync(grp, hi);
+  if (t < total && (threadIdx.x & 31) == __ffs(grp) - 1 && mhi)
+    atomicMax(pglob + m, ((unsigned long long)mhi << 32) | 0xffffffffull);
 }
 
 // ---------------------------------------------------------------------------
@@ -202,27 +232,35 @@ __global__ void k_pmax(int n_shell, int n_bf, const double* __restrict__ P, cons
 constexpr int NCOST = 13;                  // log2 buckets of the primitive-quartet count
 constexpr int NBUCKET = 2 * NCOST;         // FP64 buckets, then FP32 buckets
 
+// One (class pair, molecule) unit of the list builder.  Units of the same class
+// pair are consecutive and form a group; the quartets of a group are one launch.
+struct CPUnit {
+  int p1, p2;                   // bra and ket pair classes
+  int bra_off, ket_off;         // offsets of the molecule's class lists in `sorted`
+  int n_ket, mol;
+};
+
 struct ListArgs {
-  const int2* tasks;            // (class pair, bra position)
+  const int2* tasks;            // (unit, bra position)
   long long n_tasks;
-  const int4* cp;               // class pair: (bra class, ket class, bra list offset, ket list offset)
-  const int* cp_task0;          // first task of each class pair
-  const int* cls_n;             // pairs per class
-  const int* sorted;            // pair ids, grouped by class, I_max descending
+  const CPUnit* units;
+  const int* unit_group;        // unit -> group (class pair)
+  const int* group_task0;       // first task of each group
+  const int* sorted;            // pair ids, grouped by (molecule, class), I_max descending
   const double* sorted_imax;
   const PairRec* pairs;
-  const double* pmax;           // n_shell x n_shell
-  const unsigned long long* pglob;
-  int n_shell;
+  const MolInfo* mols;
+  const double* pmax;           // per-molecule n_shell x n_shell blocks
+  const unsigned long long* pglob;   // per molecule
   double cutoff;
   double fp32_cut;              // 0: no FP32 quartets
 };
 
-__device__ __forceinline__ double quartet_bound(const ListArgs& a, const PairRec& b, const PairRec& k, double Ib,
-                                                double Ik) {
-  const double* pm = a.pmax;
-  const int ns = a.n_shell;
-  const int sa = b.sh_hi, sb = b.sh_lo, sc = k.sh_hi, sd = k.sh_lo;
+__device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo& mi, const PairRec& b,
+                                                const PairRec& k, double Ib, double Ik) {
+  const double* pm = a.pmax + mi.pmax;
+  const int ns = mi.n_shell;
+  const int sa = b.sh_hi - mi.shell0, sb = b.sh_lo - mi.shell0, sc = k.sh_hi - mi.shell0, sd = k.sh_lo - mi.shell0;
   double m = fmax(pm[sa * ns + sb], pm[sc * ns + sd]);
   m = fmax(m, fmax(pm[sa * ns + sc], pm[sa * ns + sd]));
   m = fmax(m, fmax(pm[sb * ns + sc], pm[sb * ns + sd]));
@@ -238,10 +276,11 @@ __device__ __forceinline__ int cost_bucket(const PairRec& b, const PairRec& k) {
   return lg < NCOST ? lg : NCOST - 1;
 }
 
-// Index of (task, bucket) in the count/offset arrays: class pair, then bucket,
-// then task -> each class pair's list is bucket-sorted and deterministic.
-__device__ __forceinline__ long long slot(const ListArgs& a, long long t, int cpi, int bucket) {
-  const long long t0 = a.cp_task0[cpi], nt = a.cp_task0[cpi + 1] - t0;
+// Index of (task, bucket) in the count/offset arrays: group (class pair), then
+// bucket, then task (molecule by molecule) -> each class pair's list is bucket-
+// sorted across the whole batch, with all FP32 buckets after the FP64 ones.
+__device__ __forceinline__ long long slot(const ListArgs& a, long long t, int g, int bucket) {
+  const long long t0 = a.group_task0[g], nt = a.group_task0[g + 1] - t0;
   return t0 * NBUCKET + (long long)bucket * nt + (t - t0);
 }
 
@@ -252,13 +291,15 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
   const int lane = threadIdx.x & 31;
   if (t >= a.n_tasks) return;
   const int2 task = a.tasks[t];
-  const int4 cp = a.cp[task.x];
+  const CPUnit cp = a.units[task.x];
+  const int g = a.unit_group[task.x];
+  const MolInfo mi = a.mols[cp.mol];
   const int i = task.y;
-  const int bra = a.sorted[cp.z + i];
-  const double Ib = a.sorted_imax[cp.z + i];
+  const int bra = a.sorted[cp.bra_off + i];
+  const double Ib = a.sorted_imax[cp.bra_off + i];
   const PairRec b = a.pairs[bra];
-  const int jend = (cp.x == cp.y) ? i + 1 : a.cls_n[cp.y];
-  const double pg = __longlong_as_double((long long)*a.pglob);
+  const int jend = (cp.p1 == cp.p2) ? i + 1 : cp.n_ket;
+  const double pg = __longlong_as_double((long long)a.pglob[cp.mol]);
   int cnt[NBUCKET];
 #pragma unroll
   for (int k = 0; k < NBUCKET; ++k) cnt[k] = 0;
@@ -267,13 +308,13 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
     bool ok = false, beyond = false;
     int ket = 0, bucket = 0;
     if (j < jend) {
-      const double Ik = a.sorted_imax[cp.w + j];
+      const double Ik = a.sorted_imax[cp.ket_off + j];
       if (!(Ib * Ik * pg > a.cutoff)) {
         beyond = true;                           // kets are sorted by I_max: nothing further survives
       } else {
-        ket = a.sorted[cp.w + j];
+        ket = a.sorted[cp.ket_off + j];
         const PairRec k = a.pairs[ket];
-        const double bound = quartet_bound(a, b, k, Ib, Ik);
+        const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
         ok = bound > a.cutoff;
         if (ok) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
       }
@@ -282,14 +323,14 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
     for (int k = 0; k < NBUCKET; ++k) {
       const unsigned m = __ballot_sync(0xffffffffu, ok && bucket == k);
       if (WRITE && ok && bucket == k)
-        out[offsets[slot(a, t, task.x, k)] + cnt[k] + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
+        out[offsets[slot(a, t, g, k)] + cnt[k] + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
       cnt[k] += __popc(m);
     }
     if (__any_sync(0xffffffffu, beyond)) break;
   }
   if (!WRITE && lane == 0)
 #pragma unroll
-    for (int k = 0; k < NBUCKET; ++k) counts[slot(a, t, task.x, k)] = cnt[k];
+    for (int k = 0; k < NBUCKET; ++k) counts[slot(a, t, g, k)] = cnt[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -301,10 +342,10 @@ struct JKArgs {
   const PairRec* pairs;
   const PrimPair* prim_full;
   const PrimPair* prim_skip;
-  const double* P;              // Cartesian density, n_cart x n_cart
+  const double* P;              // Cartesian density (per-molecule blocks)
   double* J;                    // Cartesian accumulators
   double* K;
-  int n_cart;
+  const MolInfo* mols;
   unsigned long long* prim_count;   // per quartet class
 };
 
@@ -340,8 +381,11 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
     double I[Q::NA][Q::NB][Q::NC * Q::ND];
     quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I, rys_tab);
 
-    const int n = a.n_cart;
-    const double* __restrict__ P = a.P;
+    const MolInfo mi = a.mols[b.mol];
+    const int n = mi.n_cart;
+    const double* __restrict__ P = a.P + mi.cmat;
+    double* __restrict__ Jm = a.J + mi.cmat;
+    double* __restrict__ Km = a.K + mi.cmat;
     const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
     // J(ab) += f sum_cd I P(cd);  J(cd) += f sum_ab I P(ab)
     double Pcd[Q::NC][Q::ND];
@@ -358,7 +402,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         for (int c = 0; c < Q::NC; ++c)
 #pragma unroll
           for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
-        atomicAdd(a.J + (size_t)(oa + ia) * n + ob + ib, f * s);
+        atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, f * s);
       }
     double Pab[Q::NA][Q::NB];
 #pragma unroll
@@ -374,7 +418,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
           for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
-        atomicAdd(a.J + (size_t)(oc + c) * n + od + d, f * s);
+        atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
       }
     // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
     // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
@@ -392,7 +436,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         for (int ib = 0; ib < Q::NB; ++ib)
 #pragma unroll
           for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
-        atomicAdd(a.K + (size_t)(oa + ia) * n + oc + c, f * s);
+        atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
       }
 #pragma unroll
       for (int d = 0; d < Q::ND; ++d) {
@@ -401,7 +445,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         for (int ib = 0; ib < Q::NB; ++ib)
 #pragma unroll
           for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
-        atomicAdd(a.K + (size_t)(oa + ia) * n + od + d, f * s);
+        atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
       }
 #pragma unroll
       for (int ib = 0; ib < Q::NB; ++ib) {
@@ -410,14 +454,14 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
           double s = 0.0;
 #pragma unroll
           for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pad[d];
-          atomicAdd(a.K + (size_t)(ob + ib) * n + oc + c, f * s);
+          atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
         }
 #pragma unroll
         for (int d = 0; d < Q::ND; ++d) {
           double s = 0.0;
 #pragma unroll
           for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pac[c];
-          atomicAdd(a.K + (size_t)(ob + ib) * n + od + d, f * s);
+          atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
         }
       }
     }
@@ -442,12 +486,15 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
   const long long nwarps = (long long)gridDim.x * WARPS_PER_BLOCK;
   unsigned long long nprim = 0;
   const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
-  const int n = a.n_cart;
-  const double* __restrict__ P = a.P;
   for (long long t = (long long)blockIdx.x * WARPS_PER_BLOCK + wib; t < a.n; t += nwarps) {
     const int2 qd = a.quartets[t];
     const PairRec b = a.pairs[qd.x];
     const PairRec k = a.pairs[qd.y];
+    const MolInfo mi = a.mols[b.mol];
+    const int n = mi.n_cart;
+    const double* __restrict__ P = a.P + mi.cmat;
+    double* __restrict__ Jm = a.J + mi.cmat;
+    double* __restrict__ Km = a.K + mi.cmat;
     const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
                           b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
     const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
@@ -470,42 +517,42 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
       double s = 0.0;
       for (int c = 0; c < nc; ++c)
         for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
-      atomicAdd(a.J + (size_t)(oa + ia) * n + ob + ib, f * s);
+      atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, f * s);
     }
     for (int e = lane; e < ncd; e += 32) {              // J(cd)
       const int c = e / nd, d = e % nd;
       double s = 0.0;
       for (int ia = 0; ia < na; ++ia)
         for (int ib = 0; ib < nb; ++ib) s += I[(ia * nb + ib) * ncd + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ib);
-      atomicAdd(a.J + (size_t)(oc + c) * n + od + d, f * s);
+      atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
     }
     for (int e = lane; e < na * nc; e += 32) {          // K(ac) = sum_bd I P(bd)
       const int ia = e / nc, c = e % nc;
       double s = 0.0;
       for (int ib = 0; ib < nb; ++ib)
         for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
-      atomicAdd(a.K + (size_t)(oa + ia) * n + oc + c, f * s);
+      atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
     }
     for (int e = lane; e < na * nd; e += 32) {          // K(ad) = sum_bc I P(bc)
       const int ia = e / nd, d = e % nd;
       double s = 0.0;
       for (int ib = 0; ib < nb; ++ib)
         for (int c = 0; c < nc; ++c) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
-      atomicAdd(a.K + (size_t)(oa + ia) * n + od + d, f * s);
+      atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
     }
     for (int e = lane; e < nb * nc; e += 32) {          // K(bc) = sum_ad I P(ad)
       const int ib = e / nc, c = e % nc;
       double s = 0.0;
       for (int ia = 0; ia < na; ++ia)
         for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
-      atomicAdd(a.K + (size_t)(ob + ib) * n + oc + c, f * s);
+      atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
     }
     for (int e = lane; e < nb * nd; e += 32) {          // K(bd) = sum_ac I P(ac)
       const int ib = e / nd, d = e % nd;
       double s = 0.0;
       for (int ia = 0; ia < na; ++ia)
         for (int c = 0; c < nc; ++c) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
-      atomicAdd(a.K + (size_t)(ob + ib) * n + od + d, f * s);
+      atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
     }
     __syncwarp();
   }
@@ -563,35 +610,41 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int
 // ---------------------------------------------------------------------------
 // kernel: fold, reflect and return to the Tonto basis
 // ---------------------------------------------------------------------------
-__global__ void k_finalize(int n_bf, int n_cart, const double* __restrict__ Jc, const double* __restrict__ Kc,
-                           const int* __restrict__ bf_shell, const int* __restrict__ bf_local,
-                           const int* __restrict__ shell_l, const int* __restrict__ shell_cart, int spherical,
+// J = 2 (J + J^T), K = K + K^T in the Cartesian basis, then to the Tonto basis
+// (column-major), for every molecule of the batch.
+__global__ void k_finalize(BatchArgs bt, const double* __restrict__ Jc, const double* __restrict__ Kc,
                            double* __restrict__ J, double* __restrict__ K) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)n_bf * n_bf) return;
-  const int j = (int)(t / n_bf), i = (int)(t % n_bf);       // column-major output (i, j)
-  const int si = bf_shell[i], sj = bf_shell[j];
-  const int mi = bf_local[i], mj = bf_local[j];
-  const int li = shell_l[si], lj = shell_l[sj];
-  const int ci = shell_cart[si], cj = shell_cart[sj];
-  const bool ti = spherical && li >= 2, tj = spherical && lj >= 2;
+  if (t >= bt.bmat_off[bt.n_mol]) return;
+  const int m = find_mol(bt.bmat_off, bt.n_mol, t);
+  const MolInfo mi = bt.mols[m];
+  const long long r = t - mi.bmat;
+  const int j = (int)(r / mi.n_bf), i = (int)(r % mi.n_bf);
+  const int si = bt.bf_shell[mi.bf0 + i], sj = bt.bf_shell[mi.bf0 + j];
+  const int mi_ = bt.bf_local[mi.bf0 + i], mj = bt.bf_local[mi.bf0 + j];
+  const int li = bt.shell_l[si], lj = bt.shell_l[sj];
+  const int ci = bt.shell_cart[si], cj = bt.shell_cart[sj];
+  const bool ti = bt.spherical && li >= 2, tj = bt.spherical && lj >= 2;
+  const double* Jm = Jc + mi.cmat;
+  const double* Km = Kc + mi.cmat;
+  const int nc = mi.n_cart;
   double sJ = 0.0, sK = 0.0;
   const int ni = ti ? ncart(li) : 1, nj = tj ? ncart(lj) : 1;
   for (int p = 0; p < ni; ++p) {
-    const double up = ti ? c_U[li][p * (2 * li + 1) + mi] : 1.0;
+    const double up = ti ? c_U[li][p * (2 * li + 1) + mi_] : 1.0;
     if (up == 0.0) continue;
-    const int cp = ti ? ci + p : ci + mi;
+    const int cp = ti ? ci + p : ci + mi_;
     for (int q = 0; q < nj; ++q) {
       const double uq = tj ? c_U[lj][q * (2 * lj + 1) + mj] : 1.0;
       if (uq == 0.0) continue;
       const int cq = tj ? cj + q : cj + mj;
       const double w = up * uq;
-      sJ += w * (Jc[(size_t)cp * n_cart + cq] + Jc[(size_t)cq * n_cart + cp]);
-      sK += w * (Kc[(size_t)cp * n_cart + cq] + Kc[(size_t)cq * n_cart + cp]);
+      sJ += w * (Jm[(size_t)cp * nc + cq] + Jm[(size_t)cq * nc + cp]);
+      sK += w * (Km[(size_t)cp * nc + cq] + Km[(size_t)cq * nc + cp]);
     }
   }
-  J[(size_t)j * n_bf + i] = 2.0 * sJ;
-  K[(size_t)j * n_bf + i] = sK;
+  J[t] = 2.0 * sJ;
+  K[t] = sK;
 }
 
 __global__ void k_fock(long long n, const double* __restrict__ H, const double* __restrict__ J,
@@ -613,7 +666,154 @@ __device__ __forceinline__ void rys_eval_n(double x, double* u, double* w) {
   for (int i = 0; i < N; ++i) { u[i] = uu[i]; w[i] = ww[i]; }
 }
 
-__global__ void k_one_electron(int n_shell, int n_atom, const double* __restrict__ xyz, const double* __restrict__ Z,
+// One thread per shell pair record (pairs of one molecule only); the Cartesian
+// blocks go into the molecule's n_cart x n_cart slices of S, T, V.
+__global__ void k_one_electron(long long n_pairs, const PairRec* __restrict__ pairs, const MolInfo* __restrict__ mols,
+                               const double* __restrict__ xyz, const double* __restrict__ Z,
+                               const int* __restrict__ shell_atom, const int* __restrict__ shell_l,
+                               const int* __restrict__ shell_nprim, const int* __restrict__ shell_poff,
+                               const int* __restrict__ shell_cart, const double* __restrict__ exps,
+                               const double* __restrict__ coefs, double* __restrict__ S,
+                               double* __restrict__ T, double* __restrict__ V) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_pairs) return;
+  const PairRec pr = pairs[t];
+  const MolInfo mi = mols[pr.mol];
+  const int sa = pr.sh_hi, sb = pr.sh_lo;
+  const int n_cart = mi.n_cart;
+  S += mi.cmat;
+  T += mi.cmat;
+  V += mi.cmat;
+  const int la = shell_l[sa], lb = shell_l[sb];
+  const int na = ncart(la), nb = ncart(lb);
+  const double* A = xyz + 3 * shell_atom[sa];
+  const double* B = xyz + 3 * shell_atom[sb];
+  const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+  const double r2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+  double s_c[36], t_c[36], v_c[36];
+  for (int i = 0; i < na * nb; ++i) { s_c[i] = 0.0; t_c[i] = 0.0; v_c[i] = 0.0; }
+  constexpr int LD = 6;                    // 1D table edge (l <= 2: i <= 3, j <= 4)
+  const int nroot = (la + lb) / 2 + 1;
+  for (int ia = 0; ia < shell_nprim[sa]; ++ia)
+    for (int ib = 0; ib < shell_nprim[sb]; ++ib) {
+      const double a = exps[shell_poff[sa] + ia], ca = coefs[shell_poff[sa] + ia];
+      const double b = exps[shell_poff[sb] + ib], cb = coefs[shell_poff[sb] + ib];
+      const double z = a + b, oo2z = 0.5 / z;
+      const double Kab = exp(-a * b * r2 / z) * ca * cb;
+      double P[3], PA[3], PB[3];
+      for (int k = 0; k < 3; ++k) { P[k] = (a * A[k] + b * B[k]) / z; PA[k] = P[k] - A[k]; PB[k] = P[k] - B[k]; }
+      double s1[3][LD][LD];
+      for (int d = 0; d < 3; ++d) {
+        s1[d][0][0] = 1.0;
+        for (int i = 0; i <= la + 1; ++i)
+          for (int j = 0; j <= lb + 2; ++j) {
+            if (i == 0 && j == 0) continue;
+            double v;
+            if (i > 0) {
+              v = PA[d] * s1[d][i - 1][j];
+              if (i > 1) v += (i - 1) * oo2z * s1[d][i - 2][j];
+              if (j > 0) v += j * oo2z * s1[d][i - 1][j - 1];
+            } else {
+              v = PB[d] * s1[d][0][j - 1];
+              if (j > 1) v += (j - 1) * oo2z * s1[d][0][j - 2];
+            }
+            s1[d][i][j] = v;
+          }
+      }
+      const double pre = Kab * pow(M_PI / z, 1.5);
+      for (int i = 0; i < na; ++i) {
+        const int g = ncart_upto(la - 1) + i;
+        const int ix = c_comp[0][g], iy = c_comp[1][g], iz = c_comp[2][g];
+        for (int j = 0; j < nb; ++j) {
+          const int h = ncart_upto(lb - 1) + j;
+          const int jx = c_comp[0][h], jy = c_comp[1][h], jz = c_comp[2][h];
+          const double Sx = s1[0][ix][jx], Sy = s1[1][iy][jy], Sz = s1[2][iz][jz];
+          auto kin = [&](int d, int i1, int j1) {
+            double v = -2.0 * b * b * s1[d][i1][j1 + 2] + b * (2 * j1 + 1) * s1[d][i1][j1];
+            if (j1 >= 2) v += -0.5 * j1 * (j1 - 1) * s1[d][i1][j1 - 2];
+            return v;
+          };
+          s_c[i * nb + j] += pre * Sx * Sy * Sz;
+          t_c[i * nb + j] += pre * (kin(0, ix, jx) * Sy * Sz + Sx * kin(1, iy, jy) * Sz + Sx * Sy * kin(2, iz, jz));
+        }
+      }
+      for (int at = mi.atom0; at < mi.atom0 + mi.n_atom; ++at) {
+        const double* C = xyz + 3 * at;
+        const double PC[3] = {P[0] - C[0], P[1] - C[1], P[2] - C[2]};
+        const double x = z * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
+        double u[3], w[3];
+        if (nroot == 1) rys_eval_n<1>(x, u, w);
+        else if (nroot == 2) rys_eval_n<2>(x, u, w);
+        else rys_eval_n<3>(x, u, w);
+        const double pv = -Z[at] * 2.0 * M_PI / z * Kab;
+        for (int r = 0; r < nroot; ++r) {
+          double tab[3][3][3];
+          for (int d = 0; d < 3; ++d) {
+            const double c0 = PA[d] - u[r] * PC[d], bb = (1.0 - u[r]) * oo2z;
+            double g[5], h[5][3];
+            g[0] = 1.0;
+            const int L = la + lb;
+            if (L >= 1) g[1] = c0;
+            for (int e = 1; e < L; ++e) g[e + 1] = c0 * g[e] + e * bb * g[e - 1];
+            for (int e = 0; e <= L; ++e) h[e][0] = g[e];
+            for (int j = 1; j <= lb; ++j)
+              for (int e = 0; e <= L - j; ++e) h[e][j] = h[e + 1][j - 1] + AB[d] * h[e][j - 1];
+            for (int i = 0; i <= la; ++i)
+              for (int j = 0; j <= lb; ++j) tab[d][i][j] = h[i][j];
+          }
+          const double wv = pv * w[r];
+          for (int i = 0; i < na; ++i) {
+            const int g2 = ncart_upto(la - 1) + i;
+            for (int j = 0; j < nb; ++j) {
+              const int h2 = ncart_upto(lb - 1) + j;
+              v_c[i * nb + j] += wv * tab[0][c_comp[0][g2]][c_comp[0][h2]] * tab[1][c_comp[1][g2]][c_comp[1][h2]] * tab[2][c_comp[2][g2]][c_comp[2][h2]];
+            }
+          }
+        }
+      }
+    }
+  const int oa = shell_cart[sa], ob = shell_cart[sb];
+  for (int i = 0; i < na; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const size_t p = (size_t)(oa + i) * n_cart + ob + j, q = (size_t)(ob + j) * n_cart + oa + i;
+      S[p] = S[q] = s_c[i * nb + j];
+      T[p] = T[q] = t_c[i * nb + j];
+      V[p] = V[q] = v_c[i * nb + j];
+    }
+}
+
+// Cartesian symmetric matrices -> Tonto basis (column-major), no folding, for
+// every molecule of the batch.
+__global__ void k_cart_to_basis(BatchArgs bt, const double* __restrict__ Xc, double* __restrict__ X) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= bt.bmat_off[bt.n_mol]) return;
+  const int m = find_mol(bt.bmat_off, bt.n_mol, t);
+  const MolInfo mi = bt.mols[m];
+  const long long r = t - mi.bmat;
+  const int j = (int)(r / mi.n_bf), i = (int)(r % mi.n_bf);
+  const int si = bt.bf_shell[mi.bf0 + i], sj = bt.bf_shell[mi.bf0 + j];
+  const int mi_ = bt.bf_local[mi.bf0 + i], mj = bt.bf_local[mi.bf0 + j];
+  const int li = bt.shell_l[si], lj = bt.shell_l[sj], ci = bt.shell_cart[si], cj = bt.shell_cart[sj];
+  const bool ti = bt.spherical && li >= 2, tj = bt.spherical && lj >= 2;
+  const int ni = ti ? ncart(li) : 1, nj = tj ? ncart(lj) : 1;
+  const double* Xm = Xc + mi.cmat;
+  double s = 0.0;
+  for (int p = 0; p < ni; ++p) {
+    const double up = ti ? c_U[li][p * (2 * li + 1) + mi_] : 1.0;
+    if (up == 0.0) continue;
+    const int cp = ti ? ci + p : ci + mi_;
+    for (int q = 0; q < nj; ++q) {
+      const double uq = tj ? c_U[lj][q * (2 * lj + 1) + mj] : 1.0;
+      if (uq == 0.0) continue;
+      s += up * uq * Xm[(size_t)cp * mi.n_cart + (tj ? cj + q : cj + mj)];
+    }
+  }
+  X[t] = s;
+}
+
+// Single-molecule forms (shell pairs from the triangular index, one Cartesian
+// block) used by the no-allocation entry point.
+__global__ void k_one_electron_single(int n_shell, int n_atom, const double* __restrict__ xyz, const double* __restrict__ Z,
                                const int* __restrict__ shell_atom, const int* __restrict__ shell_l,
                                const int* __restrict__ shell_nprim, const int* __restrict__ shell_poff,
                                const int* __restrict__ shell_cart, const double* __restrict__ exps,
@@ -724,7 +924,7 @@ __global__ void k_one_electron(int n_shell, int n_atom, const double* __restrict
 }
 
 // Cartesian symmetric matrix -> Tonto basis (column-major), no folding.
-__global__ void k_cart_to_basis(int n_bf, int n_cart, const double* __restrict__ Xc, const int* __restrict__ bf_shell,
+__global__ void k_cart_to_basis_single(int n_bf, int n_cart, const double* __restrict__ Xc, const int* __restrict__ bf_shell,
                                 const int* __restrict__ bf_local, const int* __restrict__ shell_l,
                                 const int* __restrict__ shell_cart, int spherical, double* __restrict__ X) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -841,36 +1041,43 @@ struct tf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
-  // basis (host copies)
-  int n_atom = 0, n_shell = 0, n_bf = 0, n_cart = 0, spherical = 0;
+  // molecules (a single-molecule context is a batch of one)
+  int n_mol = 0, spherical = 0;
+  std::vector<tf::MolInfo> mols;
+  std::vector<long long> cmat_off, bmat_off, pmax_off;   // n_mol + 1 prefix offsets
+  std::vector<long long> mol_pair0;                      // first pair of each molecule (n_mol + 1)
+  int n_atom = 0, n_shell = 0, n_cart = 0, n_bf = 0;     // totals
   std::vector<double> xyz;
   std::vector<int> shell_atom, shell_l, shell_nprim, shell_first_bf, shell_poff, shell_cart, shell_nbf;
   std::vector<double> exps, coefs;
-  // pairs
+  // pairs and list units
   long long n_pairs = 0;
   std::vector<tf::PairRec> pairs_h;
-  std::vector<int> cls_n, cls_off;                // per pair class
-  std::vector<int4> cps;                          // class pairs
-  std::vector<int> cp_first_task;                 // first task of each class pair
+  std::vector<int> pair_cls;
+  std::vector<int> cls_n, cls_off;                       // [mol * NPAIRCLS + class]
+  std::vector<tf::CPUnit> units;
+  std::vector<int> unit_group, group_task0;
+  std::vector<int2> group_cls;                           // (bra class, ket class) of each group
   long long n_tasks = 0;
-  int shard_index = 0, shard_count = 1;           // round-robin share of the bra tasks
+  int shard_index = 0, shard_count = 1;                  // round-robin share of the bra tasks
   bool geometry_ready = false;
   // device
+  tf::DBuf<tf::MolInfo> d_mols;
+  tf::DBuf<long long> d_cmat_off, d_bmat_off, d_pmax_off;
   tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax;
   tf::DBuf<int> d_shell_atom, d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
-  tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_cls_n, d_schwarz_ids;
-  tf::DBuf<long long> d_counts;
+  tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_schwarz_ids;
   tf::DBuf<tf::PairRec> d_pairs;
   tf::DBuf<tf::PrimPair> d_prim_full, d_prim_skip;
   tf::DBuf<int2> d_tasks, d_quartets;
-  tf::DBuf<int> d_cp_task0;
-  tf::DBuf<int4> d_cps;
-  tf::DBuf<long long> d_offsets;
+  tf::DBuf<tf::CPUnit> d_units;
+  tf::DBuf<int> d_unit_group, d_group_task0;
+  tf::DBuf<long long> d_counts, d_offsets, d_group_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
   tf::DBuf<unsigned char> d_scan_tmp;
-  std::vector<cudaEvent_t> cls_ev;                // one per class-pair launch boundary
+  std::vector<cudaEvent_t> cls_ev;                       // one per group launch boundary
   std::vector<tf_class_stats> cls_stats;
-  std::vector<double> max_I_tonto;                // per Tonto pair index
+  std::vector<double> max_I_tonto;                       // per molecule, Tonto pair order
   tf_stats stats{};
 };
 
@@ -881,62 +1088,106 @@ static int set_device(tf_ctx* c) {
   return TF_OK;
 }
 
-// Class pairs and bra tasks (class pair, bra position); with sharding, this
-// context keeps every shard_count-th task (Tonto's round-robin parallel do).
+static BatchArgs batch_args(tf_ctx* c) {
+  return BatchArgs{c->d_mols.p,       c->n_mol,          c->d_cmat_off.p,     c->d_bmat_off.p,
+                   c->d_pmax_off.p,   c->d_cart_shell.p, c->d_cart_local.p,   c->d_bf_shell.p,
+                   c->d_bf_local.p,   c->d_shell_l.p,    c->d_shell_first_bf.p, c->d_shell_cart.p,
+                   c->d_shell_nbf.p,  c->spherical};
+}
+
+// gather (start, FP32 start, end) of every group's quartet range
+__global__ void k_group_offsets(int n_groups, const int* __restrict__ group_task0, const long long* __restrict__ offs,
+                                long long* __restrict__ out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_groups) return;
+  const long long t0 = group_task0[g], t1 = group_task0[g + 1];
+  out[3 * g] = offs[t0 * NBUCKET];
+  out[3 * g + 1] = offs[t0 * NBUCKET + (long long)NCOST * (t1 - t0)];
+  out[3 * g + 2] = offs[t1 * NBUCKET];
+}
+
+// Groups (class pairs p1 >= p2) of units (one per molecule having both classes);
+// tasks are (unit, bra position); with sharding this context keeps every
+// shard_count-th task (Tonto's round-robin parallel do).
 static int build_tasks(tf_ctx* c) {
-  c->cps.clear();
-  c->cp_first_task.clear();
+  c->units.clear();
+  c->unit_group.clear();
+  c->group_task0.clear();
+  c->group_cls.clear();
   std::vector<int2> tasks;
-  long long g = 0;
+  long long g_counter = 0;
   for (int p1 = 0; p1 < NPAIRCLS; ++p1)
     for (int p2 = 0; p2 <= p1; ++p2) {
-      if (c->cls_n[p1] == 0 || c->cls_n[p2] == 0) continue;
-      const int cpi = (int)c->cps.size();
-      c->cps.push_back(make_int4(p1, p2, c->cls_off[p1], c->cls_off[p2]));
-      c->cp_first_task.push_back((int)tasks.size());
-      for (int i = 0; i < c->cls_n[p1]; ++i, ++g)
-        if (g % c->shard_count == c->shard_index) tasks.push_back(make_int2(cpi, i));
+      const int g = (int)c->group_cls.size();
+      c->group_cls.push_back(make_int2(p1, p2));
+      c->group_task0.push_back((int)tasks.size());
+      for (int m = 0; m < c->n_mol; ++m) {
+        const int n1 = c->cls_n[m * NPAIRCLS + p1], n2 = c->cls_n[m * NPAIRCLS + p2];
+        if (n1 == 0 || n2 == 0) continue;
+        const int u = (int)c->units.size();
+        c->units.push_back(CPUnit{p1, p2, c->cls_off[m * NPAIRCLS + p1], c->cls_off[m * NPAIRCLS + p2], n2, m});
+        c->unit_group.push_back(g);
+        for (int i = 0; i < n1; ++i, ++g_counter)
+          if (g_counter % c->shard_count == c->shard_index) tasks.push_back(make_int2(u, i));
+      }
     }
-  c->cp_first_task.push_back((int)tasks.size());
+  c->group_task0.push_back((int)tasks.size());
   c->n_tasks = (long long)tasks.size();
-  TF_CUDA(c->d_cps.reserve(std::max<size_t>(c->cps.size(), 1)));
+  const size_t ng = c->group_cls.size();
+  TF_CUDA(c->d_units.reserve(std::max<size_t>(c->units.size(), 1)));
+  TF_CUDA(c->d_unit_group.reserve(std::max<size_t>(c->unit_group.size(), 1)));
+  TF_CUDA(c->d_group_task0.reserve(ng + 1));
+  TF_CUDA(c->d_group_offsets.reserve(3 * ng));
   TF_CUDA(c->d_tasks.reserve(std::max<size_t>(tasks.size(), 1)));
   TF_CUDA(c->d_counts.reserve(tasks.size() * NBUCKET + 1));
   TF_CUDA(c->d_offsets.reserve(tasks.size() * NBUCKET + 1));
-  TF_CUDA(c->d_cp_task0.reserve(c->cp_first_task.size()));
-  TF_CUDA(cudaMemcpyAsync(c->d_cp_task0.p, c->cp_first_task.data(), c->cp_first_task.size() * sizeof(int),
-                          cudaMemcpyHostToDevice, c->stream));
-  if (!c->cps.empty())
-    TF_CUDA(cudaMemcpyAsync(c->d_cps.p, c->cps.data(), c->cps.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+  if (!c->units.empty()) {
+    TF_CUDA(cudaMemcpyAsync(c->d_units.p, c->units.data(), c->units.size() * sizeof(CPUnit), cudaMemcpyHostToDevice,
+                            c->stream));
+    TF_CUDA(cudaMemcpyAsync(c->d_unit_group.p, c->unit_group.data(), c->unit_group.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, c->stream));
+  }
+  TF_CUDA(cudaMemcpyAsync(c->d_group_task0.p, c->group_task0.data(), (ng + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                          c->stream));
   if (!tasks.empty())
     TF_CUDA(cudaMemcpyAsync(c->d_tasks.p, tasks.data(), tasks.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(cudaStreamSynchronize(c->stream));
   return TF_OK;
 }
 
-// Build pair records, run pair prep + Schwarz, sort pairs per class.
+// Build pair records, run pair prep + Schwarz, sort each molecule's pairs per class.
 static int setup_pairs(tf_ctx* c) {
-  const int ns = c->n_shell;
-  c->n_pairs = (long long)ns * (ns + 1) / 2;
-  c->pairs_h.assign(c->n_pairs, PairRec{});
+  c->pairs_h.clear();
+  c->pair_cls.clear();
+  c->mol_pair0.assign(c->n_mol + 1, 0);
   long long full_tot = 0;
-  for (int a = 0; a < ns; ++a)
-    for (int b = 0; b <= a; ++b) {
-      PairRec& p = c->pairs_h[(long long)a * (a + 1) / 2 + b];
-      const bool a_hi = c->shell_l[a] >= c->shell_l[b];
-      p.sh_hi = a_hi ? a : b;
-      p.sh_lo = a_hi ? b : a;
-      p.atom_hi = c->shell_atom[p.sh_hi];
-      p.atom_lo = c->shell_atom[p.sh_lo];
-      p.cart_hi = c->shell_cart[p.sh_hi];
-      p.cart_lo = c->shell_cart[p.sh_lo];
-      p.n_full = c->shell_nprim[a] * c->shell_nprim[b];
-      p.full_off = (int)full_tot;
-      p.skip_off = (int)full_tot;
-      full_tot += p.n_full;
-      p.cls = pair_class(c->shell_l[p.sh_hi], c->shell_l[p.sh_lo]);
-      p.tonto_ab = (int)((long long)a * (a + 1) / 2 + b);
-    }
+  for (int m = 0; m < c->n_mol; ++m) {
+    const MolInfo& mi = c->mols[m];
+    c->mol_pair0[m] = (long long)c->pairs_h.size();
+    for (int la = 0; la < mi.n_shell; ++la)
+      for (int lb = 0; lb <= la; ++lb) {
+        const int a = mi.shell0 + la, b = mi.shell0 + lb;
+        PairRec p{};
+        const bool a_hi = c->shell_l[a] >= c->shell_l[b];
+        p.sh_hi = a_hi ? a : b;
+        p.sh_lo = a_hi ? b : a;
+        p.atom_hi = c->shell_atom[p.sh_hi];
+        p.atom_lo = c->shell_atom[p.sh_lo];
+        p.cart_hi = c->shell_cart[p.sh_hi];
+        p.cart_lo = c->shell_cart[p.sh_lo];
+        p.n_full = c->shell_nprim[a] * c->shell_nprim[b];
+        p.full_off = (int)full_tot;
+        p.skip_off = (int)full_tot;
+        full_tot += p.n_full;
+        p.mol = m;
+        p.tonto_ab = la * (la + 1) / 2 + lb;
+        c->pairs_h.push_back(p);
+        c->pair_cls.push_back(pair_class(c->shell_l[p.sh_hi], c->shell_l[p.sh_lo]));
+      }
+  }
+  c->mol_pair0[c->n_mol] = (long long)c->pairs_h.size();
+  c->n_pairs = (long long)c->pairs_h.size();
+  if (full_tot > 0x7fffffffLL) { set_error("too many primitive pairs"); return TF_EUNSUPPORTED; }
   TF_CUDA(c->d_pairs.reserve(c->n_pairs));
   TF_CUDA(c->d_prim_full.reserve(full_tot));
   TF_CUDA(c->d_prim_skip.reserve(full_tot));
@@ -947,9 +1198,9 @@ static int setup_pairs(tf_ctx* c) {
       (int)c->n_pairs, c->d_pairs.p, c->d_xyz.p, c->d_shell_nprim.p, c->d_shell_poff.p, c->d_exps.p, c->d_coefs.p,
       c->d_prim_full.p, c->d_prim_skip.p, c->opt.eri_primitive_pair_cutoff);
   TF_CUDA(cudaGetLastError());
-  // Schwarz per pair class
+  // Schwarz bounds per pair class
   std::vector<std::vector<int>> by_cls(NPAIRCLS);
-  for (long long p = 0; p < c->n_pairs; ++p) by_cls[c->pairs_h[p].cls].push_back((int)p);
+  for (long long p = 0; p < c->n_pairs; ++p) by_cls[c->pair_cls[p]].push_back((int)p);
   std::vector<int> ids;
   std::vector<int> cls_start(NPAIRCLS + 1, 0);
   for (int k = 0; k < NPAIRCLS; ++k) {
@@ -957,7 +1208,7 @@ static int setup_pairs(tf_ctx* c) {
     ids.insert(ids.end(), by_cls[k].begin(), by_cls[k].end());
   }
   cls_start[NPAIRCLS] = (int)ids.size();
-  TF_CUDA(c->d_schwarz_ids.reserve(ids.size()));
+  TF_CUDA(c->d_schwarz_ids.reserve(std::max<size_t>(ids.size(), 1)));
   TF_CUDA(cudaMemcpyAsync(c->d_schwarz_ids.p, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream));
 #define TF_SCHWARZ(LH, LL)                                                                                 \
@@ -984,26 +1235,30 @@ static int setup_pairs(tf_ctx* c) {
                           c->stream));
   TF_CUDA(cudaStreamSynchronize(c->stream));
   c->max_I_tonto.assign(c->n_pairs, 0.0);
-  for (long long p = 0; p < c->n_pairs; ++p) c->max_I_tonto[c->pairs_h[p].tonto_ab] = c->pairs_h[p].imax;
-  // sort each class by I_max descending (ties: Tonto pair index) -> deterministic
+  for (long long p = 0; p < c->n_pairs; ++p) {
+    const PairRec& pr = c->pairs_h[p];
+    c->max_I_tonto[c->mol_pair0[pr.mol] + pr.tonto_ab] = pr.imax;
+  }
+  // sort each (molecule, class) list by I_max descending (stable: ties keep pair order)
   std::vector<int> sorted;
   std::vector<double> simax;
-  c->cls_n.assign(NPAIRCLS, 0);
-  c->cls_off.assign(NPAIRCLS, 0);
-  for (int k = 0; k < NPAIRCLS; ++k) {
-    auto v = by_cls[k];
+  c->cls_n.assign((size_t)c->n_mol * NPAIRCLS, 0);
+  c->cls_off.assign((size_t)c->n_mol * NPAIRCLS, 0);
+  std::vector<std::vector<int>> lists((size_t)c->n_mol * NPAIRCLS);
+  for (long long p = 0; p < c->n_pairs; ++p)
+    lists[(size_t)c->pairs_h[p].mol * NPAIRCLS + c->pair_cls[p]].push_back((int)p);
+  for (size_t q = 0; q < lists.size(); ++q) {
+    auto& v = lists[q];
     std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return c->pairs_h[x].imax > c->pairs_h[y].imax; });
-    c->cls_off[k] = (int)sorted.size();
-    c->cls_n[k] = (int)v.size();
+    c->cls_off[q] = (int)sorted.size();
+    c->cls_n[q] = (int)v.size();
     for (int p : v) { sorted.push_back(p); simax.push_back(c->pairs_h[p].imax); }
   }
-  TF_CUDA(c->d_sorted.reserve(sorted.size()));
-  TF_CUDA(c->d_sorted_imax.reserve(simax.size()));
-  TF_CUDA(c->d_cls_n.reserve(NPAIRCLS));
+  TF_CUDA(c->d_sorted.reserve(std::max<size_t>(sorted.size(), 1)));
+  TF_CUDA(c->d_sorted_imax.reserve(std::max<size_t>(simax.size(), 1)));
   TF_CUDA(cudaMemcpyAsync(c->d_sorted.p, sorted.data(), sorted.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(cudaMemcpyAsync(c->d_sorted_imax.p, simax.data(), simax.size() * sizeof(double), cudaMemcpyHostToDevice,
                           c->stream));
-  TF_CUDA(cudaMemcpyAsync(c->d_cls_n.p, c->cls_n.data(), NPAIRCLS * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(cudaStreamSynchronize(c->stream));
   int rc = build_tasks(c);
   if (rc) return rc;
@@ -1062,7 +1317,7 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   constexpr int QPB = GroupCfg<LA, LB, LC, LD>::QPW * GROUP_WPB;
   const long long blocks = std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
-  GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.n_cart, a.prim_count};
+  GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count};
   k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
   return TF_OK;
 }
@@ -1087,18 +1342,9 @@ static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStre
     TF_GCASE(2, 1, 1, 1) TF_GCASE(2, 1, 2, 0) TF_GCASE(2, 1, 2, 1)
     TF_GCASE(2, 2, 1, 0) TF_GCASE(2, 2, 1, 1) TF_GCASE(2, 2, 2, 0) TF_GCASE(2, 2, 2, 1) TF_GCASE(2, 2, 2, 2)
 #undef TF_GCASE
-    default: {
-      if (std::max(std::max(la, lb), std::max(lc, ld)) > WL_MAX) {
-        set_error("quartet class not built");
-        return TF_EUNSUPPORTED;
-      }
-      int dev = 0, nsm = 148;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      const long long blocks = std::min<long long>((a.n + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK, (long long)nsm * 16);
-      k_jk_warp<<<(unsigned)blocks, 32 * WARPS_PER_BLOCK, WARPS_PER_BLOCK * W_SMEM * sizeof(double), s>>>(a, la, lb, lc, ld);
-      return TF_OK;
-    }
+    default:
+      set_error("quartet class not built");
+      return TF_EUNSUPPORTED;
   }
 }
 
@@ -1118,30 +1364,27 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
   return npq * per_prim + nq * per_q;
 }
 
+// One J/K build for every molecule of the context: dP, dJ, dK are the
+// concatenated per-molecule n_bf x n_bf (column-major) device blocks.
 static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags) {
   if (!c->geometry_ready) { set_error("no geometry"); return TF_ESTATE; }
   if (flags & ~(TF_JK_MIXED | TF_JK_DELTA | TF_JK_NO_COPYBACK)) { set_error("unknown flags"); return TF_EINVAL; }
   cudaStream_t s = c->stream;
-  const int nc = c->n_cart, nb = c->n_bf, ns = c->n_shell;
   int kernels = 0;
+  const BatchArgs bt = batch_args(c);
   TF_CUDA(cudaEventRecord(c->ev0, s));
-  // density in the Cartesian basis, pair maxima
   {
-    const long long n2 = (long long)nc * nc;
-    k_density_to_cart<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nc, nb, dP, c->d_cart_shell.p, c->d_cart_local.p,
-                                                                   c->d_shell_l.p, c->d_shell_first_bf.p,
-                                                                   c->spherical, c->d_Pc.p);
-    TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, sizeof(unsigned long long), s));
-    const long long s2 = (long long)ns * ns;
-    k_pmax<<<(unsigned)((s2 + 255) / 256), 256, 0, s>>>(ns, nb, dP, c->d_shell_first_bf.p, c->d_shell_nbf.p,
-                                                        c->d_pmax.p, c->d_pglob.p);
+    const long long nc2 = c->cmat_off[c->n_mol], ns2 = c->pmax_off[c->n_mol];
+    k_density_to_cart<<<(unsigned)std::max<long long>(1, (nc2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_Pc.p);
+    TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, c->n_mol * sizeof(unsigned long long), s));
+    k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_pmax.p, c->d_pglob.p);
     kernels += 2;
   }
-  // quartet lists (bucket-sorted per class pair; FP32 buckets last when mixed)
+  // quartet lists (bucket-sorted per class pair over the batch; FP32 buckets last when mixed)
   const bool mixed = (flags & TF_JK_MIXED) != 0;
-  ListArgs la{c->d_tasks.p, c->n_tasks, c->d_cps.p, c->d_cp_task0.p, c->d_cls_n.p, c->d_sorted.p,
-              c->d_sorted_imax.p, c->d_pairs.p, c->d_pmax.p, c->d_pglob.p, ns, c->opt.eri_schwarz_cutoff,
-              mixed ? c->opt.mixed_fp32_cut : 0.0};
+  ListArgs la{c->d_tasks.p,         c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
+              c->d_sorted.p,        c->d_sorted_imax.p, c->d_pairs.p, c->d_mols.p, c->d_pmax.p,
+              c->d_pglob.p,         c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0};
   const long long thr_list = 256;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   const long long nslots = c->n_tasks * NBUCKET;
@@ -1153,47 +1396,39 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   TF_CUDA(cudaMemsetAsync(c->d_counts.p + nslots, 0, sizeof(long long), s));
   TF_CUDA(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1),
                                         s));
-  // per class pair: start, FP32 start, end
-  const size_t ncp = c->cps.size();
-  std::vector<long long> cp_off(ncp + 1), cp_mid(ncp);
-  for (size_t k = 0; k <= ncp; ++k)
-    TF_CUDA(cudaMemcpyAsync(&cp_off[k], c->d_offsets.p + (long long)c->cp_first_task[k] * NBUCKET, sizeof(long long),
-                            cudaMemcpyDeviceToHost, s));
-  for (size_t k = 0; k < ncp; ++k) {
-    const long long t0 = c->cp_first_task[k], nt = c->cp_first_task[k + 1] - t0;
-    TF_CUDA(cudaMemcpyAsync(&cp_mid[k], c->d_offsets.p + t0 * NBUCKET + (long long)NCOST * nt, sizeof(long long),
-                            cudaMemcpyDeviceToHost, s));
-  }
+  const int ng = (int)c->group_cls.size();
+  std::vector<long long> goff(3 * ng);
+  k_group_offsets<<<(ng + 63) / 64, 64, 0, s>>>(ng, c->d_group_task0.p, c->d_offsets.p, c->d_group_offsets.p);
+  TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
   TF_CUDA(cudaStreamSynchronize(s));
-  const long long nq_total = cp_off.back();
-  TF_CUDA(c->d_quartets.reserve(nq_total));
+  const long long nq_total = ng > 0 ? goff[3 * (ng - 1) + 2] : 0;
+  TF_CUDA(c->d_quartets.reserve(std::max<long long>(nq_total, 1)));
   k_quartets<true><<<grid_list, (unsigned)thr_list, 0, s>>>(la, nullptr, c->d_offsets.p, c->d_quartets.p);
   kernels++;
   // ERIs + digestion
-  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, (size_t)nc * nc * sizeof(double), s));
-  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, (size_t)nc * nc * sizeof(double), s));
+  const long long nc2 = c->cmat_off[c->n_mol];
+  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc2 * sizeof(double), s));
+  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nc2 * sizeof(double), s));
   TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
   TF_CUDA(cudaEventRecord(c->ev1, s));
-  double flops = 0.0;
-  long long n_fp32 = 0;
-  std::vector<long long> cp_n(c->cps.size());
-  while (c->cls_ev.size() < c->cps.size() + 1) {
+  while ((int)c->cls_ev.size() < ng + 1) {
     cudaEvent_t e;
     TF_CUDA(cudaEventCreate(&e));
     c->cls_ev.push_back(e);
   }
   TF_CUDA(cudaEventRecord(c->cls_ev[0], s));
-  for (size_t k = 0; k < c->cps.size(); ++k) {
-    const int4 cp = c->cps[k];
+  long long n_fp32 = 0;
+  std::vector<long long> g_n(ng);
+  for (int g = 0; g < ng; ++g) {
     int l1h, l1l, l2h, l2l;
-    class_l(cp.x, l1h, l1l);
-    class_l(cp.y, l2h, l2l);
-    JKArgs a{c->d_quartets.p + cp_off[k], cp_mid[k] - cp_off[k], c->d_pairs.p, c->d_prim_full.p,
-             c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, nc, c->d_prim_count.p};
+    class_l(c->group_cls[g].x, l1h, l1l);
+    class_l(c->group_cls[g].y, l2h, l2l);
+    JKArgs a{c->d_quartets.p + goff[3 * g], goff[3 * g + 1] - goff[3 * g], c->d_pairs.p, c->d_prim_full.p,
+             c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p, c->d_prim_count.p};
     JKArgs a32 = a;
-    a32.quartets = c->d_quartets.p + cp_mid[k];
-    a32.n = cp_off[k + 1] - cp_mid[k];
-    cp_n[k] = a.n + a32.n;
+    a32.quartets = c->d_quartets.p + goff[3 * g + 1];
+    a32.n = goff[3 * g + 2] - goff[3 * g + 1];
+    g_n[g] = a.n + a32.n;
     n_fp32 += a32.n;
     if (a.n > 0) {
       int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
@@ -1205,15 +1440,13 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       if (rc != TF_OK) return rc;
       kernels++;
     }
-    TF_CUDA(cudaEventRecord(c->cls_ev[k + 1], s));
+    TF_CUDA(cudaEventRecord(c->cls_ev[g + 1], s));
   }
   TF_CUDA(cudaGetLastError());
   TF_CUDA(cudaEventRecord(c->ev2, s));
   {
-    const long long n2 = (long long)nb * nb;
-    k_finalize<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, c->d_Jc.p, c->d_Kc.p, c->d_bf_shell.p,
-                                                            c->d_bf_local.p, c->d_shell_l.p, c->d_shell_cart.p,
-                                                            c->spherical, dJ, dK);
+    const long long nb2 = c->bmat_off[c->n_mol];
+    k_finalize<<<(unsigned)std::max<long long>(1, (nb2 + 255) / 256), 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK);
     kernels++;
   }
   TF_CUDA(cudaGetLastError());
@@ -1221,25 +1454,24 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   TF_CUDA(cudaMemcpyAsync(pc.data(), c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   TF_CUDA(cudaStreamSynchronize(s));
   float ms_all = 0.f, ms_eri = 0.f;
-  // ev0..ev2 spans the list building and the ERIs; the finalize kernel is small
   TF_CUDA(cudaEventElapsedTime(&ms_eri, c->ev1, c->ev2));
   TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
-  double npq = 0.0;
+  double npq = 0.0, flops = 0.0;
   c->cls_stats.clear();
-  for (size_t k = 0; k < c->cps.size(); ++k) {
-    const int4 cp = c->cps[k];
+  for (int g = 0; g < ng; ++g) {
+    if (g_n[g] == 0) continue;
     int l1h, l1l, l2h, l2l;
-    class_l(cp.x, l1h, l1l);
-    class_l(cp.y, l2h, l2l);
+    class_l(c->group_cls[g].x, l1h, l1l);
+    class_l(c->group_cls[g].y, l2h, l2l);
     const double p = (double)pc[qclass_id(l1h, l1l, l2h, l2l)];
     npq += p;
-    const double fl = class_flops(l1h, l1l, l2h, l2l, (double)cp_n[k], p);
+    const double fl = class_flops(l1h, l1l, l2h, l2l, (double)g_n[g], p);
     flops += fl;
     float ms = 0.f;
-    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[k], c->cls_ev[k + 1]));
+    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[g], c->cls_ev[g + 1]));
     tf_class_stats cs;
     cs.l[0] = l1h; cs.l[1] = l1l; cs.l[2] = l2h; cs.l[3] = l2l;
-    cs.quartets = (double)cp_n[k];
+    cs.quartets = (double)g_n[g];
     cs.prim_quartets = p;
     cs.flops = fl;
     cs.ms = ms;
@@ -1252,6 +1484,139 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   c->stats.prim_quartets = npq;
   c->stats.flops = flops;
   c->stats.kernels = kernels;
+  return TF_OK;
+}
+
+static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, tf_ctx** out) {
+  if (!bases || !out || n_mol <= 0) { set_error("null argument"); return TF_EINVAL; }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { set_error("no CUDA device"); return TF_ENODEVICE; }
+  tf_ctx* c = new tf_ctx();
+  if (opt) c->opt = *opt; else tf_default_options(&c->opt);
+  c->device = c->opt.device;
+  if (c->device < 0 || c->device >= ndev) { delete c; set_error("bad device ordinal"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) { delete c; return rc; }
+  c->n_mol = n_mol;
+  c->spherical = bases[0].is_spherical ? 1 : 0;
+  std::vector<int> cart_shell, cart_local, bf_shell, bf_local;
+  c->cmat_off.assign(n_mol + 1, 0);
+  c->bmat_off.assign(n_mol + 1, 0);
+  c->pmax_off.assign(n_mol + 1, 0);
+  for (int m = 0; m < n_mol; ++m) {
+    const tf_basis* B = bases + m;
+    if (B->n_atom <= 0 || B->n_shell <= 0 || !B->xyz || !B->shell_atom || !B->shell_l || !B->shell_nprim ||
+        !B->shell_first_bf || !B->exponents || !B->coefficients) {
+      delete c; set_error("incomplete basis description"); return TF_EINVAL;
+    }
+    if ((B->is_spherical ? 1 : 0) != c->spherical) {
+      delete c; set_error("all molecules of a batch must use the same basis kind"); return TF_EINVAL;
+    }
+    MolInfo mi{};
+    mi.shell0 = c->n_shell;
+    mi.n_shell = B->n_shell;
+    mi.cart0 = c->n_cart;
+    mi.bf0 = c->n_bf;
+    mi.atom0 = c->n_atom;
+    mi.n_atom = B->n_atom;
+    int np = 0, nc = 0, nb = 0;
+    for (int s = 0; s < B->n_shell; ++s) {
+      const int l = B->shell_l[s];
+      if (l < 0 || l > LMAX_SUPPORTED) { delete c; set_error("angular momentum beyond d not built"); return TF_EUNSUPPORTED; }
+      if (B->shell_atom[s] < 0 || B->shell_atom[s] >= B->n_atom || B->shell_nprim[s] <= 0) {
+        delete c; set_error("bad shell record"); return TF_EINVAL;
+      }
+      if (B->shell_first_bf[s] != nb) { delete c; set_error("shell_first_bf not contiguous"); return TF_EINVAL; }
+      c->shell_atom.push_back(mi.atom0 + B->shell_atom[s]);
+      c->shell_l.push_back(l);
+      c->shell_nprim.push_back(B->shell_nprim[s]);
+      c->shell_first_bf.push_back(nb);
+      c->shell_poff.push_back((int)c->exps.size() + np);
+      c->shell_cart.push_back(nc);
+      const int nbf_s = (c->spherical && l >= 2) ? 2 * l + 1 : ncart(l);
+      c->shell_nbf.push_back(nbf_s);
+      for (int i = 0; i < ncart(l); ++i) { cart_shell.push_back(mi.shell0 + s); cart_local.push_back(i); }
+      for (int i = 0; i < nbf_s; ++i) { bf_shell.push_back(mi.shell0 + s); bf_local.push_back(i); }
+      np += B->shell_nprim[s];
+      nc += ncart(l);
+      nb += nbf_s;
+    }
+    c->exps.insert(c->exps.end(), B->exponents, B->exponents + np);
+    c->coefs.insert(c->coefs.end(), B->coefficients, B->coefficients + np);
+    c->xyz.insert(c->xyz.end(), B->xyz, B->xyz + 3 * B->n_atom);
+    mi.n_cart = nc;
+    mi.n_bf = nb;
+    mi.cmat = c->cmat_off[m];
+    mi.bmat = c->bmat_off[m];
+    mi.pmax = c->pmax_off[m];
+    c->cmat_off[m + 1] = c->cmat_off[m] + (long long)nc * nc;
+    c->bmat_off[m + 1] = c->bmat_off[m] + (long long)nb * nb;
+    c->pmax_off[m + 1] = c->pmax_off[m] + (long long)B->n_shell * B->n_shell;
+    c->mols.push_back(mi);
+    c->n_shell += B->n_shell;
+    c->n_cart += nc;
+    c->n_bf += nb;
+    c->n_atom += B->n_atom;
+  }
+  if (c->cmat_off[n_mol] > (1LL << 36)) { delete c; set_error("batch too large"); return TF_EUNSUPPORTED; }
+  {
+    if (cudaMemcpyToSymbol(c_U, g_tables.U, sizeof(g_tables.U)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_comp, g_tables.comp, sizeof(g_tables.comp)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_cidx, g_tables.cidx, sizeof(g_tables.cidx)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_gcomp, g_tables.comp, sizeof(g_tables.comp)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_gidx, g_tables.cidx, sizeof(g_tables.cidx)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_jk_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_schwarz_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess) {
+      delete c; set_error("constant upload"); return TF_ECUDA;
+    }
+  }
+#define TF_TRY(x)                               \
+  do {                                          \
+    int r__ = (x);                              \
+    if (r__) { tf_ctx_destroy(c); return r__; } \
+  } while (0)
+  auto up = [&](auto& buf, const auto& v) -> int {
+    if (buf.reserve(std::max<size_t>(v.size(), 1)) != cudaSuccess) { set_error("device allocation"); return TF_ENOMEM; }
+    if (!v.empty() && cudaMemcpy(buf.p, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("upload"); return TF_ECUDA;
+    }
+    return TF_OK;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->ev2) != cudaSuccess) {
+    tf_ctx_destroy(c); set_error("stream/event creation"); return TF_ECUDA;
+  }
+  TF_TRY(up(c->d_mols, c->mols));
+  TF_TRY(up(c->d_cmat_off, c->cmat_off));
+  TF_TRY(up(c->d_bmat_off, c->bmat_off));
+  TF_TRY(up(c->d_pmax_off, c->pmax_off));
+  TF_TRY(up(c->d_xyz, c->xyz));
+  TF_TRY(up(c->d_exps, c->exps));
+  TF_TRY(up(c->d_coefs, c->coefs));
+  TF_TRY(up(c->d_shell_atom, c->shell_atom));
+  TF_TRY(up(c->d_shell_nprim, c->shell_nprim));
+  TF_TRY(up(c->d_shell_poff, c->shell_poff));
+  TF_TRY(up(c->d_shell_l, c->shell_l));
+  TF_TRY(up(c->d_shell_first_bf, c->shell_first_bf));
+  TF_TRY(up(c->d_shell_nbf, c->shell_nbf));
+  TF_TRY(up(c->d_shell_cart, c->shell_cart));
+  TF_TRY(up(c->d_cart_shell, cart_shell));
+  TF_TRY(up(c->d_cart_local, cart_local));
+  TF_TRY(up(c->d_bf_shell, bf_shell));
+  TF_TRY(up(c->d_bf_local, bf_local));
+  const size_t nb2 = (size_t)c->bmat_off[n_mol], nc2 = (size_t)c->cmat_off[n_mol];
+  if (c->d_P.reserve(nb2) || c->d_J.reserve(nb2) || c->d_K.reserve(nb2) || c->d_H.reserve(nb2) ||
+      c->d_Pc.reserve(nc2) || c->d_Jc.reserve(nc2) || c->d_Kc.reserve(nc2) ||
+      c->d_pmax.reserve((size_t)c->pmax_off[n_mol]) || c->d_pglob.reserve(n_mol) || c->d_prim_count.reserve(NQCLS)) {
+    tf_ctx_destroy(c); set_error("device allocation"); return TF_ENOMEM;
+  }
+  TF_TRY(setup_pairs(c));
+#undef TF_TRY
+  *out = c;
   return TF_OK;
 }
 
@@ -1273,122 +1638,18 @@ int tf_default_options(tf_options* opt) {
 }
 
 int tf_ctx_create(const tf_basis* B, const tf_options* opt, tf_ctx** out) {
-  using namespace tf;
-  if (!B || !out) { set_error("null argument"); return TF_EINVAL; }
-  *out = nullptr;
-  if (B->n_atom <= 0 || B->n_shell <= 0 || !B->xyz || !B->shell_atom || !B->shell_l || !B->shell_nprim ||
-      !B->shell_first_bf || !B->exponents || !B->coefficients) {
-    set_error("incomplete basis description");
-    return TF_EINVAL;
-  }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { set_error("no CUDA device"); return TF_ENODEVICE; }
-  tf_ctx* c = new tf_ctx();
-  if (opt) c->opt = *opt; else tf_default_options(&c->opt);
-  c->device = c->opt.device;
-  if (c->device < 0 || c->device >= ndev) { delete c; set_error("bad device ordinal"); return TF_EINVAL; }
-  int rc = set_device(c);
-  if (rc) { delete c; return rc; }
-  c->n_atom = B->n_atom;
-  c->n_shell = B->n_shell;
-  c->spherical = B->is_spherical ? 1 : 0;
-  c->xyz.assign(B->xyz, B->xyz + 3 * B->n_atom);
-  c->shell_atom.assign(B->shell_atom, B->shell_atom + B->n_shell);
-  c->shell_l.assign(B->shell_l, B->shell_l + B->n_shell);
-  c->shell_nprim.assign(B->shell_nprim, B->shell_nprim + B->n_shell);
-  c->shell_first_bf.assign(B->shell_first_bf, B->shell_first_bf + B->n_shell);
-  int np = 0, ncart_tot = 0, nbf = 0;
-  for (int s = 0; s < B->n_shell; ++s) {
-    const int l = c->shell_l[s];
-    if (l < 0 || l > LMAX_SUPPORTED) { delete c; set_error("angular momentum beyond d not built"); return TF_EUNSUPPORTED; }
-    if (c->shell_atom[s] < 0 || c->shell_atom[s] >= B->n_atom || c->shell_nprim[s] <= 0) {
-      delete c; set_error("bad shell record"); return TF_EINVAL;
-    }
-    c->shell_poff.push_back(np);
-    np += c->shell_nprim[s];
-    c->shell_cart.push_back(ncart_tot);
-    ncart_tot += ncart(l);
-    const int nbf_s = (c->spherical && l >= 2) ? 2 * l + 1 : ncart(l);
-    c->shell_nbf.push_back(nbf_s);
-    if (c->shell_first_bf[s] != nbf) { delete c; set_error("shell_first_bf not contiguous"); return TF_EINVAL; }
-    nbf += nbf_s;
-  }
-  c->n_bf = nbf;
-  c->n_cart = ncart_tot;
-  c->exps.assign(B->exponents, B->exponents + np);
-  c->coefs.assign(B->coefficients, B->coefficients + np);
-  std::vector<int> cart_shell, cart_local, bf_shell, bf_local;
-  for (int s = 0; s < B->n_shell; ++s) {
-    for (int i = 0; i < ncart(c->shell_l[s]); ++i) { cart_shell.push_back(s); cart_local.push_back(i); }
-    for (int i = 0; i < c->shell_nbf[s]; ++i) { bf_shell.push_back(s); bf_local.push_back(i); }
-  }
-  // spherical matrices
-  {
-    double U[4][70];
-    std::memset(U, 0, sizeof(U));
-    for (int l = 0; l <= 3; ++l) {
-      std::vector<double> m = spherical_matrix(l);
-      std::copy(m.begin(), m.end(), U[l]);
-    }
-    unsigned char comp[3][NCOMP_ALL];
-    unsigned char cidx[LCOMP + 1][LCOMP + 1][LCOMP + 1];
-    std::memset(cidx, 0, sizeof(cidx));
-    for (int g = 0; g < NCOMP_ALL; ++g) {
-      comp[0][g] = (unsigned char)CT.x[g]; comp[1][g] = (unsigned char)CT.y[g]; comp[2][g] = (unsigned char)CT.z[g];
-      cidx[CT.x[g]][CT.y[g]][CT.z[g]] = (unsigned char)CT.idx[CT.x[g]][CT.y[g]][CT.z[g]];
-    }
-    if (cudaMemcpyToSymbol(c_U, U, sizeof(U)) != cudaSuccess || cudaMemcpyToSymbol(c_comp, comp, sizeof(comp)) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_gcomp, comp, sizeof(comp)) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_gidx, cidx, sizeof(cidx)) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_cidx, cidx, sizeof(cidx)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_jk_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_schwarz_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess) {
-      delete c; set_error("constant upload"); return TF_ECUDA;
-    }
-  }
-#define TF_TRY(x)                 \
-  do {                            \
-    int r__ = (x);                \
-    if (r__) { tf_ctx_destroy(c); return r__; } \
-  } while (0)
-  auto up = [&](auto& buf, const auto& v) -> int {
-    if (buf.reserve(v.size()) != cudaSuccess) { set_error("device allocation"); return TF_ENOMEM; }
-    if (cudaMemcpy(buf.p, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice) != cudaSuccess) {
-      set_error("upload"); return TF_ECUDA;
-    }
-    return TF_OK;
-  };
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev2) != cudaSuccess) {
-    tf_ctx_destroy(c); set_error("stream/event creation"); return TF_ECUDA;
-  }
-  TF_TRY(up(c->d_xyz, c->xyz));
-  TF_TRY(up(c->d_exps, c->exps));
-  TF_TRY(up(c->d_coefs, c->coefs));
-  TF_TRY(up(c->d_shell_nprim, c->shell_nprim));
-  TF_TRY(up(c->d_shell_atom, c->shell_atom));
-  TF_TRY(up(c->d_shell_poff, c->shell_poff));
-  TF_TRY(up(c->d_shell_l, c->shell_l));
-  TF_TRY(up(c->d_shell_first_bf, c->shell_first_bf));
-  TF_TRY(up(c->d_shell_nbf, c->shell_nbf));
-  TF_TRY(up(c->d_shell_cart, c->shell_cart));
-  TF_TRY(up(c->d_cart_shell, cart_shell));
-  TF_TRY(up(c->d_cart_local, cart_local));
-  TF_TRY(up(c->d_bf_shell, bf_shell));
-  TF_TRY(up(c->d_bf_local, bf_local));
-  const size_t nb2 = (size_t)nbf * nbf, nc2 = (size_t)ncart_tot * ncart_tot;
-  if (c->d_P.reserve(nb2) || c->d_J.reserve(nb2) || c->d_K.reserve(nb2) || c->d_H.reserve(nb2) ||
-      c->d_Pc.reserve(nc2) || c->d_Jc.reserve(nc2) || c->d_Kc.reserve(nc2) ||
-      c->d_pmax.reserve((size_t)c->n_shell * c->n_shell) || c->d_pglob.reserve(1) || c->d_prim_count.reserve(NQCLS)) {
-    tf_ctx_destroy(c); set_error("device allocation"); return TF_ENOMEM;
-  }
-  TF_TRY(setup_pairs(c));
-#undef TF_TRY
-  *out = c;
-  return TF_OK;
+  return tf::create_impl(B, 1, opt, out);
+}
+
+int tf_ctx_create_batch(const tf_basis* bases, int n, const tf_options* opt, tf_ctx** out) {
+  return tf::create_impl(bases, n, opt, out);
+}
+
+int tf_batch_info(const tf_ctx* c, int* n_bf_per_mol) {
+  if (!c) return TF_EINVAL;
+  if (n_bf_per_mol)
+    for (int m = 0; m < c->n_mol; ++m) n_bf_per_mol[m] = c->mols[m].n_bf;
+  return c->n_mol;
 }
 
 int tf_set_geometry(tf_ctx* c, const double* xyz) {
@@ -1438,7 +1699,7 @@ int tf_build_jk(tf_ctx* c, const double* P, double* J, double* K, int flags) {
   if (!c || !P || !J || !K) { set_error("null argument"); return TF_EINVAL; }
   int rc = set_device(c);
   if (rc) return rc;
-  const size_t bytes = (size_t)c->n_bf * c->n_bf * sizeof(double);
+  const size_t bytes = (size_t)c->bmat_off[c->n_mol] * sizeof(double);
   TF_CUDA(cudaMemcpyAsync(c->d_P.p, P, bytes, cudaMemcpyHostToDevice, c->stream));
   rc = build_jk_device(c, c->d_P.p, c->d_J.p, c->d_K.p, flags);
   if (rc) return rc;
@@ -1450,12 +1711,37 @@ int tf_build_jk(tf_ctx* c, const double* P, double* J, double* K, int flags) {
   return TF_OK;
 }
 
+int tf_build_jk_batched(tf_ctx* c, const double* const* P, double* const* J, double* const* K, int flags) {
+  using namespace tf;
+  if (!c || !P || !J || !K) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  long long bytes = 0;
+  for (int m = 0; m < c->n_mol; ++m) {
+    if (!P[m] || !J[m] || !K[m]) { set_error("null molecule array"); return TF_EINVAL; }
+    const size_t b = (size_t)c->mols[m].n_bf * c->mols[m].n_bf * sizeof(double);
+    TF_CUDA(cudaMemcpyAsync(c->d_P.p + c->bmat_off[m], P[m], b, cudaMemcpyHostToDevice, c->stream));
+    bytes += (long long)b;
+  }
+  rc = build_jk_device(c, c->d_P.p, c->d_J.p, c->d_K.p, flags);
+  if (rc) return rc;
+  for (int m = 0; m < c->n_mol; ++m) {
+    const size_t b = (size_t)c->mols[m].n_bf * c->mols[m].n_bf * sizeof(double);
+    TF_CUDA(cudaMemcpyAsync(J[m], c->d_J.p + c->bmat_off[m], b, cudaMemcpyDeviceToHost, c->stream));
+    TF_CUDA(cudaMemcpyAsync(K[m], c->d_K.p + c->bmat_off[m], b, cudaMemcpyDeviceToHost, c->stream));
+  }
+  TF_CUDA(cudaStreamSynchronize(c->stream));
+  c->stats.h2d_bytes = bytes;
+  c->stats.d2h_bytes = 2 * bytes;
+  return TF_OK;
+}
+
 int tf_build_fock(tf_ctx* c, const double* P, const double* H, double* F) {
   using namespace tf;
   if (!c || !P || !H || !F) { set_error("null argument"); return TF_EINVAL; }
   int rc = set_device(c);
   if (rc) return rc;
-  const size_t n2 = (size_t)c->n_bf * c->n_bf, bytes = n2 * sizeof(double);
+  const size_t n2 = (size_t)c->bmat_off[c->n_mol], bytes = n2 * sizeof(double);
   TF_CUDA(cudaMemcpyAsync(c->d_P.p, P, bytes, cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(cudaMemcpyAsync(c->d_H.p, H, bytes, cudaMemcpyHostToDevice, c->stream));
   rc = build_jk_device(c, c->d_P.p, c->d_J.p, c->d_K.p, 0);
@@ -1484,26 +1770,23 @@ int tf_one_electron(tf_ctx* c, const double* Z, double* S, double* T, double* V)
   int rc = set_device(c);
   if (rc) return rc;
   cudaStream_t s = c->stream;
-  const int nc = c->n_cart, nb = c->n_bf;
-  DBuf<double> dZ, dS, dT, dV;
+  DBuf<double> dZ;
   TF_CUDA(dZ.reserve(c->n_atom));
   TF_CUDA(cudaMemcpyAsync(dZ.p, Z, c->n_atom * sizeof(double), cudaMemcpyHostToDevice, s));
   // Cartesian blocks into the (reused) Cartesian accumulators, then to the basis
   double* Sc = c->d_Jc.p;
   double* Tc = c->d_Kc.p;
   double* Vc = c->d_Pc.p;
-  const long long npair = (long long)c->n_shell * (c->n_shell + 1) / 2;
-  k_one_electron<<<(unsigned)((npair + 127) / 128), 128, 0, s>>>(
-      c->n_shell, c->n_atom, c->d_xyz.p, dZ.p, c->d_shell_atom.p, c->d_shell_l.p, c->d_shell_nprim.p,
-      c->d_shell_poff.p, c->d_shell_cart.p, c->d_exps.p, c->d_coefs.p, nc, Sc, Tc, Vc);
+  k_one_electron<<<(unsigned)((c->n_pairs + 127) / 128), 128, 0, s>>>(
+      c->n_pairs, c->d_pairs.p, c->d_mols.p, c->d_xyz.p, dZ.p, c->d_shell_atom.p, c->d_shell_l.p,
+      c->d_shell_nprim.p, c->d_shell_poff.p, c->d_shell_cart.p, c->d_exps.p, c->d_coefs.p, Sc, Tc, Vc);
   TF_CUDA(cudaGetLastError());
-  const long long n2 = (long long)nb * nb;
+  const long long n2 = c->bmat_off[c->n_mol];
+  const BatchArgs bt = batch_args(c);
   double* outs[3] = {S, T, V};
   double* ins[3] = {Sc, Tc, Vc};
   for (int k = 0; k < 3; ++k) {
-    k_cart_to_basis<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, ins[k], c->d_bf_shell.p, c->d_bf_local.p,
-                                                                 c->d_shell_l.p, c->d_shell_cart.p, c->spherical,
-                                                                 c->d_J.p);
+    k_cart_to_basis<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(bt, ins[k], c->d_J.p);
     TF_CUDA(cudaMemcpyAsync(outs[k], c->d_J.p, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     TF_CUDA(cudaStreamSynchronize(s));
   }
@@ -1637,14 +1920,14 @@ int tf_one_electron_noalloc(const tf_basis* B, const double* Z, double* dS, doub
   // every Cartesian element of S, T, V is written by the pair kernel (both
   // triangles of every shell-pair block), so nothing needs clearing first
   const long long npair = (long long)B->n_shell * (B->n_shell + 1) / 2;
-  k_one_electron<<<(unsigned)((npair + 127) / 128), 128, 0, s>>>(
+  k_one_electron_single<<<(unsigned)((npair + 127) / 128), 128, 0, s>>>(
       B->n_shell, B->n_atom, sc->xyz, sc->Z, sc->shell_atom, sc->shell_l, sc->shell_nprim, sc->shell_poff,
       sc->shell_cart, sc->exps, sc->coefs, nc, sc->S, sc->T, sc->V);
   const long long n2 = (long long)nb * nb;
   double* outs[3] = {dS, dT, dV};
   double* ins[3] = {sc->S, sc->T, sc->V};
   for (int k = 0; k < 3; ++k)
-    k_cart_to_basis<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, ins[k], sc->bf_shell, sc->bf_local,
+    k_cart_to_basis_single<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, ins[k], sc->bf_shell, sc->bf_local,
                                                                  sc->shell_l, sc->shell_cart,
                                                                  B->is_spherical ? 1 : 0, outs[k]);
   TF_CUDA(cudaGetLastError());

@@ -84,6 +84,9 @@ def load_library(path: Optional[str] = None):
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
     L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
+    L.tf_ctx_create_batch.argtypes = [P(_Basis), i, P(Options), P(vp)]
+    L.tf_batch_info.argtypes = [vp, P(i)]
+    L.tf_build_jk_batched.argtypes = [vp, P(P(d)), P(P(d)), P(P(d)), i]
     L.tf_one_electron.argtypes = [vp, P(d), P(d), P(d), P(d)]
     L.tf_last_stats.argtypes = [vp, P(Stats)]
     L.tf_last_class_stats.argtypes = [vp, P(ClassStats), i]
@@ -114,6 +117,15 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+def _basis_struct(mol: Molecule, keep: list) -> _Basis:
+    sa, sl, sn, sf, ex, co = mol.flat_arrays()
+    xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64)
+    keep += [xyz, sa, sl, sn, sf, ex, co]
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))  # noqa: E731
+    return _Basis(mol.n_atom, _dp(xyz), mol.n_shell, ip(sa), ip(sl), ip(sn), ip(sf), _dp(ex), _dp(co),
+                  int(mol.spherical))
+
+
 class FockBuilder:
     """Direct J/K builder for one molecule on one GPU (C ABI context)."""
 
@@ -121,12 +133,8 @@ class FockBuilder:
                  device: int = 0, mixed_fp32_cut: float = 1e-6, deterministic: bool = False):
         L = load_library()
         self.mol = mol
-        sa, sl, sn, sf, ex, co = mol.flat_arrays()
-        self._arrays = [np.ascontiguousarray(mol.xyz, dtype=np.float64), sa, sl, sn, sf, ex, co]
-        xyz = self._arrays[0]
-        ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))  # noqa: E731
-        self._basis = _Basis(mol.n_atom, _dp(xyz), mol.n_shell, ip(sa), ip(sl), ip(sn), ip(sf), _dp(ex), _dp(co),
-                             int(mol.spherical))
+        self._arrays = []
+        self._basis = _basis_struct(mol, self._arrays)
         self.options = default_options(eri_schwarz_cutoff=schwarz_cutoff, eri_primitive_pair_cutoff=pair_cutoff,
                                        device=device, mixed_fp32_cut=mixed_fp32_cut,
                                        deterministic=int(deterministic))
@@ -222,3 +230,61 @@ class FockBuilder:
         s = Stats()
         _check(load_library().tf_last_stats(self.h, ctypes.byref(s)))
         return s.as_dict()
+
+
+class BatchFockBuilder(FockBuilder):
+    """J/K builds of many independent molecules in one launch sequence (a batched
+    context).  Device arrays hold the molecules' n_bf x n_bf blocks concatenated."""
+
+    def __init__(self, mols, schwarz_cutoff: float = 1e-9, pair_cutoff: float = 1e-6, device: int = 0,
+                 mixed_fp32_cut: float = 1e-6):
+        L = load_library()
+        self.mols = list(mols)
+        self.mol = self.mols[0]
+        self._arrays = []
+        arr = (_Basis * len(self.mols))(*[_basis_struct(m, self._arrays) for m in self.mols])
+        self._basis = arr
+        self.options = default_options(eri_schwarz_cutoff=schwarz_cutoff, eri_primitive_pair_cutoff=pair_cutoff,
+                                       device=device, mixed_fp32_cut=mixed_fp32_cut)
+        h = ctypes.c_void_p()
+        _check(L.tf_ctx_create_batch(arr, len(self.mols), ctypes.byref(self.options), ctypes.byref(h)))
+        self.h = h
+        nb = (ctypes.c_int * len(self.mols))()
+        L.tf_batch_info(h, nb)
+        self.n_bf_per_mol = [int(v) for v in nb]
+        self.offsets = np.concatenate([[0], np.cumsum([n * n for n in self.n_bf_per_mol])]).astype(np.int64)
+        self.n_bf = L.tf_n_bf(h)
+
+    def make_r_JK_batched(self, Ps, flags: int = TF_JK_FULL):
+        """J, K per molecule from host densities Ps[i] (n_bf_i x n_bf_i)."""
+        n = len(self.mols)
+        Pf = [np.asfortranarray(P, dtype=np.float64) for P in Ps]
+        Js = [np.empty_like(p, order="F") for p in Pf]
+        Ks = [np.empty_like(p, order="F") for p in Pf]
+        arr = lambda lst: (ctypes.POINTER(ctypes.c_double) * n)(*[_dp(a) for a in lst])  # noqa: E731
+        _check(load_library().tf_build_jk_batched(self.h, arr(Pf), arr(Js), arr(Ks), int(flags)))
+        return Js, Ks
+
+    def make_r_JK_device(self, P, J, K, flags: int = TF_JK_FULL, stream=None):
+        """P, J, K: contiguous float64 CUDA tensors of the concatenated blocks."""
+        import torch
+        tot = int(self.offsets[-1])
+        for t in (P, J, K):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == tot):
+                raise ValueError("batched device arrays must be contiguous float64 CUDA of the concatenated size")
+        s = stream if stream is not None else torch.cuda.current_stream(P.device)
+        _check(load_library().tf_build_jk_device(self.h, ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(J.data_ptr()),
+                                                 ctypes.c_void_p(K.data_ptr()), int(flags),
+                                                 ctypes.c_void_p(s.cuda_stream)))
+
+    def one_electron(self):
+        """S, T, V per molecule (lists)."""
+        Z = np.concatenate([np.asarray(m.Z, dtype=np.float64) for m in self.mols])
+        tot = int(self.offsets[-1])
+        S, T, V = np.empty(tot), np.empty(tot), np.empty(tot)
+        _check(load_library().tf_one_electron(self.h, _dp(Z), _dp(S), _dp(T), _dp(V)))
+        out = []
+        for X in (S, T, V):
+            out.append([X[self.offsets[i]:self.offsets[i + 1]].reshape(n, n).T.copy()
+                        for i, n in enumerate(self.n_bf_per_mol)])
+        return out
