@@ -167,18 +167,37 @@ def cpu_sample(mol, P_np, target_s: float):
 def time_to_scf(mol, fb, device):
     """Converged RHF (|dE| < 1e-9, DIIS error < 1e-6) from the core guess: plain FP64
     builds against mixed-precision incremental builds (final cycles full FP64)."""
+    import torch
+    from tonto_b200 import guess as G
+    from tonto_b200 import learned_guess as LG
     from tonto_b200.scf import RHF
     rhf = RHF(mol, schwarz_cutoff=SCHWARZ, device=device, builder=fb)
+    model = LG.MLP.load(device=device)
+    P_mono = model.extra["mono_P_local"]
     out = {}
     ref = None
-    for name, kw in (("fp64", {}), ("mixed_incremental", {"mixed": True, "incremental": True})):
-        r = rhf.run(conv=1e-9, diis_tol=1e-6, **kw)
+    variants = (("fp64_core", "core", {}),
+                ("mixed_incremental_core", "core", {"mixed": True, "incremental": True}),
+                ("fp64_learned", "learned", {}),
+                ("mixed_incremental_learned", "learned", {"mixed": True, "incremental": True}))
+    for name, guess, kw in variants:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        P0 = None
+        fb_guess = None
+        if guess == "learned":
+            P_sup = torch.tensor(G.superposition_guess(mol, P_mono), device=rhf.dev)
+            P0 = torch.tensor(LG.learned_density(mol, model, P_mono), device=rhf.dev)
+            fb_guess = lambda: P_sup  # noqa: E731
+        t_guess = time.perf_counter() - t0
+        r = rhf.run(P0=P0, conv=1e-9, diis_tol=1e-6, fallback=fb_guess, **kw)
         if ref is None:
             ref = r.energy
-        out[name] = {"seconds": round(r.seconds, 4), "iterations": r.iterations, "builds": r.builds,
-                     "energy": r.energy, "energy_error_vs_fp64": r.energy - ref, "converged": r.converged,
-                     "guess": "core"}
-    out["speedup_mixed_incremental"] = out["fp64"]["seconds"] / out["mixed_incremental"]["seconds"]
+        out[name] = {"seconds": round(r.seconds + t_guess, 4), "iterations": r.iterations, "builds": r.builds,
+                     "energy": r.energy, "energy_error_vs_fp64_core": r.energy - ref, "converged": r.converged,
+                     "guess": guess, "fell_back": r.fell_back}
+    base = out["fp64_core"]["seconds"]
+    out["speedup_vs_fp64_core"] = {k: round(base / v["seconds"], 3) for k, v in out.items() if isinstance(v, dict)}
     return out
 
 

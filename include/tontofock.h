@@ -130,6 +130,12 @@ int tf_build_jk_batched(tf_ctx* ctx, const double* const* P, double* const* J, d
 /* New atom positions ([n_atom][3] bohr): rebuilds pair data and Schwarz bounds. */
 int tf_set_geometry(tf_ctx* ctx, const double* xyz);
 
+/* Schwarz x density cutoff for subsequent builds (SCF_DATA ERI_Schwarz_cutoff).
+ * The pair data are unchanged; only which quartets are computed.  An SCF may
+ * use a looser cutoff while far from convergence and tighten it as it converges
+ * (the reference keeps it fixed). */
+int tf_set_schwarz_cutoff(tf_ctx* ctx, double cutoff);
+
 /* Restrict this context's builds to shard `index` of `count`: every count-th bra
  * shell-pair task, as one MPI rank of Tonto's round-robin parallel do
  * (FooToFortran.java:2762-2783, molecule.fock.foo:1274).  The shards' J and K sum

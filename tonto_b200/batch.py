@@ -71,7 +71,7 @@ class BatchRHF:
         return out
 
     def run(self, P0: Optional[List[torch.Tensor]] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
-            max_iter: int = 100, incremental: bool = True, mixed: bool = False, rebuild_every: int = 8,
+            max_iter: int = 100, incremental: bool = True, mixed: bool = False, rebuild_every: int = 16,
             mixed_until: float = 1e-6, fp64_final: int = 2) -> List[SCFResult]:
         nm = len(self.mols)
         torch.cuda.synchronize(self.dev)

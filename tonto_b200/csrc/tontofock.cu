@@ -1663,6 +1663,12 @@ int tf_set_geometry(tf_ctx* c, const double* xyz) {
   return setup_pairs(c);
 }
 
+int tf_set_schwarz_cutoff(tf_ctx* c, double cutoff) {
+  if (!c || !(cutoff > 0.0)) { tf::set_error("bad cutoff"); return TF_EINVAL; }
+  c->opt.eri_schwarz_cutoff = cutoff;
+  return TF_OK;
+}
+
 int tf_set_shard(tf_ctx* c, int index, int count) {
   using namespace tf;
   if (!c || count < 1 || index < 0 || index >= count) { set_error("bad shard"); return TF_EINVAL; }

@@ -81,6 +81,7 @@ def load_library(path: Optional[str] = None):
     L.tf_set_geometry.argtypes = [vp, P(d)]
     L.tf_build_jk.argtypes = [vp, P(d), P(d), P(d), i]
     L.tf_set_shard.argtypes = [vp, i, i]
+    L.tf_set_schwarz_cutoff.argtypes = [vp, d]
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
     L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
@@ -157,6 +158,11 @@ class FockBuilder:
     def set_geometry(self, xyz_bohr: np.ndarray):
         x = np.ascontiguousarray(xyz_bohr, dtype=np.float64)
         _check(load_library().tf_set_geometry(self.h, _dp(x)))
+
+    def set_schwarz_cutoff(self, cutoff: float):
+        """Schwarz x density cutoff of the following builds."""
+        _check(load_library().tf_set_schwarz_cutoff(self.h, float(cutoff)))
+        self.options.eri_schwarz_cutoff = float(cutoff)
 
     def set_shard(self, index: int, count: int):
         """Build only shard ``index`` of ``count`` (round-robin bra tasks); the shards'

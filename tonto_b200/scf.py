@@ -119,8 +119,9 @@ class RHF:
 
     def run(self, P0: Optional[torch.Tensor] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
             max_iter: int = 100, mixed: bool = False, fp64_final: int = 2, incremental: bool = False,
-            rebuild_every: int = 8, guess_name: str = "core", mixed_until: float = 1e-6,
+            rebuild_every: int = 16, guess_name: str = "core", mixed_until: float = 1e-6,
             fallback: Optional[Callable[[], torch.Tensor]] = None, fallback_after: int = 3,
+            shrink: Optional[float] = None, loose_max: float = 1e-9,
             verbose: bool = False) -> SCFResult:
         """Converge from P0 (default: core guess).
 
@@ -134,9 +135,16 @@ class RHF:
 
         ``fallback``: a callable giving a replacement density; used (once) if the DIIS
         error after ``fallback_after`` cycles is not below the first cycle's.
+
+        ``shrink``: in the cheap state, the Schwarz x density cutoff of each build is
+        ``shrink`` times the square of the previous DIIS error, clamped to [the
+        context's cutoff, ``loose_max``], so the bound tightens as the SCF converges
+        while the Fock error it admits stays well below the current error; the final
+        full FP64 builds always use the context's own cutoff.
         """
         torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
+        tight = self.fb.options.eri_schwarz_cutoff
         P = self.core_guess() if P0 is None else P0.to(self.dev, torch.float64).contiguous()
         diis = DIIS(self.diis_keep)
         hist = []
@@ -159,6 +167,13 @@ class RHF:
             else:
                 use_mixed = use_delta = False
             flags = TF_JK_MIXED if use_mixed else TF_JK_FULL
+            if shrink is not None:
+                cut = tight
+                if state == "cheap" and hist:
+                    cut = min(loose_max, max(tight, shrink * hist[-1][3] ** 2))
+                elif state == "cheap":
+                    cut = loose_max
+                self.fb.set_schwarz_cutoff(cut)
             tb = time.perf_counter()
             if use_delta:
                 J, K = self.jk((P - P_prev).contiguous(), flags | TF_JK_DELTA)
@@ -205,6 +220,8 @@ class RHF:
             Fx = diis.extrapolate(F, err)
             P, _, _ = self.density(Fx)
             it += 1
+        if shrink is not None:
+            self.fb.set_schwarz_cutoff(tight)
         torch.cuda.synchronize(self.dev)
         return SCFResult(energy=E, converged=converged, iterations=it, builds=builds,
                          seconds=time.perf_counter() - t0, build_seconds=build_s, P=P, history=hist,
