@@ -136,6 +136,13 @@ int tf_set_geometry(tf_ctx* ctx, const double* xyz);
  * (the reference keeps it fixed). */
 int tf_set_schwarz_cutoff(tf_ctx* ctx, double cutoff);
 
+/* Device memory for the screened quartet lists: a build writes and consumes them
+ * in chunks of whole (la lb|lc ld) class pairs of at most `quartets` entries
+ * (8 bytes each; default 2^30, 8 GiB).  A class pair larger than the budget is
+ * one chunk of its own.  Results do not depend on it beyond summation order.
+ * No reference counterpart (the reference keeps no quartet lists). */
+int tf_set_list_budget(tf_ctx* ctx, long long quartets);
+
 /* Restrict this context's builds to shard `index` of `count`: every count-th bra
  * shell-pair task, as one MPI rank of Tonto's round-robin parallel do
  * (FooToFortran.java:2762-2783, molecule.fock.foo:1274).  The shards' J and K sum

@@ -28,6 +28,15 @@ def test_batched_build_matches_single_builds(cuda_ok, oracle_mod):
     # the batch in mixed precision stays within the FP32 error bound
     Jm, Km = bb.make_r_JK_batched(Ps, TF_JK_MIXED)
     assert max(float(np.max(np.abs(a - b))) for a, b in zip(Jm, Js)) < 1e-8
+    # quartet lists written and consumed in small chunks (many class-pair chunks,
+    # some class pairs alone larger than the budget) give the same J and K
+    total = int(bb.stats()["quartets"])
+    for budget in (total // 7, 1000):
+        bb.set_list_budget(budget)
+        Jc, Kc = bb.make_r_JK_batched(Ps)
+        assert int(bb.stats()["quartets"]) == total
+        for a, b in zip(Jc + Kc, Js + Ks):
+            assert np.max(np.abs(a - b)) < 1e-12
 
 
 @pytest.mark.gpu

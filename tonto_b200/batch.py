@@ -8,12 +8,14 @@ is screened out entirely by the density test).  Diagonalisations are batched ove
 molecules of equal size.  Per molecule the loop is Tonto's usual_SCF with DIIS
 (keep 8), as in ``tonto_b200.scf``: cheap builds until the convergence test first
 passes, then full FP64 builds until it passes again after at least two of them.
+A molecule whose DIIS error after ``fallback_after`` cycles is not below its first
+cycle's restarts (once) from ``fallback(i)``, as in ``tonto_b200.scf``.
 """
 
 from __future__ import annotations
 
 import time
-from typing import List, Optional
+from typing import Callable, List, Optional
 
 import numpy as np
 import torch
@@ -72,7 +74,8 @@ class BatchRHF:
 
     def run(self, P0: Optional[List[torch.Tensor]] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
             max_iter: int = 100, incremental: bool = True, mixed: bool = False, rebuild_every: int = 16,
-            mixed_until: float = 1e-6, fp64_final: int = 2) -> List[SCFResult]:
+            mixed_until: float = 1e-6, fp64_final: int = 2,
+            fallback: Optional[Callable[[int], torch.Tensor]] = None, fallback_after: int = 3) -> List[SCFResult]:
         nm = len(self.mols)
         torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
@@ -88,6 +91,9 @@ class BatchRHF:
         n_final = [0] * nm
         since_full = [0] * nm
         done = [False] * nm
+        fell_back = [False] * nm
+        err_first = [None] * nm
+        cyc = [0] * nm
         hist = [[] for _ in range(nm)]
         E = [float("nan")] * nm
         it = 0
@@ -131,6 +137,17 @@ class BatchRHF:
                 err_n = float(scal[k, 1])
                 dE = float("inf") if E_old[i] is None else E[i] - E_old[i]
                 hist[i].append((it, E[i], dE, err_n, ("mixed" if use_mixed else "fp64") + ("+delta" if kinds[i] else "")))
+                if err_first[i] is None:
+                    err_first[i] = err_n
+                if (fallback is not None and not fell_back[i] and cyc[i] == fallback_after
+                        and err_n >= err_first[i]):
+                    P[i] = fallback(i).to(self.dev, torch.float64)
+                    diis[i].reset()
+                    fell_back[i] = True
+                    E_old[i] = F_prev[i] = P_prev[i] = err_first[i] = None
+                    cyc[i] = 0
+                    continue
+                cyc[i] += 1
                 passed = E_old[i] is not None and abs(dE) < conv and err_n < diis_tol
                 if state[i] == "final" and passed and n_final[i] >= min(fp64_final, it + 1):
                     done[i] = True
@@ -147,4 +164,5 @@ class BatchRHF:
         torch.cuda.synchronize(self.dev)
         secs = time.perf_counter() - t0
         return [SCFResult(energy=E[i], converged=done[i], iterations=len(hist[i]) - 1, builds=builds,
-                          seconds=secs, build_seconds=0.0, P=P[i], history=hist[i]) for i in range(nm)]
+                          seconds=secs, build_seconds=0.0, P=P[i], history=hist[i], fell_back=fell_back[i])
+                for i in range(nm)]

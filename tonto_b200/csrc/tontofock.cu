@@ -242,6 +242,7 @@ struct CPUnit {
 
 struct ListArgs {
   const int2* tasks;            // (unit, bra position)
+  long long t_base;             // tasks [t_base, n_tasks) are processed
   long long n_tasks;
   const CPUnit* units;
   const int* unit_group;        // unit -> group (class pair)
@@ -254,6 +255,7 @@ struct ListArgs {
   const unsigned long long* pglob;   // per molecule
   double cutoff;
   double fp32_cut;              // 0: no FP32 quartets
+  long long out_base;           // list index of out[0] (chunked list writes)
 };
 
 __device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo& mi, const PairRec& b,
@@ -287,7 +289,7 @@ __device__ __forceinline__ long long slot(const ListArgs& a, long long t, int g,
 template <bool WRITE>
 __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const long long* __restrict__ offsets,
                            int2* __restrict__ out) {
-  const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long t = a.t_base + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (t >= a.n_tasks) return;
   const int2 task = a.tasks[t];
@@ -323,7 +325,7 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
     for (int k = 0; k < NBUCKET; ++k) {
       const unsigned m = __ballot_sync(0xffffffffu, ok && bucket == k);
       if (WRITE && ok && bucket == k)
-        out[offsets[slot(a, t, g, k)] + cnt[k] + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
+        out[offsets[slot(a, t, g, k)] - a.out_base + cnt[k] + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
       cnt[k] += __popc(m);
     }
     if (__any_sync(0xffffffffu, beyond)) break;
@@ -1059,6 +1061,7 @@ struct tf_ctx {
   std::vector<int> unit_group, group_task0;
   std::vector<int2> group_cls;                           // (bra class, ket class) of each group
   long long n_tasks = 0;
+  long long list_budget = 1LL << 30;                     // quartets per list chunk (8 B each)
   int shard_index = 0, shard_count = 1;                  // round-robin share of the bra tasks
   bool geometry_ready = false;
   // device
@@ -1075,7 +1078,7 @@ struct tf_ctx {
   tf::DBuf<long long> d_counts, d_offsets, d_group_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
   tf::DBuf<unsigned char> d_scan_tmp;
-  std::vector<cudaEvent_t> cls_ev;                       // one per group launch boundary
+  std::vector<cudaEvent_t> cls_ev;                       // start and end of each group's launches
   std::vector<tf_class_stats> cls_stats;
   std::vector<double> max_I_tonto;                       // per molecule, Tonto pair order
   tf_stats stats{};
@@ -1382,9 +1385,9 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   }
   // quartet lists (bucket-sorted per class pair over the batch; FP32 buckets last when mixed)
   const bool mixed = (flags & TF_JK_MIXED) != 0;
-  ListArgs la{c->d_tasks.p,         c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
-              c->d_sorted.p,        c->d_sorted_imax.p, c->d_pairs.p, c->d_mols.p, c->d_pmax.p,
-              c->d_pglob.p,         c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0};
+  ListArgs la{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
+              c->d_sorted.p,   c->d_sorted_imax.p, c->d_pairs.p,  c->d_mols.p,  c->d_pmax.p,
+              c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0};
   const long long thr_list = 256;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   const long long nslots = c->n_tasks * NBUCKET;
@@ -1402,45 +1405,74 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
   TF_CUDA(cudaStreamSynchronize(s));
   const long long nq_total = ng > 0 ? goff[3 * (ng - 1) + 2] : 0;
-  TF_CUDA(c->d_quartets.reserve(std::max<long long>(nq_total, 1)));
-  k_quartets<true><<<grid_list, (unsigned)thr_list, 0, s>>>(la, nullptr, c->d_offsets.p, c->d_quartets.p);
-  kernels++;
   // ERIs + digestion
   const long long nc2 = c->cmat_off[c->n_mol];
   TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc2 * sizeof(double), s));
   TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nc2 * sizeof(double), s));
   TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
   TF_CUDA(cudaEventRecord(c->ev1, s));
-  while ((int)c->cls_ev.size() < ng + 1) {
+  while ((int)c->cls_ev.size() < 2 * ng) {
     cudaEvent_t e;
     TF_CUDA(cudaEventCreate(&e));
     c->cls_ev.push_back(e);
   }
-  TF_CUDA(cudaEventRecord(c->cls_ev[0], s));
   long long n_fp32 = 0;
   std::vector<long long> g_n(ng);
-  for (int g = 0; g < ng; ++g) {
-    int l1h, l1l, l2h, l2l;
-    class_l(c->group_cls[g].x, l1h, l1l);
-    class_l(c->group_cls[g].y, l2h, l2l);
-    JKArgs a{c->d_quartets.p + goff[3 * g], goff[3 * g + 1] - goff[3 * g], c->d_pairs.p, c->d_prim_full.p,
-             c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p, c->d_prim_count.p};
-    JKArgs a32 = a;
-    a32.quartets = c->d_quartets.p + goff[3 * g + 1];
-    a32.n = goff[3 * g + 2] - goff[3 * g + 1];
-    g_n[g] = a.n + a32.n;
-    n_fp32 += a32.n;
-    if (a.n > 0) {
-      int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
-      if (rc != TF_OK) return rc;
+  // The lists are written and consumed in chunks of whole class pairs, each at
+  // most list_budget quartets (a single larger class pair is one chunk), so a
+  // large batch needs one chunk-sized list buffer rather than the whole list.
+  std::vector<int> chunk{0};
+  long long chunk_max = 1;
+  while (chunk.back() < ng) {
+    const int g0 = chunk.back();
+    int g1 = g0 + 1;
+    while (g1 < ng && goff[3 * g1 + 2] - goff[3 * g0] <= c->list_budget) ++g1;
+    chunk_max = std::max(chunk_max, goff[3 * (g1 - 1) + 2] - goff[3 * g0]);
+    chunk.push_back(g1);
+  }
+  if (c->d_quartets.reserve(chunk_max) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("quartet list chunk does not fit in device memory");
+    return TF_ENOMEM;
+  }
+  for (size_t ci = 0; ci + 1 < chunk.size(); ++ci) {
+    const int g0 = chunk[ci], g1 = chunk[ci + 1];
+    const long long base = goff[3 * g0], nq = goff[3 * (g1 - 1) + 2] - base;
+    if (nq > 0) {
+      ListArgs lw = la;
+      lw.t_base = c->group_task0[g0];
+      lw.n_tasks = c->group_task0[g1];
+      lw.out_base = base;
+      const unsigned grid_w =
+          (unsigned)std::max<long long>(1, ((lw.n_tasks - lw.t_base) * 32 + thr_list - 1) / thr_list);
+      k_quartets<true><<<grid_w, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
       kernels++;
     }
-    if (a32.n > 0) {
-      int rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
-      if (rc != TF_OK) return rc;
-      kernels++;
+    for (int g = g0; g < g1; ++g) {
+      int l1h, l1l, l2h, l2l;
+      class_l(c->group_cls[g].x, l1h, l1l);
+      class_l(c->group_cls[g].y, l2h, l2l);
+      TF_CUDA(cudaEventRecord(c->cls_ev[2 * g], s));
+      JKArgs a{c->d_quartets.p + (goff[3 * g] - base), goff[3 * g + 1] - goff[3 * g], c->d_pairs.p,
+               c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p,
+               c->d_prim_count.p};
+      JKArgs a32 = a;
+      a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
+      a32.n = goff[3 * g + 2] - goff[3 * g + 1];
+      g_n[g] = a.n + a32.n;
+      n_fp32 += a32.n;
+      if (a.n > 0) {
+        int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
+        if (rc != TF_OK) return rc;
+        kernels++;
+      }
+      if (a32.n > 0) {
+        int rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
+        if (rc != TF_OK) return rc;
+        kernels++;
+      }
+      TF_CUDA(cudaEventRecord(c->cls_ev[2 * g + 1], s));
     }
-    TF_CUDA(cudaEventRecord(c->cls_ev[g + 1], s));
   }
   TF_CUDA(cudaGetLastError());
   TF_CUDA(cudaEventRecord(c->ev2, s));
@@ -1453,8 +1485,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   std::vector<unsigned long long> pc(NQCLS);
   TF_CUDA(cudaMemcpyAsync(pc.data(), c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   TF_CUDA(cudaStreamSynchronize(s));
-  float ms_all = 0.f, ms_eri = 0.f;
-  TF_CUDA(cudaEventElapsedTime(&ms_eri, c->ev1, c->ev2));
+  float ms_all = 0.f, ms_eri = 0.f;    // ms_eri: the ERI/digestion launches alone (no list writes)
   TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
   double npq = 0.0, flops = 0.0;
   c->cls_stats.clear();
@@ -1468,7 +1499,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     const double fl = class_flops(l1h, l1l, l2h, l2l, (double)g_n[g], p);
     flops += fl;
     float ms = 0.f;
-    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[g], c->cls_ev[g + 1]));
+    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[2 * g], c->cls_ev[2 * g + 1]));
+    ms_eri += ms;
     tf_class_stats cs;
     cs.l[0] = l1h; cs.l[1] = l1l; cs.l[2] = l2h; cs.l[3] = l2l;
     cs.quartets = (double)g_n[g];
@@ -1666,6 +1698,12 @@ int tf_set_geometry(tf_ctx* c, const double* xyz) {
 int tf_set_schwarz_cutoff(tf_ctx* c, double cutoff) {
   if (!c || !(cutoff > 0.0)) { tf::set_error("bad cutoff"); return TF_EINVAL; }
   c->opt.eri_schwarz_cutoff = cutoff;
+  return TF_OK;
+}
+
+int tf_set_list_budget(tf_ctx* c, long long quartets) {
+  if (!c || quartets <= 0) { tf::set_error("bad list budget"); return TF_EINVAL; }
+  c->list_budget = quartets;
   return TF_OK;
 }
 

@@ -82,6 +82,7 @@ def load_library(path: Optional[str] = None):
     L.tf_build_jk.argtypes = [vp, P(d), P(d), P(d), i]
     L.tf_set_shard.argtypes = [vp, i, i]
     L.tf_set_schwarz_cutoff.argtypes = [vp, d]
+    L.tf_set_list_budget.argtypes = [vp, ctypes.c_longlong]
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
     L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
@@ -163,6 +164,10 @@ class FockBuilder:
         """Schwarz x density cutoff of the following builds."""
         _check(load_library().tf_set_schwarz_cutoff(self.h, float(cutoff)))
         self.options.eri_schwarz_cutoff = float(cutoff)
+
+    def set_list_budget(self, quartets: int):
+        """Largest quartet-list chunk (entries of 8 bytes) a build keeps on the device."""
+        _check(load_library().tf_set_list_budget(self.h, int(quartets)))
 
     def set_shard(self, index: int, count: int):
         """Build only shard ``index`` of ``count`` (round-robin bra tasks); the shards'

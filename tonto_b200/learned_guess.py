@@ -278,3 +278,16 @@ def learned_density(mol: Molecule, model: MLP, P_mono_local: np.ndarray) -> np.n
     X = descriptors(atoms, frames, pairs)
     Y = model.predict(X)
     return assemble(mol, A, pairs, Y, P_mono_local)
+
+
+def learned_densities(mols: List[Molecule], model: MLP, P_mono_local: np.ndarray) -> List[np.ndarray]:
+    """Initial densities of many clusters, one network evaluation over all their pairs."""
+    geo = [cluster_geometry(m) for m in mols]
+    pairs = [pair_list(g[3]) for g in geo]
+    X = np.concatenate([descriptors(g[3], g[1], p) for g, p in zip(geo, pairs)])
+    Y = model.predict(X)
+    out, k = [], 0
+    for m, g, p in zip(mols, geo, pairs):
+        out.append(assemble(m, g[2], p, Y[k:k + len(p)], P_mono_local))
+        k += len(p)
+    return out

@@ -5,6 +5,8 @@
   uniform jitter per coordinate.  Lattice sites are taken from a k x k x k cube
   (k = ceil(n^(1/3))) in (z, y, x) order, so (H2O)_4 fills a 2x2x1 layer and
   (H2O)_32 a 4x4x2 slab.
+* Cluster batch: 256 water clusters with n seeded-uniform in [2, 24] (48-576
+  cc-pVDZ functions), cluster i built with seed 300000 + i.
 * All-trans alkane CnH(2n+2): C-C 1.54 A, C-H 1.09 A, tetrahedral angles, carbon
   zig-zag in the xy plane, seeded +-0.02 A uniform jitter per coordinate.
 """
@@ -52,6 +54,16 @@ def water_cluster_geometry(n: int, seed: int) -> Tuple[List[int], np.ndarray]:
 def water_cluster(n: int, seed: int = 0, basis: str = "cc-pVDZ", spherical: bool = True) -> Molecule:
     Z, xyz = water_cluster_geometry(n, seed)
     return build_molecule(Z, xyz * BOHR_PER_ANGSTROM, basis, spherical=spherical)
+
+
+CLUSTER_BATCH_SIZE_SEED, CLUSTER_BATCH_SEED0 = 3, 300000
+
+
+def cluster_batch(n_mol: int = 256, lo: int = 2, hi: int = 24, spherical: bool = True) -> List[Molecule]:
+    """The batch workload: water clusters with n seeded-uniform in [lo, hi]; the
+    first n_mol of the 256-cluster sequence (cluster i has seed 300000 + i)."""
+    sizes = np.random.default_rng(CLUSTER_BATCH_SIZE_SEED).integers(lo, hi + 1, size=max(256, n_mol))
+    return [water_cluster(int(sizes[i]), seed=CLUSTER_BATCH_SEED0 + i, spherical=spherical) for i in range(n_mol)]
 
 
 def alkane_geometry(n_c: int, seed: int) -> Tuple[List[int], np.ndarray]:
