@@ -327,7 +327,6 @@ def main():
     if world > 1:
         dist.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    cls_acc = {}
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))                 # L2 flush between timed builds (untimed)
@@ -335,14 +334,25 @@ def main():
             step()
             ev[k][1].record(stream)
             torch.cuda.synchronize(dev)
-            for c in fb.class_stats():
-                a = cls_acc.setdefault(c["class"], [0.0, 0.0, 0, 0.0, 0.0])
-                a[0] += c["ms"]
-                a[1] += c["flops"]
-                a[2] += 1
-                a[3] = c["prim_quartets"]
-                a[4] = c["quartets"]
+    graph_builds = bool(fb.stats()["graph"])
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    # per-class device times: builds launched class by class (events between the
+    # launches), outside the timed region
+    cls_acc = {}
+    fb.set_graph(False)
+    for k in range(2):
+        flush.fill_(float(k))
+        fb.make_r_JK_device(P, J, K)
+        torch.cuda.synchronize(dev)
+        for c in fb.class_stats():
+            a = cls_acc.setdefault(c["class"], [0.0, 0.0, 0, 0.0, 0.0])
+            a[0] += c["ms"]
+            a[1] += c["flops"]
+            a[2] += 1
+            a[3] = c["prim_quartets"]
+            a[4] = c["quartets"]
+    st_direct = fb.stats()
+    fb.set_graph(True)
     t_local = sum(step_ms)
     if world > 1:
         tt = torch.tensor([t_local], dtype=torch.float64, device=dev)
@@ -361,7 +371,8 @@ def main():
     roofline = {"bound": "fp64_pipe", "kernel": f"k_jk {dom_cls}", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": (achieved / peak) if peak else None,
                 "traffic": traffic, "peak_source": "measured on this GPU: FP64 FMA loop (tf_peak_fma)",
-                "all_classes_achieved": (st["flops"] / (st["eri_ms"] * 1e-3) / 1e12) if st["eri_ms"] else None}
+                "all_classes_achieved": (st_direct["flops"] / (st_direct["eri_ms"] * 1e-3) / 1e12)
+                if st_direct["eri_ms"] else None}
 
     # e2e through the C ABI with host buffers
     e2e = None
@@ -385,7 +396,8 @@ def main():
             "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(st["kernels"]) * args.steps,
             "e2e": e2e,
             "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"], "flops": st["flops"],
-                      "eri_ms": st["eri_ms"], "build_ms": st["build_ms"]},
+                      "graph": graph_builds, "direct_build_ms": st_direct["build_ms"],
+                      "direct_eri_ms": st_direct["eri_ms"]},
             "classes": {k: {"ms": round(v[0] / v[2], 3), "prim_quartets": v[3], "quartets": v[4],
                             "tflops": round(v[1] / (v[0] * 1e-3) / 1e12, 3) if v[0] > 0 else None}
                         for k, v in sorted(cls_acc.items(), key=lambda kv: -kv[1][0])}}

@@ -88,13 +88,15 @@ typedef struct tf_options {
 
 typedef struct tf_stats {
   double build_ms;                   /* device time of the last build (CUDA events) */
-  double eri_ms;                     /* device time of the ERI + digestion kernels */
+  double eri_ms;                     /* device time of the ERI + digestion kernels (graph builds:
+                                        the whole graph) */
   double quartets;                   /* contracted shell quartets computed */
   double quartets_fp32;              /* of which in FP32 */
   double prim_quartets;              /* primitive quartets computed */
-  double flops;                      /* algorithmic FLOP count of the last build */
+  double flops;                      /* algorithmic FLOP count of the last build (per-class model) */
   long long h2d_bytes, d2h_bytes;    /* host<->device bytes of the last call */
   int kernels;                       /* kernel launches issued by the last build */
+  int graph;                         /* 1: the build replayed a captured CUDA graph */
 } tf_stats;
 
 /* Per quartet-class figures of the last build (one entry per (la lb|lc ld) launch). */
@@ -102,7 +104,7 @@ typedef struct tf_class_stats {
   int l[4];                          /* la >= lb, lc >= ld, pair class (la lb) >= (lc ld) */
   double quartets, prim_quartets;    /* contracted and primitive quartets computed */
   double flops;                      /* algorithmic FLOPs */
-  double ms;                         /* device time of the launch (CUDA events) */
+  double ms;                         /* device time of the launch (CUDA events; 0 for graph builds) */
 } tf_class_stats;
 
 typedef struct tf_ctx tf_ctx;
@@ -142,6 +144,16 @@ int tf_set_schwarz_cutoff(tf_ctx* ctx, double cutoff);
  * one chunk of its own.  Results do not depend on it beyond summation order.
  * No reference counterpart (the reference keeps no quartet lists). */
 int tf_set_list_budget(tf_ctx* ctx, long long quartets);
+
+/* CUDA-graph builds (default on).  After a first build has sized the quartet
+ * list, each build is one captured graph (density transform, screening, list,
+ * every class launch with its quartet range read on the device, Fock
+ * accumulation) with no host round trip inside; it is re-captured when the
+ * density/J/K arrays, the precision flag or the cutoff change, and a build whose
+ * list outgrows the buffer is redone on the direct path.  on = 0: every build
+ * launches class by class after reading the list sizes back.  No reference
+ * counterpart. */
+int tf_set_graph(tf_ctx* ctx, int on);
 
 /* Restrict this context's builds to shard `index` of `count`: every count-th bra
  * shell-pair task, as one MPI rank of Tonto's round-robin parallel do

@@ -23,6 +23,7 @@
 
 #define TF_RYS_CONST __device__ const
 #include "rys_tables.inc"
+#include "boys_table.inc"
 
 namespace tf {
 
@@ -121,6 +122,17 @@ struct __align__(16) PairRec {
   double Rx, Ry, Rz;         // hi centre - lo centre
   double imax;               // Schwarz bound sqrt(max |(ab|ab)|)
 };
+
+// Quartet range of a launch in a graph-captured build: list[range[0] - base,
+// range[1] - base), read on the device and clamped to the list capacity.
+__device__ __forceinline__ void resolve_range(const long long* range, long long base, long long cap,
+                                              const int2*& q, long long& n) {
+  if (range) {
+    const long long s0 = range[0], s1 = min(range[1], base + cap);
+    q += s0 - base;
+    n = s1 > s0 ? s1 - s0 : 0;
+  }
+}
 
 // One molecule of a (possibly batched) context: its shells are a contiguous
 // global range; its matrices sit at fixed offsets in the concatenated buffers.
@@ -229,6 +241,50 @@ struct RysSmem {
   }
 };
 
+// One root: the rule is exact for f linear in t^2, so w = F0(x) and u = F1(x)/F0(x).
+// F0 and F1 come from an 8-term Taylor step about the nearest point k/8 of a grid
+// of F_0..F_8 (gen_boys_table.py; dF_m/dx = -F_{m+1}): five 16-byte table loads
+// per evaluation instead of one per polynomial coefficient.
+template <>
+struct RysSmem<1> {
+  static constexpr int SIZE = TF_BOYS_NPTS * TF_BOYS_NM;
+  static __device__ __forceinline__ void load(double* t) {
+    for (int q = threadIdx.x; q < SIZE; q += blockDim.x) t[q] = tf_boys_grid[q];
+  }
+  static __device__ __forceinline__ void eval(const double* __restrict__ t, double x, double (&u)[1], double (&w)[1]) {
+    static_assert(TF_BOYS_NTERM == 8 && TF_BOYS_NM == 10, "Taylor step written for 8 terms");
+    if (x < (double)TF_BOYS_XMAX) {
+      const int k = (int)(x * (double)TF_BOYS_H_INV + 0.5);
+      const double d = (double)k * (1.0 / TF_BOYS_H_INV) - x;
+      const double2* g = reinterpret_cast<const double2*>(t + k * TF_BOYS_NM);
+      const double2 f01 = g[0], f23 = g[1], f45 = g[2], f67 = g[3], f89 = g[4];
+      const double d2 = d * 0.5, d3 = d * (1.0 / 3.0), d4 = d * 0.25, d5 = d * 0.2, d6 = d * (1.0 / 6.0),
+                   d7 = d * (1.0 / 7.0);
+      double a = fma(d7, f67.y, f67.x);      // F0 = f0 + d (f1 + d/2 (f2 + ... + d/7 f7))
+      double b = fma(d7, f89.x, f67.y);      // F1 = f1 + d (f2 + d/2 (f3 + ... + d/7 f8))
+      a = fma(d6, a, f45.y);
+      b = fma(d6, b, f67.x);
+      a = fma(d5, a, f45.x);
+      b = fma(d5, b, f45.y);
+      a = fma(d4, a, f23.y);
+      b = fma(d4, b, f45.x);
+      a = fma(d3, a, f23.x);
+      b = fma(d3, b, f23.y);
+      a = fma(d2, a, f01.y);
+      b = fma(d2, b, f23.x);
+      a = fma(d, a, f01.x);
+      b = fma(d, b, f01.y);
+      w[0] = a;
+      u[0] = b / a;
+    } else {
+      constexpr int HOFF = rys_hoffset(1);
+      const double ix = 1.0 / x;
+      u[0] = tf_rys_hroot2[HOFF] * ix;
+      w[0] = tf_rys_hweight[HOFF] * sqrt(ix);
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // One contracted shell quartet (LA LB | LC LD), LA >= LB, LC >= LD, in
 // arithmetic type T for the 2D recurrences and (e0|f0) sums (double, or float
@@ -257,6 +313,11 @@ __device__ __forceinline__ double4 ld4(const PrimPair* p, int half) {
 }
 
 // (e0|f0) accumulation over all primitive quartets of a contracted quartet.
+#ifndef TF_PRIM_UNROLL
+#define TF_PRIM_UNROLL 1
+#endif
+constexpr int kPrimUnroll = TF_PRIM_UNROLL;
+
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp, int nbp,
                                                 const PrimPair* __restrict__ kp, int nkp,
@@ -285,6 +346,7 @@ __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp,
     if constexpr (Q::LCD > 0) { kA0 = __ldg(kq + i * PPS + 3); kA1 = __ldg(kq + i * PPS + 4); }
   };
   if (npq > 0) load_ket(0);
+#pragma unroll(kPrimUnroll)
   for (int p = 0; p < npq; ++p) {
     {
       const double2 bP = __ldg(bq + ib * PPS), bZ = __ldg(bq + ib * PPS + 1), bC = __ldg(bq + ib * PPS + 2);

@@ -122,6 +122,8 @@ struct GroupArgs {
   double* K;
   const MolInfo* mols;
   unsigned long long* prim_count;
+  const long long* range;       // graph builds: see resolve_range
+  long long base, cap;
 };
 
 __constant__ unsigned char c_gcomp[3][NCOMP_ALL];
@@ -151,10 +153,13 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
   const int fx = sc.x[gf], fy = sc.y[gf], fz = sc.z[gf];
   const long long nwarps = (long long)gridDim.x * wpb;
   unsigned long long nprim = 0;
-  for (long long base = ((long long)blockIdx.x * wpb + warp) * QPW; base < a.n; base += nwarps * QPW) {
+  const int2* quartets = a.quartets;
+  long long nq = a.n;
+  resolve_range(a.range, a.base, a.cap, quartets, nq);
+  for (long long base = ((long long)blockIdx.x * wpb + warp) * QPW; base < nq; base += nwarps * QPW) {
     const long long t = base + (in_group ? g : 0);
-    const bool act = in_group && t < a.n;
-    const int2 qd = act ? a.quartets[t] : make_int2(0, 0);
+    const bool act = in_group && t < nq;
+    const int2 qd = act ? quartets[t] : make_int2(0, 0);
     const PairRec b = a.pairs[qd.x];
     const PairRec k = a.pairs[qd.y];
     const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||

@@ -247,8 +247,9 @@ struct ListArgs {
   const CPUnit* units;
   const int* unit_group;        // unit -> group (class pair)
   const int* group_task0;       // first task of each group
-  const int* sorted;            // pair ids, grouped by (molecule, class), I_max descending
+  const int* sorted;            // pair ids, grouped by (molecule, class), in I_max bands (see setup_pairs)
   const double* sorted_imax;
+  const double* sorted_bmax;    // largest I_max of the position's band (non-increasing)
   const PairRec* pairs;
   const MolInfo* mols;
   const double* pmax;           // per-molecule n_shell x n_shell blocks
@@ -256,6 +257,7 @@ struct ListArgs {
   double cutoff;
   double fp32_cut;              // 0: no FP32 quartets
   long long out_base;           // list index of out[0] (chunked list writes)
+  long long out_cap;            // entries of out (writes beyond are dropped; the host sees the count)
 };
 
 __device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo& mi, const PairRec& b,
@@ -311,9 +313,9 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
     int ket = 0, bucket = 0;
     if (j < jend) {
       const double Ik = a.sorted_imax[cp.ket_off + j];
-      if (!(Ib * Ik * pg > a.cutoff)) {
-        beyond = true;                           // kets are sorted by I_max: nothing further survives
-      } else {
+      if (!(Ib * a.sorted_bmax[cp.ket_off + j] * pg > a.cutoff)) {
+        beyond = true;                           // bands are in decreasing I_max: nothing further survives
+      } else if (Ib * Ik * pg > a.cutoff) {
         ket = a.sorted[cp.ket_off + j];
         const PairRec k = a.pairs[ket];
         const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
@@ -324,8 +326,10 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
 #pragma unroll
     for (int k = 0; k < NBUCKET; ++k) {
       const unsigned m = __ballot_sync(0xffffffffu, ok && bucket == k);
-      if (WRITE && ok && bucket == k)
-        out[offsets[slot(a, t, g, k)] - a.out_base + cnt[k] + __popc(m & ((1u << lane) - 1u))] = make_int2(bra, ket);
+      if (WRITE && ok && bucket == k) {
+        const long long pos = offsets[slot(a, t, g, k)] - a.out_base + cnt[k] + __popc(m & ((1u << lane) - 1u));
+        if (pos < a.out_cap) out[pos] = make_int2(bra, ket);
+      }
       cnt[k] += __popc(m);
     }
     if (__any_sync(0xffffffffu, beyond)) break;
@@ -349,22 +353,43 @@ struct JKArgs {
   double* K;
   const MolInfo* mols;
   unsigned long long* prim_count;   // per quartet class
+  // graph builds: the launch's quartets are list[range[0] - base, range[1] - base),
+  // range read on the device and clamped to base + cap (quartets = list start)
+  const long long* range;
+  long long base, cap;
 };
 
+
+#ifndef TF_JK_MINB_N1
+#define TF_JK_MINB_N1 5
+#endif
+#ifndef TF_JK_MINB
+#define TF_JK_MINB 1
+#endif
+template <int LA, int LB, int LC, int LD>
+constexpr int jk_min_blocks() {
+  return Quartet<LA, LB, LC, LD>::NROOT == 1 ? TF_JK_MINB_N1 : TF_JK_MINB;
+}
+
 template <int LA, int LB, int LC, int LD, typename T>
-__global__ void __launch_bounds__(128) k_jk(JKArgs a) {
+__global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD>()) k_jk(JKArgs a) {
   using Q = Quartet<LA, LB, LC, LD>;
   using RS = RysSmem<Q::NROOT>;
   extern __shared__ double rys_tab[];
   RS::load(rys_tab);
   __syncthreads();
   unsigned long long nprim = 0;
+  const int2* quartets = a.quartets;
+  long long nq = a.n;
+  resolve_range(a.range, a.base, a.cap, quartets, nq);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long n_pad = (a.n + 31) / 32 * 32;     // whole warps stay in the loop together
+  const long long n_pad = (nq + 31) / 32 * 32;      // whole warps stay in the loop together
+  const int lane = threadIdx.x & 31;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n_pad; t += stride) {
-  const bool active = t < a.n;
-  if (active) {
-    const int2 qd = a.quartets[t];
+    // lanes past the end repeat the last quartet with weight 0, so that whole warps
+    // take part in the warp reductions below
+    const bool active = t < nq;
+    const int2 qd = quartets[active ? t : nq - 1];
     const PairRec b = a.pairs[qd.x];
     const PairRec k = a.pairs[qd.y];
     const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
@@ -373,8 +398,8 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
     const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
     const int nbp = any_same ? b.n_full : b.n_skip;
     const int nkp = any_same ? k.n_full : k.n_skip;
-    nprim += (unsigned long long)nbp * nkp;
-    double f = 1.0;
+    if (active) nprim += (unsigned long long)nbp * nkp;
+    double f = active ? 1.0 : 0.0;
     if (b.sh_hi == b.sh_lo) f *= 0.5;
     if (k.sh_hi == k.sh_lo) f *= 0.5;
     if (qd.x == qd.y) f *= 0.5;
@@ -383,6 +408,9 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
     double I[Q::NA][Q::NB][Q::NC * Q::ND];
     quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I, rys_tab);
 
+    // The lists are bra-major, so the lanes of a warp usually share the bra pair:
+    // then J(ab) is summed over the warp and added once, and P(ab) is a broadcast.
+    const bool uni = __all_sync(0xffffffffu, qd.x == __shfl_sync(0xffffffffu, qd.x, 0));
     const MolInfo mi = a.mols[b.mol];
     const int n = mi.n_cart;
     const double* __restrict__ P = a.P + mi.cmat;
@@ -404,8 +432,16 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         for (int c = 0; c < Q::NC; ++c)
 #pragma unroll
           for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
-        atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, f * s);
+        s *= f;
+        if (uni) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+          if (lane == 0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+        } else if (active) {
+          atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+        }
       }
+    if (active) {
     double Pab[Q::NA][Q::NB];
 #pragma unroll
     for (int ia = 0; ia < Q::NA; ++ia)
@@ -424,6 +460,14 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
       }
     // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
     // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
+    double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
+#pragma unroll
+    for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Pbd[ib][d] = __ldg(P + (size_t)(ob + ib) * n + od + d);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) Pbc[ib][c] = __ldg(P + (size_t)(ob + ib) * n + oc + c);
+    }
 #pragma unroll
     for (int ia = 0; ia < Q::NA; ++ia) {
       double Pad[Q::ND], Pac[Q::NC];
@@ -437,7 +481,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
 #pragma unroll
         for (int ib = 0; ib < Q::NB; ++ib)
 #pragma unroll
-          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
+          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pbd[ib][d];
         atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
       }
 #pragma unroll
@@ -446,7 +490,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
 #pragma unroll
         for (int ib = 0; ib < Q::NB; ++ib)
 #pragma unroll
-          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
+          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pbc[ib][c];
         atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
       }
 #pragma unroll
@@ -467,7 +511,7 @@ __global__ void __launch_bounds__(128) k_jk(JKArgs a) {
         }
       }
     }
-  }
+    }
   }
   // primitive-quartet counter (per class, one atomic per warp)
 #pragma unroll
@@ -1033,6 +1077,31 @@ struct DBuf {
   }
 };
 
+// Per-context host staging in pinned memory (group offsets and primitive counts
+// read back after a build; pinned so that a captured graph can copy into them).
+struct PinnedStage {
+  long long* goff = nullptr;                 // 3 per group
+  unsigned long long* pc = nullptr;          // tf::NQCLS
+  size_t n_goff = 0;
+  ~PinnedStage() {
+    if (goff) cudaFreeHost(goff);
+    if (pc) cudaFreeHost(pc);
+  }
+  cudaError_t reserve(size_t ng3) {
+    if (!pc) {
+      cudaError_t e = cudaMallocHost(&pc, tf::NQCLS * sizeof(unsigned long long));
+      if (e != cudaSuccess) return e;
+    }
+    if (ng3 <= n_goff && goff) return cudaSuccess;
+    if (goff) cudaFreeHost(goff);
+    goff = nullptr;
+    n_goff = 0;
+    cudaError_t e = cudaMallocHost(&goff, std::max<size_t>(ng3, 1) * sizeof(long long));
+    if (e == cudaSuccess) n_goff = std::max<size_t>(ng3, 1);
+    return e;
+  }
+};
+
 }  // namespace tf
 
 // ===========================================================================
@@ -1067,7 +1136,7 @@ struct tf_ctx {
   // device
   tf::DBuf<tf::MolInfo> d_mols;
   tf::DBuf<long long> d_cmat_off, d_bmat_off, d_pmax_off;
-  tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax;
+  tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax, d_sorted_bmax;
   tf::DBuf<int> d_shell_atom, d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
   tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_schwarz_ids;
   tf::DBuf<tf::PairRec> d_pairs;
@@ -1082,9 +1151,27 @@ struct tf_ctx {
   std::vector<tf_class_stats> cls_stats;
   std::vector<double> max_I_tonto;                       // per molecule, Tonto pair order
   tf_stats stats{};
+  // graph builds
+  bool use_graph = true;
+  long long graph_cap = 0;                               // list entries a captured build may use
+  cudaGraphExec_t graph_exec = nullptr;
+  const double* graph_key_P = nullptr;
+  double* graph_key_J = nullptr;
+  double* graph_key_K = nullptr;
+  bool graph_key_mixed = false;
+  double graph_key_cutoff = 0.0;
+  int graph_kernels = 0;
+  tf::PinnedStage pin_obj;
+  tf::PinnedStage* pin = &pin_obj;
 };
 
 namespace tf {
+
+static void drop_graph(tf_ctx* c) {
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  c->graph_exec = nullptr;
+  c->graph_key_P = nullptr;
+}
 
 static int set_device(tf_ctx* c) {
   TF_CUDA(cudaSetDevice(c->device));
@@ -1113,6 +1200,7 @@ __global__ void k_group_offsets(int n_groups, const int* __restrict__ group_task
 // tasks are (unit, bra position); with sharding this context keeps every
 // shard_count-th task (Tonto's round-robin parallel do).
 static int build_tasks(tf_ctx* c) {
+  drop_graph(c);                       // captured launches hold the old task arrays and grid sizes
   c->units.clear();
   c->unit_group.clear();
   c->group_task0.clear();
@@ -1160,6 +1248,7 @@ static int build_tasks(tf_ctx* c) {
 
 // Build pair records, run pair prep + Schwarz, sort each molecule's pairs per class.
 static int setup_pairs(tf_ctx* c) {
+  drop_graph(c);
   c->pairs_h.clear();
   c->pair_cls.clear();
   c->mol_pair0.assign(c->n_mol + 1, 0);
@@ -1242,25 +1331,44 @@ static int setup_pairs(tf_ctx* c) {
     const PairRec& pr = c->pairs_h[p];
     c->max_I_tonto[c->mol_pair0[pr.mol] + pr.tonto_ab] = pr.imax;
   }
-  // sort each (molecule, class) list by I_max descending (stable: ties keep pair order)
+  // Order each (molecule, class) list by I_max band (half decades, largest first)
+  // and by pair id inside a band.  The list kernels stop a bra's ket scan at the
+  // first band whose largest I_max fails the screen, and the pair-id order inside a
+  // band puts neighbouring shells on neighbouring lanes, so the ERI kernels' pair,
+  // primitive, density and Fock accesses of a warp fall on few cache lines.
   std::vector<int> sorted;
-  std::vector<double> simax;
+  std::vector<double> simax, sbmax;
   c->cls_n.assign((size_t)c->n_mol * NPAIRCLS, 0);
   c->cls_off.assign((size_t)c->n_mol * NPAIRCLS, 0);
   std::vector<std::vector<int>> lists((size_t)c->n_mol * NPAIRCLS);
   for (long long p = 0; p < c->n_pairs; ++p)
     lists[(size_t)c->pairs_h[p].mol * NPAIRCLS + c->pair_cls[p]].push_back((int)p);
+  auto band = [&](int p) {
+    const double v = c->pairs_h[p].imax;
+    return v > 0.0 ? (int)std::floor(2.0 * std::log10(v)) : -1000000;
+  };
   for (size_t q = 0; q < lists.size(); ++q) {
     auto& v = lists[q];
-    std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return c->pairs_h[x].imax > c->pairs_h[y].imax; });
+    std::sort(v.begin(), v.end(), [&](int x, int y) {
+      const int bx = band(x), by = band(y);
+      return bx != by ? bx > by : x < y;
+    });
     c->cls_off[q] = (int)sorted.size();
     c->cls_n[q] = (int)v.size();
-    for (int p : v) { sorted.push_back(p); simax.push_back(c->pairs_h[p].imax); }
+    for (size_t i = 0; i < v.size();) {
+      size_t e = i;
+      double bm = 0.0;
+      while (e < v.size() && band(v[e]) == band(v[i])) bm = std::max(bm, c->pairs_h[v[e++]].imax);
+      for (; i < e; ++i) { sorted.push_back(v[i]); simax.push_back(c->pairs_h[v[i]].imax); sbmax.push_back(bm); }
+    }
   }
   TF_CUDA(c->d_sorted.reserve(std::max<size_t>(sorted.size(), 1)));
   TF_CUDA(c->d_sorted_imax.reserve(std::max<size_t>(simax.size(), 1)));
+  TF_CUDA(c->d_sorted_bmax.reserve(std::max<size_t>(sbmax.size(), 1)));
   TF_CUDA(cudaMemcpyAsync(c->d_sorted.p, sorted.data(), sorted.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(cudaMemcpyAsync(c->d_sorted_imax.p, simax.data(), simax.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          c->stream));
+  TF_CUDA(cudaMemcpyAsync(c->d_sorted_bmax.p, sbmax.data(), sbmax.size() * sizeof(double), cudaMemcpyHostToDevice,
                           c->stream));
   TF_CUDA(cudaStreamSynchronize(c->stream));
   int rc = build_tasks(c);
@@ -1276,6 +1384,8 @@ static void class_l(int k, int& lh, int& ll) {
   ll = k - lh * (lh + 1) / 2;
 }
 
+// Launch set-up (shared-memory attribute, resident blocks per SM), done once per
+// kernel and before any graph capture: a zero-sized, range-less JKArgs only sets up.
 template <int LA, int LB, int LC, int LD, typename T>
 static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
@@ -1285,17 +1395,18 @@ static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T>, 128, smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
+  if (a.n <= 0 && !a.range) return;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int thr = 128;
-  const long long blocks = std::min<long long>((a.n + thr - 1) / thr, (long long)nsm * blocks_per_sm);
+  const long long full = (long long)nsm * blocks_per_sm;
+  const long long blocks = a.range ? full : std::min<long long>((a.n + thr - 1) / thr, full);
   k_jk<LA, LB, LC, LD, T><<<(unsigned)blocks, thr, smem, s>>>(a);
 }
 
 template <int LA, int LB, int LC, int LD>
 static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32) {
-  if (a.n <= 0) return;
   if (fp32) launch_jk_t<LA, LB, LC, LD, float>(a, s);
   else launch_jk_t<LA, LB, LC, LD, double>(a, s);
 }
@@ -1304,7 +1415,6 @@ constexpr int GROUP_WPB = 4;
 
 template <int LA, int LB, int LC, int LD>
 static int launch_group(const JKArgs& a, cudaStream_t s) {
-  if (a.n <= 0) return TF_OK;
   constexpr size_t smem = group_smem_bytes<LA, LB, LC, LD>(GROUP_WPB);
   static bool attr = false;
   if (!attr) {
@@ -1319,8 +1429,17 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   constexpr int QPB = GroupCfg<LA, LB, LC, LD>::QPW * GROUP_WPB;
-  const long long blocks = std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
-  GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count};
+  static int group_blocks_per_sm = -1;
+  if (group_blocks_per_sm < 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group_blocks_per_sm, k_jk_group<LA, LB, LC, LD>, 32 * GROUP_WPB,
+                                                  smem);
+    if (group_blocks_per_sm < 1) group_blocks_per_sm = 1;
+  }
+  if (a.n <= 0 && !a.range) return TF_OK;
+  const long long full = (long long)nsm * group_blocks_per_sm;
+  const long long blocks = a.range ? full : std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
+  GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count,
+              a.range, a.base, a.cap};
   k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
   return TF_OK;
 }
@@ -1367,27 +1486,20 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
   return npq * per_prim + nq * per_q;
 }
 
-// One J/K build for every molecule of the context: dP, dJ, dK are the
-// concatenated per-molecule n_bf x n_bf (column-major) device blocks.
-static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags) {
-  if (!c->geometry_ready) { set_error("no geometry"); return TF_ESTATE; }
-  if (flags & ~(TF_JK_MIXED | TF_JK_DELTA | TF_JK_NO_COPYBACK)) { set_error("unknown flags"); return TF_EINVAL; }
+// Density transform, pair maxima, quartet counts, their scan and the per-group
+// (start, FP32 start, end) offsets on the device: the part of a build shared by
+// the dynamic and the graph paths.
+static int enqueue_counts(tf_ctx* c, const double* dP, bool mixed, ListArgs& la, int& kernels) {
   cudaStream_t s = c->stream;
-  int kernels = 0;
   const BatchArgs bt = batch_args(c);
-  TF_CUDA(cudaEventRecord(c->ev0, s));
-  {
-    const long long nc2 = c->cmat_off[c->n_mol], ns2 = c->pmax_off[c->n_mol];
-    k_density_to_cart<<<(unsigned)std::max<long long>(1, (nc2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_Pc.p);
-    TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, c->n_mol * sizeof(unsigned long long), s));
-    k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_pmax.p, c->d_pglob.p);
-    kernels += 2;
-  }
-  // quartet lists (bucket-sorted per class pair over the batch; FP32 buckets last when mixed)
-  const bool mixed = (flags & TF_JK_MIXED) != 0;
-  ListArgs la{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
-              c->d_sorted.p,   c->d_sorted_imax.p, c->d_pairs.p,  c->d_mols.p,  c->d_pmax.p,
-              c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0};
+  const long long nc2 = c->cmat_off[c->n_mol], ns2 = c->pmax_off[c->n_mol];
+  k_density_to_cart<<<(unsigned)std::max<long long>(1, (nc2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_Pc.p);
+  TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, c->n_mol * sizeof(unsigned long long), s));
+  k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_pmax.p, c->d_pglob.p);
+  kernels += 2;
+  la = ListArgs{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
+                c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_pairs.p,  c->d_mols.p,  c->d_pmax.p,
+                c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX};
   const long long thr_list = 256;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   const long long nslots = c->n_tasks * NBUCKET;
@@ -1395,29 +1507,189 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   kernels++;
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
-  TF_CUDA(c->d_scan_tmp.reserve(tmp_bytes));
+  if (tmp_bytes > c->d_scan_tmp.n) { set_error("scan scratch not sized"); return TF_ESTATE; }
   TF_CUDA(cudaMemsetAsync(c->d_counts.p + nslots, 0, sizeof(long long), s));
   TF_CUDA(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1),
                                         s));
   const int ng = (int)c->group_cls.size();
-  std::vector<long long> goff(3 * ng);
   k_group_offsets<<<(ng + 63) / 64, 64, 0, s>>>(ng, c->d_group_task0.p, c->d_offsets.p, c->d_group_offsets.p);
-  TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
-  TF_CUDA(cudaStreamSynchronize(s));
-  const long long nq_total = ng > 0 ? goff[3 * (ng - 1) + 2] : 0;
-  // ERIs + digestion
-  const long long nc2 = c->cmat_off[c->n_mol];
-  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc2 * sizeof(double), s));
-  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nc2 * sizeof(double), s));
+  kernels += 3;
+  const long long nc = c->cmat_off[c->n_mol];
+  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc * sizeof(double), s));
+  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nc * sizeof(double), s));
   TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
-  TF_CUDA(cudaEventRecord(c->ev1, s));
+  return TF_OK;
+}
+
+static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, int& kernels) {
+  cudaStream_t s = c->stream;
+  const BatchArgs bt = batch_args(c);
+  const long long nb2 = c->bmat_off[c->n_mol];
+  k_finalize<<<(unsigned)std::max<long long>(1, (nb2 + 255) / 256), 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK);
+  kernels++;
+  TF_CUDA(cudaGetLastError());
+  const int ng = (int)c->group_cls.size();
+  TF_CUDA(cudaMemcpyAsync(c->pin->goff, c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  TF_CUDA(cudaMemcpyAsync(c->pin->pc, c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          s));
+  return TF_OK;
+}
+
+// Graph path: every class launch reads its quartet range from the device
+// (persistent grids of fixed size), so the whole build is one captured graph
+// with no host round trip inside.  The list buffer holds list_cap quartets; a
+// build whose list is longer is detected on the host after the graph (the
+// ranges are clamped, so nothing is written out of bounds) and re-run on the
+// dynamic path with a larger buffer.
+static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* dK, bool mixed, int& kernels) {
+  cudaStream_t s = c->stream;
+  ListArgs la;
+  int rc = enqueue_counts(c, dP, mixed, la, kernels);
+  if (rc) return rc;
+  ListArgs lw = la;
+  lw.out_cap = c->graph_cap;
+  const long long thr_list = 256;
+  const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
+  k_quartets<true><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
+  kernels++;
+  const int ng = (int)c->group_cls.size();
+  for (int g = 0; g < ng; ++g) {
+    int l1h, l1l, l2h, l2l;
+    class_l(c->group_cls[g].x, l1h, l1l);
+    class_l(c->group_cls[g].y, l2h, l2l);
+    {
+      JKArgs a{c->d_quartets.p, 0, c->d_pairs.p, c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p,
+               c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap};
+      JKArgs a32 = a;
+      a32.range = c->d_group_offsets.p + 3 * g + 1;
+      rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
+      if (rc != TF_OK) return rc;
+      kernels++;
+      if (mixed) {
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
+        if (rc != TF_OK) return rc;
+        kernels++;
+      }
+    }
+  }
+  return enqueue_finalize(c, dJ, dK, kernels);
+}
+
+// Statistics of the finished build from the pinned read-backs and the events.
+static int finish_stats(tf_ctx* c, int kernels, bool graph) {
+  const int ng = (int)c->group_cls.size();
+  const long long* goff = c->pin->goff;
+  const unsigned long long* pc = c->pin->pc;
+  float ms_all = 0.f, ms_eri = 0.f;
+  TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
+  double npq = 0.0, flops = 0.0;
+  long long n_fp32 = 0;
+  c->cls_stats.clear();
+  for (int g = 0; g < ng; ++g) {
+    const long long nq = goff[3 * g + 2] - goff[3 * g];
+    n_fp32 += goff[3 * g + 2] - goff[3 * g + 1];
+    if (nq == 0) continue;
+    int l1h, l1l, l2h, l2l;
+    class_l(c->group_cls[g].x, l1h, l1l);
+    class_l(c->group_cls[g].y, l2h, l2l);
+    const double p = (double)pc[qclass_id(l1h, l1l, l2h, l2l)];
+    npq += p;
+    const double fl = class_flops(l1h, l1l, l2h, l2l, (double)nq, p);
+    flops += fl;
+    float ms = 0.f;                       // per-class device time: direct builds only
+    if (!graph) {
+      TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[2 * g], c->cls_ev[2 * g + 1]));
+      ms_eri += ms;
+    }
+    tf_class_stats cs;
+    cs.l[0] = l1h; cs.l[1] = l1l; cs.l[2] = l2h; cs.l[3] = l2l;
+    cs.quartets = (double)nq;
+    cs.prim_quartets = p;
+    cs.flops = fl;
+    cs.ms = ms;
+    c->cls_stats.push_back(cs);
+  }
+  c->stats.build_ms = ms_all;
+  c->stats.eri_ms = graph ? ms_all : ms_eri;
+  c->stats.quartets = ng > 0 ? (double)goff[3 * (ng - 1) + 2] : 0.0;
+  c->stats.quartets_fp32 = (double)n_fp32;
+  c->stats.prim_quartets = npq;
+  c->stats.flops = flops;
+  c->stats.kernels = kernels;
+  c->stats.graph = graph ? 1 : 0;
+  return TF_OK;
+}
+
+// One J/K build for every molecule of the context: dP, dJ, dK are the
+// concatenated per-molecule n_bf x n_bf (column-major) device blocks.
+static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags) {
+  if (!c->geometry_ready) { set_error("no geometry"); return TF_ESTATE; }
+  if (flags & ~(TF_JK_MIXED | TF_JK_DELTA | TF_JK_NO_COPYBACK)) { set_error("unknown flags"); return TF_EINVAL; }
+  cudaStream_t s = c->stream;
+  const bool mixed = (flags & TF_JK_MIXED) != 0;
+  const int ng = (int)c->group_cls.size();
   while ((int)c->cls_ev.size() < 2 * ng) {
     cudaEvent_t e;
     TF_CUDA(cudaEventCreate(&e));
     c->cls_ev.push_back(e);
   }
-  long long n_fp32 = 0;
-  std::vector<long long> g_n(ng);
+  TF_CUDA(c->pin->reserve(3 * (size_t)ng));
+  {
+    size_t tmp_bytes = 0;
+    const long long nslots = c->n_tasks * NBUCKET;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
+    TF_CUDA(c->d_scan_tmp.reserve(tmp_bytes));
+  }
+  // graph path: once a dynamic build has sized the list buffer and set up every
+  // launch, later builds with the same arrays replay one captured graph
+  if (c->use_graph && c->graph_cap > 0) {
+    const bool same = c->graph_exec && c->graph_key_P == dP && c->graph_key_J == dJ && c->graph_key_K == dK &&
+                      c->graph_key_mixed == mixed && c->graph_key_cutoff == c->opt.eri_schwarz_cutoff;
+    if (!same) {
+      drop_graph(c);
+      for (int g = 0; g < ng; ++g) {         // launch set-up of every class, outside the capture
+        int l1h, l1l, l2h, l2l;
+        class_l(c->group_cls[g].x, l1h, l1l);
+        class_l(c->group_cls[g].y, l2h, l2l);
+        const JKArgs none{};
+        for (int fp32 = 0; fp32 < 2; ++fp32) {
+          const int rc = dispatch_jk(l1h, l1l, l2h, l2l, none, s, fp32 != 0);
+          if (rc != TF_OK) return rc;
+        }
+      }
+      int kernels = 0;
+      cudaGraph_t graph = nullptr;
+      TF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_graph_body(c, dP, dJ, dK, mixed, kernels);
+      cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (rc != TF_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+      if (ce != cudaSuccess) { set_error(cudaGetErrorString(ce)); return TF_ECUDA; }
+      ce = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) { c->graph_exec = nullptr; set_error(cudaGetErrorString(ce)); return TF_ECUDA; }
+      c->graph_key_P = dP; c->graph_key_J = dJ; c->graph_key_K = dK;
+      c->graph_key_mixed = mixed;
+      c->graph_key_cutoff = c->opt.eri_schwarz_cutoff;
+      c->graph_kernels = kernels;
+    }
+    TF_CUDA(cudaEventRecord(c->ev0, s));
+    TF_CUDA(cudaGraphLaunch(c->graph_exec, s));
+    TF_CUDA(cudaEventRecord(c->ev2, s));
+    TF_CUDA(cudaStreamSynchronize(s));
+    const long long total = ng > 0 ? c->pin->goff[3 * (ng - 1) + 2] : 0;
+    if (total <= c->graph_cap) return finish_stats(c, c->graph_kernels, true);
+    drop_graph(c);                          // list outgrew the buffer: redo this build dynamically
+  }
+  int kernels = 0;
+  TF_CUDA(cudaEventRecord(c->ev0, s));
+  ListArgs la;
+  int rc = enqueue_counts(c, dP, mixed, la, kernels);
+  if (rc) return rc;
+  std::vector<long long> goff(3 * ng);
+  TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  TF_CUDA(cudaStreamSynchronize(s));
+  TF_CUDA(cudaEventRecord(c->ev1, s));
+  const long long nq_total = ng > 0 ? goff[3 * (ng - 1) + 2] : 0;
   // The lists are written and consumed in chunks of whole class pairs, each at
   // most list_budget quartets (a single larger class pair is one chunk), so a
   // large batch needs one chunk-sized list buffer rather than the whole list.
@@ -1430,11 +1702,25 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     chunk_max = std::max(chunk_max, goff[3 * (g1 - 1) + 2] - goff[3 * g0]);
     chunk.push_back(g1);
   }
-  if (c->d_quartets.reserve(chunk_max) != cudaSuccess) {
+  // a single chunk whose list fits leaves a buffer that later graph builds reuse
+  const bool one_chunk = chunk.size() == 2;
+  const long long want = one_chunk ? std::max<long long>(chunk_max + chunk_max / 4, c->d_quartets.n) : chunk_max;
+  if (c->d_quartets.reserve(want) != cudaSuccess) {
     cudaGetLastError();
-    set_error("quartet list chunk does not fit in device memory");
-    return TF_ENOMEM;
+    if (c->d_quartets.reserve(chunk_max) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("quartet list chunk does not fit in device memory");
+      return TF_ENOMEM;
+    }
   }
+  if (one_chunk && c->graph_cap != (long long)c->d_quartets.n) {
+    drop_graph(c);
+    c->graph_cap = (long long)c->d_quartets.n;
+  } else if (!one_chunk) {
+    drop_graph(c);
+    c->graph_cap = 0;
+  }
+  const long long thr_list = 256;
   for (size_t ci = 0; ci + 1 < chunk.size(); ++ci) {
     const int g0 = chunk[ci], g1 = chunk[ci + 1];
     const long long base = goff[3 * g0], nq = goff[3 * (g1 - 1) + 2] - base;
@@ -1455,68 +1741,29 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       TF_CUDA(cudaEventRecord(c->cls_ev[2 * g], s));
       JKArgs a{c->d_quartets.p + (goff[3 * g] - base), goff[3 * g + 1] - goff[3 * g], c->d_pairs.p,
                c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p,
-               c->d_prim_count.p};
+               c->d_prim_count.p, nullptr, 0, LLONG_MAX};
       JKArgs a32 = a;
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
       a32.n = goff[3 * g + 2] - goff[3 * g + 1];
-      g_n[g] = a.n + a32.n;
-      n_fp32 += a32.n;
       if (a.n > 0) {
-        int rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
         if (rc != TF_OK) return rc;
         kernels++;
       }
       if (a32.n > 0) {
-        int rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
         if (rc != TF_OK) return rc;
         kernels++;
       }
       TF_CUDA(cudaEventRecord(c->cls_ev[2 * g + 1], s));
     }
   }
-  TF_CUDA(cudaGetLastError());
+  (void)nq_total;
+  rc = enqueue_finalize(c, dJ, dK, kernels);
+  if (rc) return rc;
   TF_CUDA(cudaEventRecord(c->ev2, s));
-  {
-    const long long nb2 = c->bmat_off[c->n_mol];
-    k_finalize<<<(unsigned)std::max<long long>(1, (nb2 + 255) / 256), 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK);
-    kernels++;
-  }
-  TF_CUDA(cudaGetLastError());
-  std::vector<unsigned long long> pc(NQCLS);
-  TF_CUDA(cudaMemcpyAsync(pc.data(), c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   TF_CUDA(cudaStreamSynchronize(s));
-  float ms_all = 0.f, ms_eri = 0.f;    // ms_eri: the ERI/digestion launches alone (no list writes)
-  TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
-  double npq = 0.0, flops = 0.0;
-  c->cls_stats.clear();
-  for (int g = 0; g < ng; ++g) {
-    if (g_n[g] == 0) continue;
-    int l1h, l1l, l2h, l2l;
-    class_l(c->group_cls[g].x, l1h, l1l);
-    class_l(c->group_cls[g].y, l2h, l2l);
-    const double p = (double)pc[qclass_id(l1h, l1l, l2h, l2l)];
-    npq += p;
-    const double fl = class_flops(l1h, l1l, l2h, l2l, (double)g_n[g], p);
-    flops += fl;
-    float ms = 0.f;
-    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[2 * g], c->cls_ev[2 * g + 1]));
-    ms_eri += ms;
-    tf_class_stats cs;
-    cs.l[0] = l1h; cs.l[1] = l1l; cs.l[2] = l2h; cs.l[3] = l2l;
-    cs.quartets = (double)g_n[g];
-    cs.prim_quartets = p;
-    cs.flops = fl;
-    cs.ms = ms;
-    c->cls_stats.push_back(cs);
-  }
-  c->stats.build_ms = ms_all;
-  c->stats.eri_ms = ms_eri;
-  c->stats.quartets = (double)nq_total;
-  c->stats.quartets_fp32 = (double)n_fp32;
-  c->stats.prim_quartets = npq;
-  c->stats.flops = flops;
-  c->stats.kernels = kernels;
-  return TF_OK;
+  return finish_stats(c, kernels, false);
 }
 
 static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, tf_ctx** out) {
@@ -1704,6 +1951,15 @@ int tf_set_schwarz_cutoff(tf_ctx* c, double cutoff) {
 int tf_set_list_budget(tf_ctx* c, long long quartets) {
   if (!c || quartets <= 0) { tf::set_error("bad list budget"); return TF_EINVAL; }
   c->list_budget = quartets;
+  return TF_OK;
+}
+
+int tf_set_graph(tf_ctx* c, int on) {
+  if (!c) { tf::set_error("null argument"); return TF_EINVAL; }
+  int rc = tf::set_device(c);
+  if (rc) return rc;
+  c->use_graph = on != 0;
+  tf::drop_graph(c);
   return TF_OK;
 }
 
@@ -2003,6 +2259,7 @@ void tf_ctx_destroy(tf_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  tf::drop_graph(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);

@@ -51,7 +51,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("build_ms", ctypes.c_double), ("eri_ms", ctypes.c_double), ("quartets", ctypes.c_double),
                 ("quartets_fp32", ctypes.c_double), ("prim_quartets", ctypes.c_double),
                 ("flops", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
-                ("kernels", ctypes.c_int)]
+                ("kernels", ctypes.c_int), ("graph", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -83,6 +83,7 @@ def load_library(path: Optional[str] = None):
     L.tf_set_shard.argtypes = [vp, i, i]
     L.tf_set_schwarz_cutoff.argtypes = [vp, d]
     L.tf_set_list_budget.argtypes = [vp, ctypes.c_longlong]
+    L.tf_set_graph.argtypes = [vp, i]
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
     L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
@@ -168,6 +169,10 @@ class FockBuilder:
     def set_list_budget(self, quartets: int):
         """Largest quartet-list chunk (entries of 8 bytes) a build keeps on the device."""
         _check(load_library().tf_set_list_budget(self.h, int(quartets)))
+
+    def set_graph(self, on: bool):
+        """Replay builds as one captured CUDA graph (default) or launch class by class."""
+        _check(load_library().tf_set_graph(self.h, int(bool(on))))
 
     def set_shard(self, index: int, count: int):
         """Build only shard ``index`` of ``count`` (round-robin bra tasks); the shards'
