@@ -321,6 +321,8 @@ def main():
             dist.all_reduce(J)
             dist.all_reduce(K)
 
+    # class schedule of the graph builds, chosen by timing (set-up, untimed)
+    tune = fb.autotune(P, J, K, max_streams=4)
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize(dev)
@@ -392,7 +394,9 @@ def main():
             "config": {"workload": WORKLOAD if args.waters == N_WATER else f"(H2O){args.waters} cc-pVDZ (profiling case)",
                        "n_bf": n, "schwarz_cutoff": SCHWARZ, "l2": "flushed (256 MB write) "
                        "between timed builds", "parallelism": f"round-robin bra pairs x{world} + NCCL all-reduce"
-                       if world > 1 else "single GPU"},
+                       if world > 1 else "single GPU",
+                       "class_schedule": {"graph_branches": tune["streams"],
+                                          "autotune_ms": [round(v, 3) for v in tune["ms"]]}},
             "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(st["kernels"]) * args.steps,
             "e2e": e2e,
             "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"], "flops": st["flops"],

@@ -155,6 +155,23 @@ int tf_set_list_budget(tf_ctx* ctx, long long quartets);
  * counterpart. */
 int tf_set_graph(tf_ctx* ctx, int on);
 
+/* Result of tf_autotune. */
+typedef struct tf_tune {
+  int streams;                       /* graph branches chosen for the class launches */
+  int candidates;                    /* schedules timed (1 .. max_streams branches) */
+  double ms[8];                      /* best graph build time of each candidate */
+  double direct_ms;                  /* the class-by-class build used for the class times */
+} tf_tune;
+
+/* Autotuner for the class schedule of graph builds.  One class-by-class build of
+ * the density dP (device arrays as tf_build_jk_device) gives each class pair's
+ * device time; then for 1 .. max_streams (<= 8) graph branches the class pairs
+ * are assigned longest first to the least-loaded branch, each schedule is
+ * captured and timed over three builds, and the fastest is kept for this
+ * context's later graph builds.  Fills *out if not NULL.  Results do not depend
+ * on the schedule beyond summation order.  No reference counterpart. */
+int tf_autotune(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags, int max_streams, tf_tune* out);
+
 /* Restrict this context's builds to shard `index` of `count`: every count-th bra
  * shell-pair task, as one MPI rank of Tonto's round-robin parallel do
  * (FooToFortran.java:2762-2783, molecule.fock.foo:1274).  The shards' J and K sum

@@ -61,3 +61,28 @@ def test_graph_list_overflow_falls_back(cuda_ok, oracle_mod):
     J, K = fb.make_r_JK(P)
     assert fb.stats()["graph"] == 1
     assert np.max(np.abs(J - Jr)) < 1e-11 and np.max(np.abs(K - Kr)) < 1e-11
+
+
+@pytest.mark.gpu
+def test_autotuned_schedule_keeps_results(cuda_ok, oracle_mod):
+    import torch
+    from tonto_b200.fock import FockBuilder
+    mol = water_cluster(4, seed=7)
+    n = mol.n_bf
+    rng = np.random.default_rng(11)
+    A = rng.normal(size=(n, n)) * 0.05
+    P = A + A.T
+    fb = FockBuilder(mol, schwarz_cutoff=1e-12)
+    dev = torch.device("cuda", 0)
+    Pd = torch.tensor(np.ascontiguousarray(P.T), device=dev)
+    J = torch.empty_like(Pd)
+    K = torch.empty_like(Pd)
+    tune = fb.autotune(Pd, J, K, max_streams=3)
+    assert 1 <= tune["streams"] <= 3 and tune["candidates"] == 3
+    assert all(0.0 < t < 1e6 for t in tune["ms"])
+    Jr, Kr = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12).jk(P)
+    for _ in range(2):
+        fb.make_r_JK_device(Pd, J, K)
+        torch.cuda.synchronize()
+        assert fb.stats()["graph"] == 1
+        assert np.max(np.abs(J.cpu().numpy().T - Jr)) < 1e-11 and np.max(np.abs(K.cpu().numpy().T - Kr)) < 1e-11

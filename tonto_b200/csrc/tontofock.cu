@@ -1161,6 +1161,13 @@ struct tf_ctx {
   bool graph_key_mixed = false;
   double graph_key_cutoff = 0.0;
   int graph_kernels = 0;
+  // class schedule (autotuned): graph branches and the branch of each class pair
+  int sched_streams = 1;
+  std::vector<int> sched_stream_of;
+  std::vector<cudaStream_t> side;                        // branch streams besides the context stream
+  cudaEvent_t fork_ev = nullptr;
+  std::vector<cudaEvent_t> join_ev;
+  tf_tune tune{};                                        // last autotuner result
   tf::PinnedStage pin_obj;
   tf::PinnedStage* pin = &pin_obj;
 };
@@ -1553,25 +1560,38 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
   k_quartets<true><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
   kernels++;
   const int ng = (int)c->group_cls.size();
+  // class schedule: the class launches are spread over sched_streams branches of
+  // the graph (the autotuner's choice), so that one class's tail overlaps another
+  // class's start; J and K are summed with atomics, so the order is free
+  const int ns = std::max(1, std::min(c->sched_streams, 1 + (int)c->side.size()));
+  if (ns > 1) {
+    TF_CUDA(cudaEventRecord(c->fork_ev, s));
+    for (int i = 0; i + 1 < ns; ++i) TF_CUDA(cudaStreamWaitEvent(c->side[i], c->fork_ev, 0));
+  }
   for (int g = 0; g < ng; ++g) {
     int l1h, l1l, l2h, l2l;
     class_l(c->group_cls[g].x, l1h, l1l);
     class_l(c->group_cls[g].y, l2h, l2l);
-    {
-      JKArgs a{c->d_quartets.p, 0, c->d_pairs.p, c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p,
-               c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap};
-      JKArgs a32 = a;
-      a32.range = c->d_group_offsets.p + 3 * g + 1;
-      rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
+    const int si = ns > 1 && g < (int)c->sched_stream_of.size() ? c->sched_stream_of[g] % ns : 0;
+    cudaStream_t sg = si == 0 ? s : c->side[si - 1];
+    JKArgs a{c->d_quartets.p, 0, c->d_pairs.p, c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p,
+             c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap};
+    JKArgs a32 = a;
+    a32.range = c->d_group_offsets.p + 3 * g + 1;
+    rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false);
+    if (rc != TF_OK) return rc;
+    kernels++;
+    if (mixed) {
+      rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, sg, true);
       if (rc != TF_OK) return rc;
       kernels++;
-      if (mixed) {
-        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
-        if (rc != TF_OK) return rc;
-        kernels++;
-      }
     }
   }
+  if (ns > 1)
+    for (int i = 0; i + 1 < ns; ++i) {
+      TF_CUDA(cudaEventRecord(c->join_ev[i], c->side[i]));
+      TF_CUDA(cudaStreamWaitEvent(s, c->join_ev[i], 0));
+    }
   return enqueue_finalize(c, dJ, dK, kernels);
 }
 
@@ -1963,6 +1983,77 @@ int tf_set_graph(tf_ctx* c, int on) {
   return TF_OK;
 }
 
+int tf_autotune(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, int max_streams, tf_tune* out) {
+  using namespace tf;
+  if (!c || !dP || !dJ || !dK || max_streams < 1 || max_streams > 8) { set_error("bad argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  while ((int)c->side.size() < max_streams - 1) {
+    cudaStream_t x;
+    cudaEvent_t e;
+    TF_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    c->side.push_back(x);
+    TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->join_ev.push_back(e);
+  }
+  if (!c->fork_ev) TF_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+  const bool use_graph = c->use_graph;
+  tf_tune res{};
+  // class-pair times from a class-by-class build
+  c->use_graph = false;
+  drop_graph(c);
+  rc = build_jk_device(c, dP, dJ, dK, flags);
+  c->use_graph = use_graph;
+  if (rc) return rc;
+  res.direct_ms = c->stats.build_ms;
+  const int ng = (int)c->group_cls.size();
+  std::vector<double> t(ng, 0.0);
+  for (int g = 0; g < ng; ++g) {
+    float ms = 0.f;
+    TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[2 * g], c->cls_ev[2 * g + 1]));
+    t[g] = ms;
+  }
+  std::vector<int> order(ng);
+  for (int g = 0; g < ng; ++g) order[g] = g;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return t[x] > t[y]; });
+  int best = 1;
+  double best_ms = 1e300;
+  std::vector<int> best_of(ng, 0);
+  if (c->graph_cap > 0) {
+    const bool saved = c->use_graph;
+    c->use_graph = true;
+    for (int ns = 1; ns <= max_streams; ++ns) {
+      std::vector<double> load(ns, 0.0);
+      std::vector<int> of(ng, 0);
+      for (int g : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        of[g] = k;
+        load[k] += t[g];
+      }
+      c->sched_streams = ns;
+      c->sched_stream_of = of;
+      drop_graph(c);
+      double ms = 1e300;
+      for (int rep = 0; rep < 4; ++rep) {
+        rc = build_jk_device(c, dP, dJ, dK, flags);
+        if (rc) { c->use_graph = saved; return rc; }
+        if (rep > 0 && c->stats.graph) ms = std::min(ms, c->stats.build_ms);
+      }
+      res.ms[ns - 1] = ms;
+      res.candidates = ns;
+      if (ms < best_ms * 0.99) { best_ms = ms; best = ns; best_of = of; }
+    }
+    c->use_graph = saved;
+  }
+  c->sched_streams = best;
+  c->sched_stream_of = best_of;
+  drop_graph(c);
+  res.streams = best;
+  c->tune = res;
+  if (out) *out = res;
+  return TF_OK;
+}
+
 int tf_set_shard(tf_ctx* c, int index, int count) {
   using namespace tf;
   if (!c || count < 1 || index < 0 || index >= count) { set_error("bad shard"); return TF_EINVAL; }
@@ -2260,6 +2351,9 @@ void tf_ctx_destroy(tf_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   tf::drop_graph(c);
+  for (cudaStream_t x : c->side) cudaStreamDestroy(x);
+  for (cudaEvent_t x : c->join_ev) cudaEventDestroy(x);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);

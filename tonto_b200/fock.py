@@ -57,6 +57,15 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("streams", ctypes.c_int), ("candidates", ctypes.c_int), ("ms", ctypes.c_double * 8),
+                ("direct_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"streams": self.streams, "candidates": self.candidates, "direct_ms": self.direct_ms,
+                "ms": [self.ms[i] for i in range(self.candidates)]}
+
+
 class ClassStats(ctypes.Structure):
     _fields_ = [("l", ctypes.c_int * 4), ("quartets", ctypes.c_double), ("prim_quartets", ctypes.c_double),
                 ("flops", ctypes.c_double), ("ms", ctypes.c_double)]
@@ -84,6 +93,7 @@ def load_library(path: Optional[str] = None):
     L.tf_set_schwarz_cutoff.argtypes = [vp, d]
     L.tf_set_list_budget.argtypes = [vp, ctypes.c_longlong]
     L.tf_set_graph.argtypes = [vp, i]
+    L.tf_autotune.argtypes = [vp, vp, vp, vp, i, i, P(Tune)]
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
     L.tf_build_jk_batch.argtypes = [P(vp), i, P(P(d)), P(P(d)), P(P(d)), i]
@@ -173,6 +183,18 @@ class FockBuilder:
     def set_graph(self, on: bool):
         """Replay builds as one captured CUDA graph (default) or launch class by class."""
         _check(load_library().tf_set_graph(self.h, int(bool(on))))
+
+    def autotune(self, P, J, K, flags: int = TF_JK_FULL, max_streams: int = 4) -> dict:
+        """Choose the class schedule of graph builds by timing (device arrays as make_r_JK_device)."""
+        import torch
+        for t in (P, J, K):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("autotune takes contiguous float64 CUDA arrays")
+        res = Tune()
+        _check(load_library().tf_autotune(self.h, ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(J.data_ptr()),
+                                          ctypes.c_void_p(K.data_ptr()), int(flags), int(max_streams),
+                                          ctypes.byref(res)))
+        return res.as_dict()
 
     def set_shard(self, index: int, count: int):
         """Build only shard ``index`` of ``count`` (round-robin bra tasks); the shards'
