@@ -60,6 +60,8 @@ extern "C" {
 #define TF_JK_MIXED       0x1   /* quartets with Schwarz x density bound < mixed_cut in FP32 (FP64 roots, accumulation) */
 #define TF_JK_DELTA       0x2   /* incremental: P is a density difference; J, K are increments */
 #define TF_JK_NO_COPYBACK 0x4   /* (device entry points only) leave results on the device */
+#define TF_JK_J_ONLY      0x8   /* Coulomb only: K is returned as zero (screening as for J and K) */
+#define TF_JK_K_ONLY      0x10  /* exchange only: J is returned as zero */
 
 /* Precision of a context's default build */
 #define TF_PRECISION_FP64  0
@@ -125,6 +127,20 @@ int tf_ctx_create_batch(const tf_basis* bases, int n, const tf_options* opt, tf_
 
 /* Number of molecules of the context; fills n_bf_per_mol[n] if not NULL. */
 int tf_batch_info(const tf_ctx* ctx, int* n_bf_per_mol);
+
+/* Unrestricted J and K: MOLECULE.FOCK:make_u_JK_direct (molecule.fock.foo:2360-2504).
+ * Ja, Ka from the alpha density Pa and Jb, Kb from the beta density Pb, with the
+ * shell quartets screened on max |Pa + Pb| as the reference does and each ERI
+ * evaluated once for both spins.  Host arrays, n_bf x n_bf column-major; the
+ * Fock matrices are F_a = H + Ja + Jb - Ka, F_b = H + Ja + Jb - Kb.  flags as
+ * tf_build_jk (TF_JK_MIXED, TF_JK_DELTA, TF_JK_J_ONLY, TF_JK_K_ONLY). */
+int tf_build_jk_uhf(tf_ctx* ctx, const double* Pa, const double* Pb, double* Ja, double* Jb, double* Ka,
+                    double* Kb, int flags);
+
+/* The same on device arrays (the context's concatenated molecule blocks), ordered
+ * on `stream` (NULL: the context's own stream). */
+int tf_build_jk_uhf_device(tf_ctx* ctx, const double* dPa, const double* dPb, double* dJa, double* dJb,
+                           double* dKa, double* dKb, int flags, void* stream);
 
 /* J, K of every molecule of a batched context (host arrays per molecule). */
 int tf_build_jk_batched(tf_ctx* ctx, const double* const* P, double* const* J, double* const* K, int flags);

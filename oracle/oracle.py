@@ -53,6 +53,7 @@ def lib():
         L.oracle_jk_sample.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_long, ctypes.c_int, ctypes.c_long,
                                        ctypes.c_long]
         L.oracle_counts.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+        L.oracle_jk_uhf.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, ctypes.c_int]
         L.oracle_spherical_matrix.argtypes = [ctypes.c_int, dp]
         L.oracle_spherical_matrix.restype = ctypes.c_int
         L.oracle_components.argtypes = [ctypes.c_int, ip]
@@ -127,6 +128,14 @@ class Oracle:
         K = np.zeros((self.n_bf, self.n_bf), order="F")
         lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(n_ranks), int(rank))
         return np.ascontiguousarray(J), np.ascontiguousarray(K)
+
+    def jk_uhf(self, Pa: np.ndarray, Pb: np.ndarray, n_threads: int = 0):
+        """Unrestricted (Ja, Jb, Ka, Kb) (Tonto's make_u_JK_direct): screened on Pa + Pb."""
+        Pa = np.asfortranarray(Pa, dtype=np.float64)
+        Pb = np.asfortranarray(Pb, dtype=np.float64)
+        out = [np.zeros((self.n_bf, self.n_bf), order="F") for _ in range(4)]
+        lib().oracle_jk_uhf(self.h, _dp(Pa), _dp(Pb), *[_dp(x) for x in out], int(n_threads))
+        return tuple(np.ascontiguousarray(x) for x in out)
 
     def counts(self, reset: bool = False) -> np.ndarray:
         out = np.zeros(625 * 2)
@@ -251,3 +260,45 @@ def scf(mol, orc: Optional[Oracle] = None, P0: Optional[np.ndarray] = None, conv
     return {"E": E, "E_e": E - enuc, "V_NN": enuc, "V_ee": Vee, "T": float(np.sum(P * T)),
             "V_eN": float(np.sum(P * V)), "P": P, "iterations": it, "builds": n_builds,
             "seconds": time.time() - t0, "history": history, "S": S, "H": H}
+
+
+def uhf_scf(mol, n_alpha: int, n_beta: int, orc: Optional[Oracle] = None, conv: float = 1e-9,
+            diis_tol: float = 1e-6, diis_keep: int = 8, max_iter: int = 200, verbose: bool = False) -> Dict:
+    """Converged UHF with the oracle's unrestricted J/K, from the core guess:
+    F_a = H + Ja + Jb - Ka, F_b = H + Ja + Jb - Kb, DIIS on both spins together."""
+    orc = orc or Oracle(mol)
+    S, T, V = orc.one_electron()
+    H = T + V
+    X = orthogonaliser(S)
+    enuc = mol.nuclear_repulsion()
+    Pa, _, _ = density_from_fock(H, X, n_alpha)
+    Pb, _, _ = density_from_fock(H, X, n_beta)
+    Pa, Pb = 0.5 * Pa, 0.5 * Pb          # density_from_fock gives 2 C C^T (closed-shell convention)
+    diis = DIIS(diis_keep)
+    E_old = None
+    it = 0
+    history = []
+    while True:
+        Ja, Jb, Ka, Kb = orc.jk_uhf(Pa, Pb)
+        Fa = H + Ja + Jb - Ka
+        Fb = H + Ja + Jb - Kb
+        E = 0.5 * float(np.sum(Pa * (H + Fa)) + np.sum(Pb * (H + Fb))) + enuc
+        ea = Fa @ Pa @ S - S @ Pa @ Fa
+        eb = Fb @ Pb @ S - S @ Pb @ Fb
+        err = np.concatenate([ea, eb])
+        err_norm = float(np.linalg.norm(err))
+        dE = np.inf if E_old is None else E - E_old
+        history.append((it, E, dE, err_norm))
+        if verbose:
+            print(f"oracle uhf {it:3d} E={E:.12f} dE={dE:.3e} err={err_norm:.3e}")
+        if E_old is not None and abs(dE) < conv and err_norm < diis_tol:
+            break
+        if it >= max_iter:
+            break
+        E_old = E
+        Fx = diis.extrapolate(np.concatenate([Fa, Fb]), err)
+        n = Fa.shape[0]
+        Pa = 0.5 * density_from_fock(Fx[:n], X, n_alpha)[0]
+        Pb = 0.5 * density_from_fock(Fx[n:], X, n_beta)[0]
+        it += 1
+    return {"E": E, "Pa": Pa, "Pb": Pb, "iterations": it, "history": history}

@@ -566,16 +566,18 @@ void oracle_jk(OracleCtx* c, const double* P, double* J, double* K, long max_ab_
   oracle_jk_sample(c, P, J, K, max_ab_pairs, n_threads, 1, 0);
 }
 
-// The outer shell-pair loop restricted to ab = ab_offset, ab_offset + ab_stride, ...
-// (one "rank" of Tonto's round-robin parallel do); used to time a bounded sample.
-void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long max_ab_pairs, int n_threads,
-                      long ab_stride, long ab_offset) {
-  Ctx* C = reinterpret_cast<Ctx*>(c);
+// J, K of nd densities Ps[0..nd) (nd = 1: make_r_JK_direct, molecule.fock.foo:1235-1363;
+// nd = 2: make_u_JK_direct, molecule.fock.foo:2360-2504, alpha and beta), screened
+// with the maxima of Pscreen.  The outer shell-pair loop is restricted to
+// ab = ab_offset, ab_offset + ab_stride, ... (one "rank" of Tonto's round-robin
+// parallel do); used to time a bounded sample.
+static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* Ps, double* const* Js,
+                    double* const* Ks, long max_ab_pairs, int n_threads, long ab_stride, long ab_offset) {
   const Basis& B = C->B;
   const int n = B.n_bf;
   const double cutoff = C->schwarz_cutoff;
   std::vector<double> Pm;
-  max_density(*C, P, Pm);
+  max_density(*C, Pscreen, Pm);
   double P_max = 0.0, I_max_all = 0.0;
   for (double v : Pm) P_max = std::max(P_max, v);
   for (double v : C->max_I) I_max_all = std::max(I_max_all, v);
@@ -587,8 +589,8 @@ void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long 
 #else
   int nt = 1;
 #endif
-  std::vector<std::vector<double>> Jt(nt, std::vector<double>((size_t)n * n, 0.0));
-  std::vector<std::vector<double>> Kt(nt, std::vector<double>((size_t)n * n, 0.0));
+  std::vector<std::vector<double>> Jt(nt * nd, std::vector<double>((size_t)n * n, 0.0));
+  std::vector<std::vector<double>> Kt(nt * nd, std::vector<double>((size_t)n * n, 0.0));
   std::vector<std::vector<ClassCount>> cnt(nt, std::vector<ClassCount>(625));
 #pragma omp parallel num_threads(nt)
   {
@@ -597,8 +599,6 @@ void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long 
 #else
     int tid = 0;
 #endif
-    double* Jl = Jt[tid].data();
-    double* Kl = Kt[tid].data();
     Work W;
     Side s_ab_skip, s_ab_full, s_cd;
     // round-robin over ab, as Tonto's parallel do (FooToFortran.java:2762-2783)
@@ -648,57 +648,88 @@ void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long 
           cnt1.prim_quartets += (double)s_ab.n() * s_cd.n();
         }
         int fc = B.shell_first_bf[cc], fd = B.shell_first_bf[dd];
-        int nc = B.nbf_of(pcd.la), nd = B.nbf_of(pcd.lb);
+        int nc = B.nbf_of(pcd.la), ndd = B.nbf_of(pcd.lb);
         const double* I = W.out.data();
-        size_t abcd = 0;
-        for (int d = fd; d < fd + nd; ++d)
-          for (int c2 = fc; c2 < fc + nc; ++c2)
-            for (int b = fb; b < fb + nb; ++b)
-              for (int a = fa; a < fa + na; ++a) {
-                double Iv = factor * I[abcd++];
-                Jl[(size_t)b * n + a] += Iv * P[(size_t)c2 * n + d];
-                Jl[(size_t)d * n + c2] += Iv * P[(size_t)a * n + b];
-                Kl[(size_t)c2 * n + a] += Iv * P[(size_t)b * n + d];
-                Kl[(size_t)d * n + a] += Iv * P[(size_t)b * n + c2];
-                Kl[(size_t)c2 * n + b] += Iv * P[(size_t)a * n + d];
-                Kl[(size_t)d * n + b] += Iv * P[(size_t)a * n + c2];
-              }
+        for (int sp = 0; sp < nd; ++sp) {
+          const double* P = Ps[sp];
+          double* Jl = Jt[tid * nd + sp].data();
+          double* Kl = Kt[tid * nd + sp].data();
+          size_t abcd = 0;
+          for (int d = fd; d < fd + ndd; ++d)
+            for (int c2 = fc; c2 < fc + nc; ++c2)
+              for (int b = fb; b < fb + nb; ++b)
+                for (int a = fa; a < fa + na; ++a) {
+                  double Iv = factor * I[abcd++];
+                  Jl[(size_t)b * n + a] += Iv * P[(size_t)c2 * n + d];
+                  Jl[(size_t)d * n + c2] += Iv * P[(size_t)a * n + b];
+                  Kl[(size_t)c2 * n + a] += Iv * P[(size_t)b * n + d];
+                  Kl[(size_t)d * n + a] += Iv * P[(size_t)b * n + c2];
+                  Kl[(size_t)c2 * n + b] += Iv * P[(size_t)a * n + d];
+                  Kl[(size_t)d * n + b] += Iv * P[(size_t)a * n + c2];
+                }
+        }
       }
     }
   }
-  for (size_t q = 0; q < (size_t)n * n; ++q) {
-    double sj = 0, sk = 0;
-    for (int t = 0; t < nt; ++t) { sj += Jt[t][q]; sk += Kt[t][q]; }
-    J[q] = sj; K[q] = sk;
+  for (int sp = 0; sp < nd; ++sp) {
+    double* J = Js[sp];
+    double* K = Ks[sp];
+    for (size_t q = 0; q < (size_t)n * n; ++q) {
+      double sj = 0, sk = 0;
+      for (int t = 0; t < nt; ++t) { sj += Jt[t * nd + sp][q]; sk += Kt[t * nd + sp][q]; }
+      J[q] = sj; K[q] = sk;
+    }
+    // weight_diagonal_blocks(J,2); blockwise_symmetric_fold(K); J = 2J; reflect
+    for (int s = 0; s < B.n_shell; ++s) {
+      int f = B.shell_first_bf[s], m = B.nbf_of(B.shell_l[s]);
+      for (int j = f; j < f + m; ++j) for (int i = f; i < f + m; ++i) J[(size_t)j * n + i] *= 2.0;
+    }
+    for (int a = 0; a < B.n_shell; ++a) for (int b = 0; b <= a; ++b) {
+      int fa = B.shell_first_bf[a], na = B.nbf_of(B.shell_l[a]);
+      int fb = B.shell_first_bf[b], nb = B.nbf_of(B.shell_l[b]);
+      if (a == b) {
+        std::vector<double> blk((size_t)na * na);
+        for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i) blk[(size_t)j * na + i] = K[(size_t)(fa + j) * n + fa + i];
+        for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i)
+          K[(size_t)(fa + j) * n + fa + i] = blk[(size_t)j * na + i] + blk[(size_t)i * na + j];
+      } else {
+        for (int j = 0; j < nb; ++j) for (int i = 0; i < na; ++i)
+          K[(size_t)(fb + j) * n + fa + i] += K[(size_t)(fa + i) * n + fb + j];
+      }
+    }
+    for (size_t q = 0; q < (size_t)n * n; ++q) J[q] *= 2.0;
+    for (int i = 0; i < n; ++i) for (int j = 0; j < i; ++j) {
+      J[(size_t)i * n + j] = J[(size_t)j * n + i];
+      K[(size_t)i * n + j] = K[(size_t)j * n + i];
+    }
   }
   for (int t = 0; t < nt; ++t)
     for (int q = 0; q < 625; ++q) {
       C->counts[q].quartets += cnt[t][q].quartets;
       C->counts[q].prim_quartets += cnt[t][q].prim_quartets;
     }
-  // weight_diagonal_blocks(J,2); blockwise_symmetric_fold(K); J = 2J; reflect
-  for (int s = 0; s < B.n_shell; ++s) {
-    int f = B.shell_first_bf[s], m = B.nbf_of(B.shell_l[s]);
-    for (int j = f; j < f + m; ++j) for (int i = f; i < f + m; ++i) J[(size_t)j * n + i] *= 2.0;
-  }
-  for (int a = 0; a < B.n_shell; ++a) for (int b = 0; b <= a; ++b) {
-    int fa = B.shell_first_bf[a], na = B.nbf_of(B.shell_l[a]);
-    int fb = B.shell_first_bf[b], nb = B.nbf_of(B.shell_l[b]);
-    if (a == b) {
-      std::vector<double> blk((size_t)na * na);
-      for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i) blk[(size_t)j * na + i] = K[(size_t)(fa + j) * n + fa + i];
-      for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i)
-        K[(size_t)(fa + j) * n + fa + i] = blk[(size_t)j * na + i] + blk[(size_t)i * na + j];
-    } else {
-      for (int j = 0; j < nb; ++j) for (int i = 0; i < na; ++i)
-        K[(size_t)(fb + j) * n + fa + i] += K[(size_t)(fa + i) * n + fb + j];
-    }
-  }
-  for (size_t q = 0; q < (size_t)n * n; ++q) J[q] *= 2.0;
-  for (int i = 0; i < n; ++i) for (int j = 0; j < i; ++j) {
-    J[(size_t)i * n + j] = J[(size_t)j * n + i];
-    K[(size_t)i * n + j] = K[(size_t)j * n + i];
-  }
+}
+
+void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long max_ab_pairs, int n_threads,
+                      long ab_stride, long ab_offset) {
+  const double* Ps[1] = {P};
+  double* Js[1] = {J};
+  double* Ks[1] = {K};
+  jk_impl(reinterpret_cast<Ctx*>(c), P, 1, Ps, Js, Ks, max_ab_pairs, n_threads, ab_stride, ab_offset);
+}
+
+// make_u_JK_direct (molecule.fock.foo:2360-2504): screening on the maxima of
+// Pa + Pb (:2397-2400), then alpha and beta J, K from each ERI.
+void oracle_jk_uhf(OracleCtx* c, const double* Pa, const double* Pb, double* Ja, double* Jb, double* Ka, double* Kb,
+                   int n_threads) {
+  Ctx* C = reinterpret_cast<Ctx*>(c);
+  const size_t nn = (size_t)C->B.n_bf * C->B.n_bf;
+  std::vector<double> PP(nn);
+  for (size_t q = 0; q < nn; ++q) PP[q] = Pa[q] + Pb[q];
+  const double* Ps[2] = {Pa, Pb};
+  double* Js[2] = {Ja, Jb};
+  double* Ks[2] = {Ka, Kb};
+  jk_impl(C, PP.data(), 2, Ps, Js, Ks, -1, n_threads, 1, 0);
 }
 
 // Counters accumulated over oracle_jk calls: out[class*2 + {0,1}] =

@@ -119,3 +119,25 @@ def test_oracle_jk_symmetry_and_threads(oracle_mod):
     J4, K4 = orc.jk(P, n_threads=4)
     assert np.allclose(J1, J1.T, atol=0) and np.allclose(K1, K1.T, atol=0)
     assert np.max(np.abs(J1 - J4)) < 1e-12 and np.max(np.abs(K1 - K4)) < 1e-12
+
+
+def test_oracle_uhf_jk_closed_shell_halves(oracle_mod):
+    """make_u_JK_direct with P_a = P_b = P/2 screens on P and gives half of the
+    restricted J and K for each spin."""
+    mol = water_cluster(1, seed=0)
+    orc = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
+    rng = np.random.default_rng(4)
+    A = rng.normal(size=(mol.n_bf, mol.n_bf)) * 0.1
+    P = A + A.T
+    J, K = orc.jk(P)
+    Ja, Jb, Ka, Kb = orc.jk_uhf(0.5 * P, 0.5 * P)
+    for X, Y in ((Ja, J), (Jb, J), (Ka, K), (Kb, K)):
+        assert np.max(np.abs(X - 0.5 * Y)) < 1e-14
+
+
+def test_oracle_uhf_scf_closed_shell_equals_rhf(oracle_mod):
+    mol = water_cluster(1, seed=0)
+    orc = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
+    r = oracle_mod.scf(mol, orc)
+    u = oracle_mod.uhf_scf(mol, 5, 5, orc)
+    assert abs(u["E"] - r["E"]) < 1e-9

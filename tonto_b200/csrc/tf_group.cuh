@@ -124,6 +124,10 @@ struct GroupArgs {
   unsigned long long* prim_count;
   const long long* range;       // graph builds: see resolve_range
   long long base, cap;
+  const double* P2;             // unrestricted: beta density and its J, K (else null)
+  double* J2;
+  double* K2;
+  int want;                     // bit 0 J, bit 1 K
 };
 
 __constant__ unsigned char c_gcomp[3][NCOMP_ALL];
@@ -261,68 +265,82 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
     if (act) {
       const MolInfo mi = a.mols[b.mol];
       const int n = mi.n_cart;
-      const double* __restrict__ P = a.P + mi.cmat;
-      double* __restrict__ Jm = a.J + mi.cmat;
-      double* __restrict__ Km = a.K + mi.cmat;
       double f = 1.0;
       if (b.sh_hi == b.sh_lo) f *= 0.5;
       if (k.sh_hi == k.sh_lo) f *= 0.5;
       if (qd.x == qd.y) f *= 0.5;
       constexpr int NA = Q::NA, NB = Q::NB, NC = Q::NC, ND = Q::ND, NCD = NC * ND;
       const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
-      for (int e = gl; e < NA * NB; e += G) {            // J(ab) = sum_cd I P(cd)
-        const int ia = e / NB, ibb = e - ia * NB;
-        double s = 0.0;
+      auto digest_j = [&](const double* __restrict__ P, double* __restrict__ Jm) {
+        for (int e = gl; e < NA * NB; e += G) {            // J(ab) = sum_cd I P(cd)
+          const int ia = e / NB, ibb = e - ia * NB;
+          double s = 0.0;
 #pragma unroll
-        for (int c = 0; c < NC; ++c)
+          for (int c = 0; c < NC; ++c)
 #pragma unroll
-          for (int d = 0; d < ND; ++d) s += I[e * NCD + c * ND + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
-        atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ibb, f * s);
+            for (int d = 0; d < ND; ++d) s += I[e * NCD + c * ND + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
+          atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ibb, f * s);
+        }
+        for (int e = gl; e < NCD; e += G) {                // J(cd) = sum_ab I P(ab)
+          const int c = e / ND, d = e - c * ND;
+          double s = 0.0;
+#pragma unroll
+          for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ++ibb)
+              s += I[(ia * NB + ibb) * NCD + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ibb);
+          atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+        }
+      };
+      if (a.want & 1) {
+        digest_j(a.P + mi.cmat, a.J + mi.cmat);
+        if (a.P2) digest_j(a.P2 + mi.cmat, a.J2 + mi.cmat);
       }
-      for (int e = gl; e < NCD; e += G) {                // J(cd) = sum_ab I P(ab)
-        const int c = e / ND, d = e - c * ND;
-        double s = 0.0;
+      auto digest_k = [&](const double* __restrict__ P, double* __restrict__ Km) {
+        for (int e = gl; e < NA * NC; e += G) {            // K(ac) = sum_bd I P(bd)
+          const int ia = e / NC, c = e - ia * NC;
+          double s = 0.0;
 #pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
+          for (int ibb = 0; ibb < NB; ++ibb)
 #pragma unroll
-          for (int ibb = 0; ibb < NB; ++ibb) s += I[(ia * NB + ibb) * NCD + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ibb);
-        atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
-      }
-      for (int e = gl; e < NA * NC; e += G) {            // K(ac) = sum_bd I P(bd)
-        const int ia = e / NC, c = e - ia * NC;
-        double s = 0.0;
+            for (int d = 0; d < ND; ++d)
+              s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + od + d);
+          atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
+        }
+        for (int e = gl; e < NA * ND; e += G) {            // K(ad) = sum_bc I P(bc)
+          const int ia = e / ND, d = e - ia * ND;
+          double s = 0.0;
 #pragma unroll
-        for (int ibb = 0; ibb < NB; ++ibb)
+          for (int ibb = 0; ibb < NB; ++ibb)
 #pragma unroll
-          for (int d = 0; d < ND; ++d) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + od + d);
-        atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
-      }
-      for (int e = gl; e < NA * ND; e += G) {            // K(ad) = sum_bc I P(bc)
-        const int ia = e / ND, d = e - ia * ND;
-        double s = 0.0;
+            for (int c = 0; c < NC; ++c)
+              s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + oc + c);
+          atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
+        }
+        for (int e = gl; e < NB * NC; e += G) {            // K(bc) = sum_ad I P(ad)
+          const int ibb = e / NC, c = e - ibb * NC;
+          double s = 0.0;
 #pragma unroll
-        for (int ibb = 0; ibb < NB; ++ibb)
+          for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
-          for (int c = 0; c < NC; ++c) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + oc + c);
-        atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
-      }
-      for (int e = gl; e < NB * NC; e += G) {            // K(bc) = sum_ad I P(ad)
-        const int ibb = e / NC, c = e - ibb * NC;
-        double s = 0.0;
+            for (int d = 0; d < ND; ++d)
+              s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
+          atomicAdd(Km + (size_t)(ob + ibb) * n + oc + c, f * s);
+        }
+        for (int e = gl; e < NB * ND; e += G) {            // K(bd) = sum_ac I P(ac)
+          const int ibb = e / ND, d = e - ibb * ND;
+          double s = 0.0;
 #pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
+          for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
-          for (int d = 0; d < ND; ++d) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
-        atomicAdd(Km + (size_t)(ob + ibb) * n + oc + c, f * s);
-      }
-      for (int e = gl; e < NB * ND; e += G) {            // K(bd) = sum_ac I P(ac)
-        const int ibb = e / ND, d = e - ibb * ND;
-        double s = 0.0;
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-          for (int c = 0; c < NC; ++c) s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
-        atomicAdd(Km + (size_t)(ob + ibb) * n + od + d, f * s);
+            for (int c = 0; c < NC; ++c)
+              s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
+          atomicAdd(Km + (size_t)(ob + ibb) * n + od + d, f * s);
+        }
+      };
+      if (a.want & 2) {
+        digest_k(a.P + mi.cmat, a.K + mi.cmat);
+        if (a.P2) digest_k(a.P2 + mi.cmat, a.K2 + mi.cmat);
       }
     }
     __syncwarp();

@@ -165,7 +165,8 @@ struct BatchArgs {
 
 // P_cart[p][q] = sum U_A[p][m] P[m][m'] U_B[q][m'] over the shell blocks, for every
 // molecule of the batch (P, Pc: concatenated per-molecule blocks).
-__global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, double* __restrict__ Pc) {
+__global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, const double* __restrict__ P2,
+                                  double* __restrict__ Pc) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b.cmat_off[b.n_mol]) return;
   const int m = find_mol(b.cmat_off, b.n_mol, t);
@@ -178,10 +179,12 @@ __global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, dou
   const int fp = b.shell_first_bf[sp], fq = b.shell_first_bf[sq];
   const bool tp = b.spherical && lp >= 2, tq = b.spherical && lq >= 2;
   const double* Pm = P + mi.bmat;
+  const double* Pm2 = P2 ? P2 + mi.bmat : nullptr;      // second density: the sum is transformed
   const int n_bf = mi.n_bf;
   double s = 0.0;
   if (!tp && !tq) {
-    s = Pm[(size_t)(fq + iq) * n_bf + fp + ip];
+    const size_t at = (size_t)(fq + iq) * n_bf + fp + ip;
+    s = Pm[at] + (Pm2 ? Pm2[at] : 0.0);
   } else {
     const int mp = tp ? 2 * lp + 1 : 1, mq = tq ? 2 * lq + 1 : 1;
     for (int a = 0; a < mp; ++a) {
@@ -191,7 +194,8 @@ __global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, dou
       for (int bb = 0; bb < mq; ++bb) {
         const double ub = tq ? c_U[lq][iq * mq + bb] : 1.0;
         const int ib = tq ? fq + bb : fq + iq;
-        s += ua * ub * Pm[(size_t)ib * n_bf + ia];
+        const size_t at = (size_t)ib * n_bf + ia;
+        s += ua * ub * (Pm[at] + (Pm2 ? Pm2[at] : 0.0));
       }
     }
   }
@@ -200,8 +204,8 @@ __global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, dou
 
 // max |P(a,b)| over each shell pair block (Tonto basis) and, per molecule, the
 // maximum over all pairs (an upper bound: the high word is rounded up).
-__global__ void k_pmax(BatchArgs b, const double* __restrict__ P, double* __restrict__ pmax,
-                       unsigned long long* __restrict__ pglob) {
+__global__ void k_pmax(BatchArgs b, const double* __restrict__ P, const double* __restrict__ P2,
+                       double* __restrict__ pmax, unsigned long long* __restrict__ pglob) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long total = b.pmax_off[b.n_mol];
   double mx = 0.0;
@@ -213,8 +217,12 @@ __global__ void k_pmax(BatchArgs b, const double* __restrict__ P, double* __rest
     const int sa = mi.shell0 + (int)(r / mi.n_shell), sb = mi.shell0 + (int)(r % mi.n_shell);
     const int fa = b.shell_first_bf[sa], fb = b.shell_first_bf[sb], na = b.shell_nbf[sa], nb = b.shell_nbf[sb];
     const double* Pm = P + mi.bmat;
+    const double* Pm2 = P2 ? P2 + mi.bmat : nullptr;    // unrestricted: of P_alpha + P_beta, as the reference
     for (int j = 0; j < nb; ++j)
-      for (int i = 0; i < na; ++i) mx = fmax(mx, fabs(Pm[(size_t)(fb + j) * mi.n_bf + fa + i]));
+      for (int i = 0; i < na; ++i) {
+        const size_t at = (size_t)(fb + j) * mi.n_bf + fa + i;
+        mx = fmax(mx, fabs(Pm[at] + (Pm2 ? Pm2[at] : 0.0)));
+      }
     pmax[t] = mx;
   }
   // nonnegative doubles order like their bit patterns; reduce the high words
@@ -357,6 +365,12 @@ struct JKArgs {
   // range read on the device and clamped to base + cap (quartets = list start)
   const long long* range;
   long long base, cap;
+  // unrestricted builds: the beta density and its J, K (else null); P, J, K above
+  // are then the alpha ones.  want: bit 0 J, bit 1 K.
+  const double* P2;
+  double* J2;
+  double* K2;
+  int want;
 };
 
 
@@ -413,104 +427,114 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD>()) k_jk(JKA
     const bool uni = __all_sync(0xffffffffu, qd.x == __shfl_sync(0xffffffffu, qd.x, 0));
     const MolInfo mi = a.mols[b.mol];
     const int n = mi.n_cart;
-    const double* __restrict__ P = a.P + mi.cmat;
-    double* __restrict__ Jm = a.J + mi.cmat;
-    double* __restrict__ Km = a.K + mi.cmat;
     const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
-    // J(ab) += f sum_cd I P(cd);  J(cd) += f sum_ab I P(ab)
-    double Pcd[Q::NC][Q::ND];
+    // J(ab) += f sum_cd I P(cd);  J(cd) += f sum_ab I P(ab)  (per spin when unrestricted)
+    auto digest_j = [&](const double* __restrict__ P, double* __restrict__ Jm) {
+      double Pcd[Q::NC][Q::ND];
 #pragma unroll
-    for (int c = 0; c < Q::NC; ++c)
+      for (int c = 0; c < Q::NC; ++c)
 #pragma unroll
-      for (int d = 0; d < Q::ND; ++d) Pcd[c][d] = __ldg(P + (size_t)(oc + c) * n + od + d);
+        for (int d = 0; d < Q::ND; ++d) Pcd[c][d] = __ldg(P + (size_t)(oc + c) * n + od + d);
 #pragma unroll
-    for (int ia = 0; ia < Q::NA; ++ia)
+      for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
-      for (int ib = 0; ib < Q::NB; ++ib) {
-        double s = 0.0;
+        for (int ib = 0; ib < Q::NB; ++ib) {
+          double s = 0.0;
 #pragma unroll
-        for (int c = 0; c < Q::NC; ++c)
+          for (int c = 0; c < Q::NC; ++c)
 #pragma unroll
-          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
-        s *= f;
-        if (uni) {
+            for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
+          s *= f;
+          if (uni) {
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          if (lane == 0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
-        } else if (active) {
-          atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+          } else if (active) {
+            atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+          }
         }
-      }
-    if (active) {
-    double Pab[Q::NA][Q::NB];
-#pragma unroll
-    for (int ia = 0; ia < Q::NA; ++ia)
-#pragma unroll
-      for (int ib = 0; ib < Q::NB; ++ib) Pab[ia][ib] = __ldg(P + (size_t)(oa + ia) * n + ob + ib);
-#pragma unroll
-    for (int c = 0; c < Q::NC; ++c)
-#pragma unroll
-      for (int d = 0; d < Q::ND; ++d) {
-        double s = 0.0;
+      if (active) {
+        double Pab[Q::NA][Q::NB];
 #pragma unroll
         for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
-          for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
-        atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+          for (int ib = 0; ib < Q::NB; ++ib) Pab[ia][ib] = __ldg(P + (size_t)(oa + ia) * n + ob + ib);
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) {
+            double s = 0.0;
+#pragma unroll
+            for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+              for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
+            atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+          }
       }
+    };
+    if (a.want & 1) {                    // uniform over the warp (the J(ab) sums shuffle)
+      digest_j(a.P + mi.cmat, a.J + mi.cmat);
+      if (a.P2) digest_j(a.P2 + mi.cmat, a.J2 + mi.cmat);
+    }
     // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
     // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
-    double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
-#pragma unroll
-    for (int ib = 0; ib < Q::NB; ++ib) {
-#pragma unroll
-      for (int d = 0; d < Q::ND; ++d) Pbd[ib][d] = __ldg(P + (size_t)(ob + ib) * n + od + d);
-#pragma unroll
-      for (int c = 0; c < Q::NC; ++c) Pbc[ib][c] = __ldg(P + (size_t)(ob + ib) * n + oc + c);
-    }
-#pragma unroll
-    for (int ia = 0; ia < Q::NA; ++ia) {
-      double Pad[Q::ND], Pac[Q::NC];
-#pragma unroll
-      for (int d = 0; d < Q::ND; ++d) Pad[d] = __ldg(P + (size_t)(oa + ia) * n + od + d);
-#pragma unroll
-      for (int c = 0; c < Q::NC; ++c) Pac[c] = __ldg(P + (size_t)(oa + ia) * n + oc + c);
-#pragma unroll
-      for (int c = 0; c < Q::NC; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int ib = 0; ib < Q::NB; ++ib)
-#pragma unroll
-          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pbd[ib][d];
-        atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
-      }
-#pragma unroll
-      for (int d = 0; d < Q::ND; ++d) {
-        double s = 0.0;
-#pragma unroll
-        for (int ib = 0; ib < Q::NB; ++ib)
-#pragma unroll
-          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pbc[ib][c];
-        atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
-      }
+    // (twice for an unrestricted build: alpha and beta densities)
+    auto digest_k = [&](const double* __restrict__ P, double* __restrict__ Km) {
+      double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
 #pragma unroll
       for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d) Pbd[ib][d] = __ldg(P + (size_t)(ob + ib) * n + od + d);
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c) Pbc[ib][c] = __ldg(P + (size_t)(ob + ib) * n + oc + c);
+      }
+#pragma unroll
+      for (int ia = 0; ia < Q::NA; ++ia) {
+        double Pad[Q::ND], Pac[Q::NC];
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d) Pad[d] = __ldg(P + (size_t)(oa + ia) * n + od + d);
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c) Pac[c] = __ldg(P + (size_t)(oa + ia) * n + oc + c);
 #pragma unroll
         for (int c = 0; c < Q::NC; ++c) {
           double s = 0.0;
 #pragma unroll
-          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pad[d];
-          atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
+          for (int ib = 0; ib < Q::NB; ++ib)
+#pragma unroll
+            for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pbd[ib][d];
+          atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
         }
 #pragma unroll
         for (int d = 0; d < Q::ND; ++d) {
           double s = 0.0;
 #pragma unroll
-          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pac[c];
-          atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
+          for (int ib = 0; ib < Q::NB; ++ib)
+#pragma unroll
+            for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pbc[ib][c];
+          atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
+        }
+#pragma unroll
+        for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+          for (int c = 0; c < Q::NC; ++c) {
+            double s = 0.0;
+#pragma unroll
+            for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pad[d];
+            atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
+          }
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) {
+            double s = 0.0;
+#pragma unroll
+            for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pac[c];
+            atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
+          }
         }
       }
-    }
+    };
+    if (active && (a.want & 2)) {
+      digest_k(a.P + mi.cmat, a.K + mi.cmat);
+      if (a.P2) digest_k(a.P2 + mi.cmat, a.K2 + mi.cmat);
     }
   }
   // primitive-quartet counter (per class, one atomic per warp)
@@ -1137,6 +1161,7 @@ struct tf_ctx {
   tf::DBuf<tf::MolInfo> d_mols;
   tf::DBuf<long long> d_cmat_off, d_bmat_off, d_pmax_off;
   tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax, d_sorted_bmax;
+  tf::DBuf<double> d_PcB, d_JcB, d_KcB, d_Pb, d_Jb, d_Kb;  // unrestricted builds (allocated on first use)
   tf::DBuf<int> d_shell_atom, d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
   tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_schwarz_ids;
   tf::DBuf<tf::PairRec> d_pairs;
@@ -1159,6 +1184,7 @@ struct tf_ctx {
   double* graph_key_J = nullptr;
   double* graph_key_K = nullptr;
   bool graph_key_mixed = false;
+  int graph_key_want = 3;
   double graph_key_cutoff = 0.0;
   int graph_kernels = 0;
   // class schedule (autotuned): graph branches and the branch of each class pair
@@ -1446,7 +1472,7 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   const long long full = (long long)nsm * group_blocks_per_sm;
   const long long blocks = a.range ? full : std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
   GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count,
-              a.range, a.base, a.cap};
+              a.range, a.base, a.cap, a.P2, a.J2, a.K2, a.want};
   k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
   return TF_OK;
 }
@@ -1496,14 +1522,20 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
 // Density transform, pair maxima, quartet counts, their scan and the per-group
 // (start, FP32 start, end) offsets on the device: the part of a build shared by
 // the dynamic and the graph paths.
-static int enqueue_counts(tf_ctx* c, const double* dP, bool mixed, ListArgs& la, int& kernels) {
+static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool mixed, ListArgs& la, int& kernels) {
   cudaStream_t s = c->stream;
   const BatchArgs bt = batch_args(c);
   const long long nc2 = c->cmat_off[c->n_mol], ns2 = c->pmax_off[c->n_mol];
-  k_density_to_cart<<<(unsigned)std::max<long long>(1, (nc2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_Pc.p);
+  const unsigned gc = (unsigned)std::max<long long>(1, (nc2 + 255) / 256);
+  k_density_to_cart<<<gc, 256, 0, s>>>(bt, dP, nullptr, c->d_Pc.p);
+  kernels++;
+  if (dPb) {                                   // unrestricted: the beta density too
+    k_density_to_cart<<<gc, 256, 0, s>>>(bt, dPb, nullptr, c->d_PcB.p);
+    kernels++;
+  }
   TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, c->n_mol * sizeof(unsigned long long), s));
-  k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, c->d_pmax.p, c->d_pglob.p);
-  kernels += 2;
+  k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, dPb, c->d_pmax.p, c->d_pglob.p);
+  kernels++;
   la = ListArgs{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
                 c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_pairs.p,  c->d_mols.p,  c->d_pmax.p,
                 c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX};
@@ -1524,16 +1556,25 @@ static int enqueue_counts(tf_ctx* c, const double* dP, bool mixed, ListArgs& la,
   const long long nc = c->cmat_off[c->n_mol];
   TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc * sizeof(double), s));
   TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nc * sizeof(double), s));
+  if (dPb) {
+    TF_CUDA(cudaMemsetAsync(c->d_JcB.p, 0, nc * sizeof(double), s));
+    TF_CUDA(cudaMemsetAsync(c->d_KcB.p, 0, nc * sizeof(double), s));
+  }
   TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
   return TF_OK;
 }
 
-static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, int& kernels) {
+static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, double* dJb, double* dKb, int& kernels) {
   cudaStream_t s = c->stream;
   const BatchArgs bt = batch_args(c);
   const long long nb2 = c->bmat_off[c->n_mol];
-  k_finalize<<<(unsigned)std::max<long long>(1, (nb2 + 255) / 256), 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK);
+  const unsigned gb = (unsigned)std::max<long long>(1, (nb2 + 255) / 256);
+  k_finalize<<<gb, 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK);
   kernels++;
+  if (dKb) {                                   // unrestricted: the beta J and K
+    k_finalize<<<gb, 256, 0, s>>>(bt, c->d_JcB.p, c->d_KcB.p, dJb, dKb);
+    kernels++;
+  }
   TF_CUDA(cudaGetLastError());
   const int ng = (int)c->group_cls.size();
   TF_CUDA(cudaMemcpyAsync(c->pin->goff, c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -1548,10 +1589,11 @@ static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, int& kernels) {
 // build whose list is longer is detected on the host after the graph (the
 // ranges are clamped, so nothing is written out of bounds) and re-run on the
 // dynamic path with a larger buffer.
-static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* dK, bool mixed, int& kernels) {
+static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* dK, bool mixed, int want,
+                              int& kernels) {
   cudaStream_t s = c->stream;
   ListArgs la;
-  int rc = enqueue_counts(c, dP, mixed, la, kernels);
+  int rc = enqueue_counts(c, dP, nullptr, mixed, la, kernels);
   if (rc) return rc;
   ListArgs lw = la;
   lw.out_cap = c->graph_cap;
@@ -1575,7 +1617,8 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
     const int si = ns > 1 && g < (int)c->sched_stream_of.size() ? c->sched_stream_of[g] % ns : 0;
     cudaStream_t sg = si == 0 ? s : c->side[si - 1];
     JKArgs a{c->d_quartets.p, 0, c->d_pairs.p, c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p,
-             c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap};
+             c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap,
+             nullptr, nullptr, nullptr, want};
     JKArgs a32 = a;
     a32.range = c->d_group_offsets.p + 3 * g + 1;
     rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false);
@@ -1592,7 +1635,7 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
       TF_CUDA(cudaEventRecord(c->join_ev[i], c->side[i]));
       TF_CUDA(cudaStreamWaitEvent(s, c->join_ev[i], 0));
     }
-  return enqueue_finalize(c, dJ, dK, kernels);
+  return enqueue_finalize(c, dJ, dK, nullptr, nullptr, kernels);
 }
 
 // Statistics of the finished build from the pinned read-backs and the events.
@@ -1642,11 +1685,25 @@ static int finish_stats(tf_ctx* c, int kernels, bool graph) {
 
 // One J/K build for every molecule of the context: dP, dJ, dK are the
 // concatenated per-molecule n_bf x n_bf (column-major) device blocks.
-static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags) {
+static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags,
+                           const double* dPb = nullptr, double* dJb = nullptr, double* dKb = nullptr) {
   if (!c->geometry_ready) { set_error("no geometry"); return TF_ESTATE; }
-  if (flags & ~(TF_JK_MIXED | TF_JK_DELTA | TF_JK_NO_COPYBACK)) { set_error("unknown flags"); return TF_EINVAL; }
+  if (flags & ~(TF_JK_MIXED | TF_JK_DELTA | TF_JK_NO_COPYBACK | TF_JK_J_ONLY | TF_JK_K_ONLY)) {
+    set_error("unknown flags"); return TF_EINVAL;
+  }
+  if ((flags & TF_JK_J_ONLY) && (flags & TF_JK_K_ONLY)) { set_error("J-only and K-only together"); return TF_EINVAL; }
+  const int want = (flags & TF_JK_J_ONLY) ? 1 : (flags & TF_JK_K_ONLY) ? 2 : 3;
   cudaStream_t s = c->stream;
   const bool mixed = (flags & TF_JK_MIXED) != 0;
+  if (dPb) {                                    // unrestricted: per-spin Cartesian densities and exchange
+    const long long nc = c->cmat_off[c->n_mol];
+    if (!dJb || !dKb || c->d_PcB.reserve(nc) != cudaSuccess || c->d_JcB.reserve(nc) != cudaSuccess ||
+        c->d_KcB.reserve(nc) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("device allocation");
+      return TF_ENOMEM;
+    }
+  }
   const int ng = (int)c->group_cls.size();
   while ((int)c->cls_ev.size() < 2 * ng) {
     cudaEvent_t e;
@@ -1662,9 +1719,10 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   }
   // graph path: once a dynamic build has sized the list buffer and set up every
   // launch, later builds with the same arrays replay one captured graph
-  if (c->use_graph && c->graph_cap > 0) {
+  if (c->use_graph && c->graph_cap > 0 && !dPb) {
     const bool same = c->graph_exec && c->graph_key_P == dP && c->graph_key_J == dJ && c->graph_key_K == dK &&
-                      c->graph_key_mixed == mixed && c->graph_key_cutoff == c->opt.eri_schwarz_cutoff;
+                      c->graph_key_mixed == mixed && c->graph_key_cutoff == c->opt.eri_schwarz_cutoff &&
+                      c->graph_key_want == want;
     if (!same) {
       drop_graph(c);
       for (int g = 0; g < ng; ++g) {         // launch set-up of every class, outside the capture
@@ -1680,7 +1738,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       int kernels = 0;
       cudaGraph_t graph = nullptr;
       TF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      int rc = enqueue_graph_body(c, dP, dJ, dK, mixed, kernels);
+      int rc = enqueue_graph_body(c, dP, dJ, dK, mixed, want, kernels);
       cudaError_t ce = cudaStreamEndCapture(s, &graph);
       if (rc != TF_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
       if (ce != cudaSuccess) { set_error(cudaGetErrorString(ce)); return TF_ECUDA; }
@@ -1690,6 +1748,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       c->graph_key_P = dP; c->graph_key_J = dJ; c->graph_key_K = dK;
       c->graph_key_mixed = mixed;
       c->graph_key_cutoff = c->opt.eri_schwarz_cutoff;
+      c->graph_key_want = want;
       c->graph_kernels = kernels;
     }
     TF_CUDA(cudaEventRecord(c->ev0, s));
@@ -1703,7 +1762,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   int kernels = 0;
   TF_CUDA(cudaEventRecord(c->ev0, s));
   ListArgs la;
-  int rc = enqueue_counts(c, dP, mixed, la, kernels);
+  int rc = enqueue_counts(c, dP, dPb, mixed, la, kernels);
   if (rc) return rc;
   std::vector<long long> goff(3 * ng);
   TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -1724,8 +1783,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   }
   // a single chunk whose list fits leaves a buffer that later graph builds reuse
   const bool one_chunk = chunk.size() == 2;
-  const long long want = one_chunk ? std::max<long long>(chunk_max + chunk_max / 4, c->d_quartets.n) : chunk_max;
-  if (c->d_quartets.reserve(want) != cudaSuccess) {
+  const long long list_n = one_chunk ? std::max<long long>(chunk_max + chunk_max / 4, c->d_quartets.n) : chunk_max;
+  if (c->d_quartets.reserve(list_n) != cudaSuccess) {
     cudaGetLastError();
     if (c->d_quartets.reserve(chunk_max) != cudaSuccess) {
       cudaGetLastError();
@@ -1761,7 +1820,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       TF_CUDA(cudaEventRecord(c->cls_ev[2 * g], s));
       JKArgs a{c->d_quartets.p + (goff[3 * g] - base), goff[3 * g + 1] - goff[3 * g], c->d_pairs.p,
                c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p,
-               c->d_prim_count.p, nullptr, 0, LLONG_MAX};
+               c->d_prim_count.p, nullptr, 0, LLONG_MAX,
+               dPb ? c->d_PcB.p : nullptr, dPb ? c->d_JcB.p : nullptr, dPb ? c->d_KcB.p : nullptr, want};
       JKArgs a32 = a;
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
       a32.n = goff[3 * g + 2] - goff[3 * g + 1];
@@ -1779,7 +1839,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     }
   }
   (void)nq_total;
-  rc = enqueue_finalize(c, dJ, dK, kernels);
+  rc = enqueue_finalize(c, dJ, dK, dJb, dKb, kernels);
   if (rc) return rc;
   TF_CUDA(cudaEventRecord(c->ev2, s));
   TF_CUDA(cudaStreamSynchronize(s));
@@ -2099,6 +2159,54 @@ int tf_build_jk(tf_ctx* c, const double* P, double* J, double* K, int flags) {
   TF_CUDA(cudaStreamSynchronize(c->stream));
   c->stats.h2d_bytes = (long long)bytes;
   c->stats.d2h_bytes = 2 * (long long)bytes;
+  return TF_OK;
+}
+
+int tf_build_jk_uhf_device(tf_ctx* c, const double* dPa, const double* dPb, double* dJa, double* dJb, double* dKa,
+                           double* dKb, int flags, void* stream) {
+  using namespace tf;
+  if (!c || !dPa || !dPb || !dJa || !dJb || !dKa || !dKb) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  if (user && user != c->stream) {
+    cudaEvent_t e;
+    TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TF_CUDA(cudaEventRecord(e, user));
+    TF_CUDA(cudaStreamWaitEvent(c->stream, e, 0));
+    rc = build_jk_device(c, dPa, dJa, dKa, flags, dPb, dJb, dKb);
+    TF_CUDA(cudaEventRecord(e, c->stream));
+    TF_CUDA(cudaStreamWaitEvent(user, e, 0));
+    TF_CUDA(cudaEventDestroy(e));
+    return rc;
+  }
+  return build_jk_device(c, dPa, dJa, dKa, flags, dPb, dJb, dKb);
+}
+
+int tf_build_jk_uhf(tf_ctx* c, const double* Pa, const double* Pb, double* Ja, double* Jb, double* Ka, double* Kb,
+                    int flags) {
+  using namespace tf;
+  if (!c || !Pa || !Pb || !Ja || !Jb || !Ka || !Kb) { set_error("null argument"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  const long long nb = c->bmat_off[c->n_mol];
+  const size_t bytes = (size_t)nb * sizeof(double);
+  if (c->d_Pb.reserve(nb) != cudaSuccess || c->d_Jb.reserve(nb) != cudaSuccess || c->d_Kb.reserve(nb) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("device allocation");
+    return TF_ENOMEM;
+  }
+  TF_CUDA(cudaMemcpyAsync(c->d_P.p, Pa, bytes, cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA(cudaMemcpyAsync(c->d_Pb.p, Pb, bytes, cudaMemcpyHostToDevice, c->stream));
+  rc = build_jk_device(c, c->d_P.p, c->d_J.p, c->d_K.p, flags, c->d_Pb.p, c->d_Jb.p, c->d_Kb.p);
+  if (rc) return rc;
+  TF_CUDA(cudaMemcpyAsync(Ja, c->d_J.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaMemcpyAsync(Jb, c->d_Jb.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaMemcpyAsync(Ka, c->d_K.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaMemcpyAsync(Kb, c->d_Kb.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TF_CUDA(cudaStreamSynchronize(c->stream));
+  c->stats.h2d_bytes = 2 * (long long)bytes;
+  c->stats.d2h_bytes = 4 * (long long)bytes;
   return TF_OK;
 }
 

@@ -28,6 +28,8 @@ LIB_PATH = os.path.join(HERE, "libtontofock.so")
 TF_JK_FULL = 0x0
 TF_JK_MIXED = 0x1
 TF_JK_DELTA = 0x2
+TF_JK_J_ONLY = 0x8
+TF_JK_K_ONLY = 0x10
 
 
 class TontoFockError(RuntimeError):
@@ -93,6 +95,8 @@ def load_library(path: Optional[str] = None):
     L.tf_set_schwarz_cutoff.argtypes = [vp, d]
     L.tf_set_list_budget.argtypes = [vp, ctypes.c_longlong]
     L.tf_set_graph.argtypes = [vp, i]
+    L.tf_build_jk_uhf.argtypes = [vp, P(d), P(d), P(d), P(d), P(d), P(d), i]
+    L.tf_build_jk_uhf_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, i, vp]
     L.tf_autotune.argtypes = [vp, vp, vp, vp, i, i, P(Tune)]
     L.tf_build_jk_device.argtypes = [vp, vp, vp, vp, i, vp]
     L.tf_build_fock.argtypes = [vp, P(d), P(d), P(d)]
@@ -230,6 +234,29 @@ class FockBuilder:
         _check(load_library().tf_build_jk_device(self.h, ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(J.data_ptr()),
                                                  ctypes.c_void_p(K.data_ptr()), int(flags),
                                                  ctypes.c_void_p(s.cuda_stream)))
+
+    def make_u_JK(self, Pa: np.ndarray, Pb: np.ndarray, flags: int = TF_JK_FULL):
+        """Unrestricted (Ja, Jb, Ka, Kb) from the alpha and beta densities (host arrays):
+        MOLECULE.FOCK:make_u_JK_direct."""
+        n = self.n_bf
+        Pa = np.asfortranarray(Pa, dtype=np.float64)
+        Pb = np.asfortranarray(Pb, dtype=np.float64)
+        if Pa.shape != (n, n) or Pb.shape != (n, n):
+            raise ValueError(f"Pa, Pb must be {n}x{n}")
+        out = [np.empty((n, n), order="F") for _ in range(4)]
+        _check(load_library().tf_build_jk_uhf(self.h, _dp(Pa), _dp(Pb), *[_dp(x) for x in out], int(flags)))
+        return tuple(out)
+
+    def make_u_JK_device(self, Pa, Pb, Ja, Jb, Ka, Kb, flags: int = TF_JK_FULL, stream=None):
+        """Unrestricted J, K on device tensors (n_bf, n_bf), ordered on ``stream``."""
+        import torch
+        for t in (Pa, Pb, Ja, Jb, Ka, Kb):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == self.n_bf ** 2):
+                raise ValueError("device tensors must be contiguous float64 CUDA (n_bf, n_bf)")
+        s = stream if stream is not None else torch.cuda.current_stream(Pa.device)
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        _check(load_library().tf_build_jk_uhf_device(self.h, ptr(Pa), ptr(Pb), ptr(Ja), ptr(Jb), ptr(Ka), ptr(Kb),
+                                                     int(flags), ctypes.c_void_p(s.cuda_stream)))
 
     def make_r_Fock_mx(self, P: np.ndarray, H: np.ndarray) -> np.ndarray:
         n = self.n_bf

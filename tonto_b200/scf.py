@@ -226,3 +226,66 @@ class RHF:
         return SCFResult(energy=E, converged=converged, iterations=it, builds=builds,
                          seconds=time.perf_counter() - t0, build_seconds=build_s, P=P, history=hist,
                          guess=guess_name, fell_back=fell_back)
+
+
+class UHF(RHF):
+    """Unrestricted Hartree-Fock on the unrestricted J/K build (make_u_JK_direct):
+    F_a = H + Ja + Jb - Ka, F_b = H + Ja + Jb - Kb; DIIS (keep 8) on both spins
+    together, with the commutator errors of both spins as one vector."""
+
+    def __init__(self, mol: Molecule, multiplicity: int = 1, **kw):
+        super().__init__(mol, **kw)
+        n_el = mol.n_electrons
+        n_unp = multiplicity - 1
+        if n_unp < 0 or (n_el - n_unp) % 2 or n_unp > n_el:
+            raise ValueError("multiplicity does not fit the electron count")
+        self.n_alpha = (n_el + n_unp) // 2
+        self.n_beta = (n_el - n_unp) // 2
+        n = mol.n_bf
+        self._buf = [torch.empty((n, n), dtype=torch.float64, device=self.dev) for _ in range(4)]
+
+    def spin_density(self, F: torch.Tensor, n: int) -> torch.Tensor:
+        e, C = torch.linalg.eigh(self.X.T @ F @ self.X)
+        Co = (self.X @ C)[:, :n]
+        return Co @ Co.T
+
+    def run(self, conv: float = 1e-9, diis_tol: float = 1e-6, max_iter: int = 200, flags: int = TF_JK_FULL,
+            verbose: bool = False) -> SCFResult:
+        torch.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        Pa = self.spin_density(self.H, self.n_alpha)
+        Pb = self.spin_density(self.H, self.n_beta)
+        diis = DIIS(self.diis_keep)
+        Ja, Jb, Ka, Kb = self._buf
+        E_old = None
+        hist = []
+        it = 0
+        converged = False
+        E = float("nan")
+        n = self.mol.n_bf
+        while True:
+            self.fb.make_u_JK_device(Pa.contiguous(), Pb.contiguous(), Ja, Jb, Ka, Kb, flags)
+            Fa = self.H + Ja + Jb - Ka
+            Fb = self.H + Ja + Jb - Kb
+            E = float(0.5 * (torch.sum(Pa * (self.H + Fa)) + torch.sum(Pb * (self.H + Fb)))) + self.e_nuc
+            err = torch.cat([Fa @ Pa @ self.S - self.S @ Pa @ Fa, Fb @ Pb @ self.S - self.S @ Pb @ Fb])
+            err_n = float(torch.linalg.norm(err))
+            dE = float("inf") if E_old is None else E - E_old
+            hist.append((it, E, dE, err_n, "fp64"))
+            if verbose:
+                print(f"uhf {it:3d} E={E:.12f} dE={dE:.3e} err={err_n:.3e}")
+            if E_old is not None and abs(dE) < conv and err_n < diis_tol:
+                converged = True
+                break
+            if it >= max_iter:
+                break
+            E_old = E
+            Fx = diis.extrapolate(torch.cat([Fa, Fb]), err)
+            Pa = self.spin_density(Fx[:n], self.n_alpha)
+            Pb = self.spin_density(Fx[n:], self.n_beta)
+            it += 1
+        torch.cuda.synchronize(self.dev)
+        res = SCFResult(energy=E, converged=converged, iterations=it, builds=it + 1,
+                        seconds=time.perf_counter() - t0, build_seconds=0.0, P=Pa + Pb, history=hist)
+        res.Pa, res.Pb = Pa, Pb
+        return res
