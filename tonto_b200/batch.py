@@ -4,12 +4,23 @@ Every cycle issues a single build of a batched context (tf_ctx_create_batch):
 each molecule contributes its full density (first cycle, periodic rebuilds and
 the final cycles), its density change since the last cycle (incremental
 cycles; G is linear in the density), or nothing once converged (a zero change
-is screened out entirely by the density test).  Diagonalisations are batched over
-molecules of equal size.  Per molecule the loop is Tonto's usual_SCF with DIIS
-(keep 8), as in ``tonto_b200.scf``: cheap builds until the convergence test first
-passes, then full FP64 builds until it passes again after at least two of them.
-A molecule whose DIIS error after ``fallback_after`` cycles is not below its first
-cycle's restarts (once) from ``fallback(i)``, as in ``tonto_b200.scf``.
+is screened out entirely by the density test).  Per molecule the loop is Tonto's
+usual_SCF with DIIS (keep 8), as in ``tonto_b200.scf``: cheap builds until the
+convergence test first passes, then full FP64 builds until it passes again after
+at least two of them.  A molecule whose DIIS error after ``fallback_after`` cycles
+is not below its first cycle's restarts (once) from ``fallback(i)``.
+
+Everything between the builds runs on the device in batches: the molecules are
+grouped into a few size buckets, each padded to its largest member, and the
+Fock matrices, energies, DIIS errors, DIIS extrapolations and new densities of a
+bucket are batched matrix products.  The density of an (extrapolated) Fock matrix
+is the projector on its n_occ lowest orbitals; it is obtained by trace-correcting
+purification (Niklasson, Phys. Rev. B 66, 155115 (2002), "TC2") of the Fock
+matrix in the orthogonal basis: X_0 = (e_max - F') / (e_max - e_min) with
+Gershgorin bounds, then X <- X^2 or 2X - X^2, whichever moves tr X towards
+n_occ, until X is idempotent.  This is the same projector as the aufbau density
+from a diagonalisation (the SCF converges to the same fixed point), at the cost
+of batched matrix products instead of one eigensolver call per molecule.
 """
 
 from __future__ import annotations
@@ -22,70 +33,141 @@ import torch
 
 from .basis import Molecule
 from .fock import TF_JK_DELTA, TF_JK_FULL, TF_JK_MIXED, BatchFockBuilder
-from .scf import DIIS, SCFResult
+from .scf import SCFResult
+
+
+class _Bucket:
+    """Molecules of similar size, padded to the largest (n)."""
+
+    def __init__(self, ids: List[int], n_bf: List[int], dev):
+        self.ids = ids
+        self.m = len(ids)
+        self.n = max(n_bf[i] for i in ids)
+        self.n_bf = torch.tensor([n_bf[i] for i in ids], device=dev)
+        r = torch.arange(self.n, device=dev)
+        self.valid = r[None, :] < self.n_bf[:, None]                       # (m, n) real rows
+
+
+def purify(Fo: torch.Tensor, valid: torch.Tensor, n_occ: torch.Tensor, tol: float = 1e-13,
+           max_iter: int = 100) -> torch.Tensor:
+    """TC2 purification of a batch of symmetric matrices Fo (m, n, n) (orthogonal
+    basis; rows with valid == False are padding): the projector on the n_occ[i]
+    lowest eigenvectors of each real block (padding stays unoccupied)."""
+    m, n, _ = Fo.shape
+    eye = torch.eye(n, dtype=Fo.dtype, device=Fo.device)
+    Fo = Fo * (valid[:, :, None] & valid[:, None, :])
+    d = torch.diagonal(Fo, dim1=1, dim2=2)
+    r = Fo.abs().sum(2) - d.abs()
+    big = torch.finfo(Fo.dtype).max
+    e_min = torch.where(valid, d - r, torch.full_like(d, big)).min(1).values
+    e_max = torch.where(valid, d + r, torch.full_like(d, -big)).max(1).values
+    # padding rows get e_max on the diagonal: they map to 0 and stay there
+    Fo = Fo + torch.diag_embed((~valid).to(Fo.dtype) * e_max[:, None])
+    X = (e_max[:, None, None] * eye - Fo) / (e_max - e_min)[:, None, None]
+    N = n_occ.to(Fo.dtype)
+    for it in range(max_iter):
+        X2 = torch.bmm(X, X)
+        t1 = torch.diagonal(X, dim1=1, dim2=2).sum(1)
+        t2 = torch.diagonal(X2, dim1=1, dim2=2).sum(1)
+        square = (t2 - N).abs() < (2.0 * t1 - t2 - N).abs()
+        X = torch.where(square[:, None, None], X2, 2.0 * X - X2)
+        if it >= 8 and it % 4 == 0 and float((t1 - t2).abs().max()) < tol * n:   # tr(X - X^2)
+            break
+    return 0.5 * (X + X.transpose(1, 2))
 
 
 class BatchRHF:
     def __init__(self, mols: List[Molecule], schwarz_cutoff: float = 1e-12, device: int = 0,
-                 mixed_fp32_cut: float = 1e-6):
+                 mixed_fp32_cut: float = 1e-6, n_buckets: int = 4):
         self.mols = list(mols)
+        nm = len(self.mols)
         self.dev = torch.device("cuda", device)
+        dev = self.dev
         self.fb = BatchFockBuilder(self.mols, schwarz_cutoff=schwarz_cutoff, device=device,
                                    mixed_fp32_cut=mixed_fp32_cut)
-        S, T, V = self.fb.one_electron()
-        t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=self.dev)  # noqa: E731
-        self.S = [t(x) for x in S]
-        self.H = [t(a) + t(b) for a, b in zip(T, V)]
-        self.X = []
-        for s in self.S:
-            e, U = torch.linalg.eigh(s)
-            self.X.append((U / torch.sqrt(e)) @ U.T)
-        self.n_occ = [m.n_electrons // 2 for m in self.mols]
-        self.e_nuc = [m.nuclear_repulsion() for m in self.mols]
+        n_bf = [m.n_bf for m in self.mols]
+        self.n_bf = n_bf
+        order = sorted(range(nm), key=lambda i: n_bf[i])
+        nb = max(1, min(n_buckets, nm))
+        cuts = [order[(k * nm) // nb:((k + 1) * nm) // nb] for k in range(nb)]
+        self.buckets = [_Bucket(ids, n_bf, dev) for ids in cuts if ids]
+        # concatenated <-> padded index maps (the matrices are symmetric)
         self.off = [int(v) for v in self.fb.offsets]
+        for b in self.buckets:
+            idx = []
+            for k, i in enumerate(b.ids):
+                n = n_bf[i]
+                rr, cc = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+                idx.append((k * b.n * b.n + rr * b.n + cc).ravel())
+            b.pad_idx = torch.tensor(np.concatenate(idx), device=dev)
+            b.cat_idx = torch.cat([torch.arange(self.off[i], self.off[i + 1], device=dev) for i in b.ids])
+        S, T, V = self.fb.one_electron()
+        for b in self.buckets:
+            b.S = self._pad(b, [S[i] for i in b.ids])
+            b.H = self._pad(b, [T[i] + V[i] for i in b.ids])
+            X = torch.zeros_like(b.S)
+            for k in range(b.m):
+                n = n_bf[b.ids[k]]
+                e, U = torch.linalg.eigh(b.S[k, :n, :n])
+                X[k, :n, :n] = (U / torch.sqrt(e)) @ U.T
+            b.X = X
+            b.n_occ = torch.tensor([self.mols[i].n_electrons // 2 for i in b.ids], device=dev)
+            b.e_nuc = torch.tensor([self.mols[i].nuclear_repulsion() for i in b.ids], dtype=torch.float64,
+                                   device=dev)
         tot = self.off[-1]
-        self.Xin = torch.zeros(tot, dtype=torch.float64, device=self.dev)
-        self.J = torch.zeros(tot, dtype=torch.float64, device=self.dev)
-        self.K = torch.zeros(tot, dtype=torch.float64, device=self.dev)
-        # molecules grouped by size for batched diagonalisation
-        self.by_size = {}
-        for i, m in enumerate(self.mols):
-            self.by_size.setdefault(m.n_bf, []).append(i)
+        self.Xin = torch.zeros(tot, dtype=torch.float64, device=dev)
+        self.J = torch.zeros(tot, dtype=torch.float64, device=dev)
+        self.K = torch.zeros(tot, dtype=torch.float64, device=dev)
 
-    def _view(self, buf, i):
-        n = self.mols[i].n_bf
-        return buf[self.off[i]:self.off[i + 1]].view(n, n)
-
-    def densities(self, Fs, idx):
-        """New densities of molecules idx from their (extrapolated) Fock matrices."""
-        out = {}
-        groups = {}
-        for i in idx:
-            groups.setdefault(self.mols[i].n_bf, []).append(i)
-        for n, ids in groups.items():
-            Xs = torch.stack([self.X[i] for i in ids])
-            Fo = torch.stack([Fs[i] for i in ids])
-            _, C = torch.linalg.eigh(Xs.transpose(1, 2) @ Fo @ Xs)
-            C = Xs @ C
-            for k, i in enumerate(ids):
-                Co = C[k, :, : self.n_occ[i]]
-                out[i] = 2.0 * Co @ Co.T
+    def _pad(self, b: _Bucket, mats) -> torch.Tensor:
+        out = torch.zeros((b.m, b.n, b.n), dtype=torch.float64, device=self.dev)
+        for k, a in enumerate(mats):
+            n = a.shape[0]
+            out[k, :n, :n] = torch.as_tensor(np.ascontiguousarray(a) if isinstance(a, np.ndarray) else a,
+                                             dtype=torch.float64, device=self.dev)
         return out
+
+    def _from_cat(self, b: _Bucket, buf: torch.Tensor) -> torch.Tensor:
+        out = torch.zeros(b.m * b.n * b.n, dtype=torch.float64, device=self.dev)
+        out[b.pad_idx] = buf[b.cat_idx]
+        return out.view(b.m, b.n, b.n)
+
+    def _to_cat(self, b: _Bucket, X: torch.Tensor, buf: torch.Tensor):
+        buf[b.cat_idx] = X.reshape(-1)[b.pad_idx]
+
+    def densities(self, b: _Bucket, F: torch.Tensor) -> torch.Tensor:
+        """Aufbau densities 2 C_occ C_occ^T of a bucket's Fock matrices (padded)."""
+        Fo = torch.bmm(b.X.transpose(1, 2), torch.bmm(F, b.X))
+        Po = purify(Fo, b.valid, b.n_occ)
+        return 2.0 * torch.bmm(b.X, torch.bmm(Po, b.X.transpose(1, 2)))
 
     def run(self, P0: Optional[List[torch.Tensor]] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
             max_iter: int = 100, incremental: bool = True, mixed: bool = False, rebuild_every: int = 16,
             mixed_until: float = 1e-6, fp64_final: int = 2,
-            fallback: Optional[Callable[[int], torch.Tensor]] = None, fallback_after: int = 3) -> List[SCFResult]:
+            fallback: Optional[Callable[[int], torch.Tensor]] = None, fallback_after: int = 3,
+            diis_keep: int = 8) -> List[SCFResult]:
         nm = len(self.mols)
-        torch.cuda.synchronize(self.dev)
+        dev = self.dev
+        torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        if P0 is None:
-            P = self.densities(self.H, range(nm))
-        else:
-            P = {i: P0[i].to(self.dev, torch.float64) for i in range(nm)}
-        diis = [DIIS(8) for _ in range(nm)]
-        F_prev = [None] * nm
-        P_prev = [None] * nm
+        bk = self.buckets
+        for b in bk:
+            if P0 is None:
+                b.P = self.densities(b, b.H)
+            else:
+                b.P = self._pad(b, [P0[i].to(dev, torch.float64) for i in b.ids])
+            b.P_prev = torch.zeros_like(b.P)
+            b.F_prev = torch.zeros_like(b.P)
+            b.Fh = torch.zeros((b.m, diis_keep) + b.P.shape[1:], dtype=torch.float64, device=dev)
+            b.Eh = torch.zeros_like(b.Fh)
+            b.count = torch.zeros(b.m, dtype=torch.long, device=dev)
+        where, row = {}, {}
+        r0 = 0
+        for bi, b in enumerate(bk):
+            for k, i in enumerate(b.ids):
+                where[i] = (bi, k)
+                row[i] = r0 + k
+            r0 += b.m
         E_old = [None] * nm
         state = ["cheap" if (incremental or mixed) else "final"] * nm
         n_final = [0] * nm
@@ -94,57 +176,56 @@ class BatchRHF:
         fell_back = [False] * nm
         err_first = [None] * nm
         cyc = [0] * nm
+        have_prev = [False] * nm
         hist = [[] for _ in range(nm)]
         E = [float("nan")] * nm
         it = 0
         builds = 0
+        mask = lambda b, v: torch.tensor([v[i] for i in b.ids], device=dev)  # noqa: E731
         while not all(done) and it <= max_iter:
             active = [i for i in range(nm) if not done[i]]
             any_final = any(state[i] == "final" for i in active)
             use_mixed = mixed and not any_final and all(
                 E_old[i] is None or abs(hist[i][-1][2]) >= mixed_until for i in active)
-            kinds = {}
-            self.Xin.zero_()
-            for i in active:
-                delta = (state[i] == "cheap" and incremental and F_prev[i] is not None
-                         and since_full[i] < rebuild_every)
-                kinds[i] = delta
-                self._view(self.Xin, i).copy_(P[i] - P_prev[i] if delta else P[i])
+            delta = [(not done[i]) and state[i] == "cheap" and incremental and have_prev[i]
+                     and since_full[i] < rebuild_every for i in range(nm)]
+            live = [not d for d in done]
+            for b in bk:
+                dm = mask(b, delta)[:, None, None]
+                D = torch.where(dm, b.P - b.P_prev, b.P) * mask(b, live)[:, None, None]
+                self._to_cat(b, D, self.Xin)
             flags = (TF_JK_MIXED if use_mixed else TF_JK_FULL) | TF_JK_DELTA
             self.fb.make_r_JK_device(self.Xin, self.J, self.K, flags)
             builds += 1
-            Fs = {}
-            errs = {}
+            scal = []
+            for b in bk:
+                G = self._from_cat(b, self.J) - 0.5 * self._from_cat(b, self.K)
+                b.F = torch.where(mask(b, delta)[:, None, None], b.F_prev + G, b.H + G)
+                b.err = torch.bmm(b.F, torch.bmm(b.P, b.S)) - torch.bmm(b.S, torch.bmm(b.P, b.F))
+                e_b = 0.5 * (b.P * (b.H + b.F)).sum((1, 2)) + b.e_nuc
+                scal.append(torch.stack([e_b, torch.linalg.norm(b.err.reshape(b.m, -1), dim=1)], 1))
+            scal = torch.cat(scal).cpu().numpy()                 # the per-cycle host sync
+            cont = [False] * nm
+            restart = []
             for i in active:
-                J, K = self._view(self.J, i).T, self._view(self.K, i).T     # column-major blocks
-                G = J - 0.5 * K
-                if kinds[i]:
-                    F = F_prev[i] + G
+                E[i] = float(scal[row[i], 0])
+                err_n = float(scal[row[i], 1])
+                dE = float("inf") if E_old[i] is None else E[i] - E_old[i]
+                hist[i].append((it, E[i], dE, err_n, ("mixed" if use_mixed else "fp64") + ("+delta" if delta[i] else "")))
+                if delta[i]:
                     since_full[i] += 1
                 else:
-                    F = self.H[i] + G
                     since_full[i] = 0
                     if state[i] == "final":
                         n_final[i] += 1
-                Fs[i] = F
-                errs[i] = F @ P[i] @ self.S[i] - self.S[i] @ P[i] @ F
-            # scalars of all active molecules in one transfer
-            scal = torch.stack([torch.stack([0.5 * torch.sum(P[i] * (self.H[i] + Fs[i])), torch.linalg.norm(errs[i])])
-                                for i in active]).cpu().numpy()
-            nxt = []
-            for k, i in enumerate(active):
-                E[i] = float(scal[k, 0]) + self.e_nuc[i]
-                err_n = float(scal[k, 1])
-                dE = float("inf") if E_old[i] is None else E[i] - E_old[i]
-                hist[i].append((it, E[i], dE, err_n, ("mixed" if use_mixed else "fp64") + ("+delta" if kinds[i] else "")))
                 if err_first[i] is None:
                     err_first[i] = err_n
                 if (fallback is not None and not fell_back[i] and cyc[i] == fallback_after
                         and err_n >= err_first[i]):
-                    P[i] = fallback(i).to(self.dev, torch.float64)
-                    diis[i].reset()
+                    restart.append(i)
                     fell_back[i] = True
-                    E_old[i] = F_prev[i] = P_prev[i] = err_first[i] = None
+                    E_old[i] = err_first[i] = None
+                    have_prev[i] = False
                     cyc[i] = 0
                     continue
                 cyc[i] += 1
@@ -155,14 +236,62 @@ class BatchRHF:
                 if state[i] == "cheap" and passed:
                     state[i] = "final"
                 E_old[i] = E[i]
-                F_prev[i], P_prev[i] = Fs[i], P[i]
-                Fs[i] = diis[i].extrapolate(Fs[i], errs[i])
-                nxt.append(i)
-            if nxt:
-                P.update(self.densities(Fs, nxt))
+                have_prev[i] = True
+                cont[i] = True
+            # DIIS (keep 8) and new densities of the molecules that go on
+            for b in bk:
+                cm = mask(b, cont)
+                if not any(cont[i] for i in b.ids):
+                    continue
+                c3 = cm[:, None, None]
+                b.P_prev = torch.where(c3, b.P, b.P_prev)
+                b.F_prev = torch.where(c3, b.F, b.F_prev)
+                Fx = self._diis(b, cm, diis_keep)
+                b.P = torch.where(c3, self.densities(b, Fx), b.P)
+            for i in restart:
+                bi, k = where[i]
+                b = bk[bi]
+                n = self.n_bf[i]
+                b.P[k].zero_()
+                b.P[k, :n, :n] = fallback(i).to(dev, torch.float64)
+                b.count[k] = 0
             it += 1
-        torch.cuda.synchronize(self.dev)
+        torch.cuda.synchronize(dev)
         secs = time.perf_counter() - t0
-        return [SCFResult(energy=E[i], converged=done[i], iterations=len(hist[i]) - 1, builds=builds,
-                          seconds=secs, build_seconds=0.0, P=P[i], history=hist[i], fell_back=fell_back[i])
-                for i in range(nm)]
+        out = []
+        for i in range(nm):
+            bi, k = where[i]
+            n = self.n_bf[i]
+            out.append(SCFResult(energy=E[i], converged=done[i], iterations=len(hist[i]) - 1, builds=builds,
+                                 seconds=secs, build_seconds=0.0, P=bk[bi].P[k, :n, :n].clone(),
+                                 history=hist[i], fell_back=fell_back[i]))
+        return out
+
+    @staticmethod
+    def _diis(b: _Bucket, cm: torch.Tensor, keep: int) -> torch.Tensor:
+        """Pulay DIIS per molecule of a bucket; the rows cm store this cycle's F and
+        commutator error first (a ring of the last ``keep``)."""
+        dev = b.F.device
+        pos = b.count % keep
+        sel = torch.arange(b.m, device=dev)[cm]
+        b.Fh[sel, pos[cm]] = b.F[cm]
+        b.Eh[sel, pos[cm]] = b.err[cm]
+        b.count = torch.where(cm, b.count + 1, b.count)
+        used = torch.arange(keep, device=dev)[None, :] < b.count.clamp(max=keep)[:, None]      # (m, keep)
+        Ef = b.Eh.reshape(b.m, keep, -1)
+        B = torch.bmm(Ef, Ef.transpose(1, 2))
+        scale = torch.diagonal(B, dim1=1, dim2=2).amax(1).clamp(min=1e-300)
+        B = B / scale[:, None, None]
+        um = used[:, :, None] & used[:, None, :]
+        eye = torch.eye(keep, dtype=B.dtype, device=dev)
+        B = torch.where(um, B, eye.expand_as(B) * (~used)[:, :, None].to(B.dtype))
+        A = torch.zeros((b.m, keep + 1, keep + 1), dtype=B.dtype, device=dev)
+        A[:, :keep, :keep] = B
+        A[:, :keep, keep] = -used.to(B.dtype)
+        A[:, keep, :keep] = -used.to(B.dtype)
+        A[:, keep, keep] = (b.count == 0).to(B.dtype)      # nothing stored yet: keeps the system regular
+        rhs = torch.zeros((b.m, keep + 1), dtype=B.dtype, device=dev)
+        rhs[:, keep] = -1.0
+        c = torch.linalg.solve(A, rhs)[:, :keep]
+        Fx = torch.einsum("mk,mkij->mij", c, b.Fh)
+        return torch.where((b.count < 2)[:, None, None], b.F, Fx)
