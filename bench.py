@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--batch-mols", type=int, default=64,
                     help="clusters of the batch time-to-SCF measurement (0: skip; 256: the full batch)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-alkane", action="store_true", help="skip the C40H82 mixed-precision measurement")
     ap.add_argument("--waters", type=int, default=N_WATER,
                     help="cluster size (default 32: the benchmark workload; smaller sizes for profiling)")
     return ap.parse_args()
@@ -201,6 +202,39 @@ def time_to_scf(mol, fb, device):
     base = out["fp64_core"]["seconds"]
     out["speedup_vs_fp64_core"] = {k: round(base / v["seconds"], 3) for k, v in out.items() if isinstance(v, dict)}
     return out
+
+
+def mixed_precision_alkane(device: int):
+    """All-trans C40H82 def2-SVP (970 functions): the FP64 SCF from the core guess
+    against the mixed-precision incremental SCF (quartets with Schwarz x density
+    bound below 1e-6 in FP32, FP64 roots, weights and accumulation; the last two
+    cycles rebuilt in FP64), and the energy error of one all-mixed build at the
+    converged density."""
+    import torch
+    from tonto_b200.fock import TF_JK_MIXED
+    from tonto_b200.molecules import alkane
+    from tonto_b200.scf import RHF
+    mol = alkane(40, seed=0)
+    rhf = RHF(mol, schwarz_cutoff=SCHWARZ, device=device, mixed_fp32_cut=1e-6)
+    r64 = rhf.run(conv=1e-9, diis_tol=1e-6)
+    rmx = rhf.run(conv=1e-9, diis_tol=1e-6, mixed=True, incremental=True)
+    P = r64.P.contiguous()
+    e = {}
+    st = None
+    for name, flags in (("fp64", 0), ("mixed", TF_JK_MIXED)):
+        J, K = rhf.jk(P, flags)
+        F = rhf.H + J - 0.5 * K
+        e[name] = float(0.5 * torch.sum(P * (rhf.H + F))) + rhf.e_nuc
+        st = rhf.fb.stats()
+    rhf.fb.close()
+    return {"workload": "C40H82 all-trans, def2-SVP spherical, 970 bf, Schwarz 1e-12, FP32 below bound 1e-6",
+            "fp64": {"energy": r64.energy, "iterations": r64.iterations, "seconds": round(r64.seconds, 3),
+                     "converged": r64.converged},
+            "mixed_incremental_final_fp64": {"energy": rmx.energy, "iterations": rmx.iterations,
+                                             "seconds": round(rmx.seconds, 3), "converged": rmx.converged,
+                                             "energy_error_vs_fp64": rmx.energy - r64.energy},
+            "one_mixed_build_at_converged_density": {"energy_error_vs_fp64": e["mixed"] - e["fp64"],
+                                                     "fp32_quartet_fraction": st["quartets_fp32"] / st["quartets"]}}
 
 
 def time_to_scf_batch(n_mol: int, device: int):
@@ -410,6 +444,8 @@ def main():
         line["time_to_scf"] = time_to_scf(mol, fb, local)
         if args.batch_mols > 0:
             line["time_to_scf_batch"] = time_to_scf_batch(args.batch_mols, local)
+        if not args.no_alkane:
+            line["mixed_precision_alkane"] = mixed_precision_alkane(local)
 
     if rank == 0 and world == 1 and not args.no_cpu:
         orc, stride, cores = cpu_sample(mol, np.asfortranarray(P.cpu().numpy()), target_s=15.0)

@@ -85,7 +85,8 @@ typedef struct tf_options {
   double eri_primitive_pair_cutoff;  /* SHELL1QUARTET pair_cutoff (Tonto default 1e-6, macros.in:695) */
   double mixed_fp32_cut;             /* TF_JK_MIXED: Schwarz x density bound below which FP32 is used */
   int device;                        /* CUDA device ordinal */
-  int deterministic;                 /* 1: atomics-free privatised accumulation (bitwise reproducible) */
+  int deterministic;                 /* reserved, set 0: J and K accumulate with FP64 atomics
+                                        (reproducible to rounding, not bitwise) */
 } tf_options;
 
 typedef struct tf_stats {
