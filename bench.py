@@ -159,11 +159,12 @@ def cpu_sample(mol, P_np, target_s: float):
     oracle.build()
     orc = oracle.Oracle(mol, schwarz_cutoff=SCHWARZ)
     cores = os.cpu_count() or 1
-    stride = 1024
+    # calibrate on every 128th bra pair (enough work items to load all cores evenly),
+    # then choose the stride so that one sample takes about target_s
+    stride = 128
     t = orc.jk_sample(P_np, stride, 0, cores)
-    # choose the stride so that one sample takes about target_s
     est_full = t * stride
-    stride = max(1, int(math.ceil(est_full / target_s)))
+    stride = max(1, int(math.floor(est_full / target_s)))
     return orc, stride, cores
 
 
