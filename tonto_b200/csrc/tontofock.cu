@@ -266,6 +266,13 @@ struct ListArgs {
   double fp32_cut;              // 0: no FP32 quartets
   long long out_base;           // list index of out[0] (chunked list writes)
   long long out_cap;            // entries of out (writes beyond are dropped; the host sees the count)
+  // screening record (optional): the counting pass stores one byte per candidate
+  // ket (its bucket, or 0xff when screened out) at cand[cand_off[t] + j] and the
+  // number of candidates it examined in task_len[t]; the writing pass then only
+  // compacts, without screening again
+  unsigned char* cand;
+  const long long* cand_off;
+  int* task_len;
 };
 
 __device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo& mi, const PairRec& b,
@@ -296,30 +303,51 @@ __device__ __forceinline__ long long slot(const ListArgs& a, long long t, int g,
   return t0 * NBUCKET + (long long)bucket * nt + (t - t0);
 }
 
-template <bool WRITE>
-__global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const long long* __restrict__ offsets,
-                           int2* __restrict__ out) {
+// One warp per bra task.  MODE 0: screen every candidate ket and count the
+// survivors per bucket (and record the screening when a.cand is set); MODE 1:
+// screen again and write the survivors; MODE 2: write the survivors from the
+// recorded screening.  Lanes are grouped by bucket with one warp match per 32
+// candidates; per-warp bucket counters live in shared memory.
+constexpr int LIST_THREADS = 256;
+
+template <int MODE>
+__global__ void __launch_bounds__(LIST_THREADS) k_quartets(ListArgs a, long long* __restrict__ counts,
+                                                           const long long* __restrict__ offsets,
+                                                           int2* __restrict__ out) {
+  __shared__ int scnt[LIST_THREADS / 32][NBUCKET];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long t = a.t_base + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (t >= a.n_tasks) return;
+  if (t >= a.n_tasks) return;                    // uniform over the warp
+  for (int k = lane; k < NBUCKET; k += 32) scnt[warp][k] = 0;
+  __syncwarp();
   const int2 task = a.tasks[t];
   const CPUnit cp = a.units[task.x];
   const int g = a.unit_group[task.x];
-  const MolInfo mi = a.mols[cp.mol];
   const int i = task.y;
   const int bra = a.sorted[cp.bra_off + i];
-  const double Ib = a.sorted_imax[cp.bra_off + i];
-  const PairRec b = a.pairs[bra];
   const int jend = (cp.p1 == cp.p2) ? i + 1 : cp.n_ket;
-  const double pg = __longlong_as_double((long long)a.pglob[cp.mol]);
-  int cnt[NBUCKET];
-#pragma unroll
-  for (int k = 0; k < NBUCKET; ++k) cnt[k] = 0;
-  for (int j0 = 0; j0 < jend; j0 += 32) {
+  const long long coff = a.cand ? a.cand_off[t] : 0;
+  const int len = MODE == 2 ? a.task_len[t] : jend;
+  double Ib = 0.0, pg = 0.0;
+  PairRec b{};
+  MolInfo mi{};
+  if (MODE != 2) {
+    Ib = a.sorted_imax[cp.bra_off + i];
+    b = a.pairs[bra];
+    mi = a.mols[cp.mol];
+    pg = __longlong_as_double((long long)a.pglob[cp.mol]);
+  }
+  int scanned = 0;
+  for (int j0 = 0; j0 < len; j0 += 32) {
     const int j = j0 + lane;
-    bool ok = false, beyond = false;
-    int ket = 0, bucket = 0;
-    if (j < jend) {
+    bool beyond = false;
+    int ket = 0, bucket = -1;
+    if (MODE == 2) {
+      if (j < len) {
+        const unsigned char cb = a.cand[coff + j];
+        if (cb != 0xff) { bucket = cb; ket = a.sorted[cp.ket_off + j]; }
+      }
+    } else if (j < jend) {
       const double Ik = a.sorted_imax[cp.ket_off + j];
       if (!(Ib * a.sorted_bmax[cp.ket_off + j] * pg > a.cutoff)) {
         beyond = true;                           // bands are in decreasing I_max: nothing further survives
@@ -327,24 +355,27 @@ __global__ void k_quartets(ListArgs a, long long* __restrict__ counts, const lon
         ket = a.sorted[cp.ket_off + j];
         const PairRec k = a.pairs[ket];
         const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
-        ok = bound > a.cutoff;
-        if (ok) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
+        if (bound > a.cutoff) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
       }
+      if (MODE == 0 && a.cand) a.cand[coff + j] = bucket >= 0 ? (unsigned char)bucket : (unsigned char)0xff;
     }
-#pragma unroll
-    for (int k = 0; k < NBUCKET; ++k) {
-      const unsigned m = __ballot_sync(0xffffffffu, ok && bucket == k);
-      if (WRITE && ok && bucket == k) {
-        const long long pos = offsets[slot(a, t, g, k)] - a.out_base + cnt[k] + __popc(m & ((1u << lane) - 1u));
-        if (pos < a.out_cap) out[pos] = make_int2(bra, ket);
-      }
-      cnt[k] += __popc(m);
+    const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const int base = bucket >= 0 ? scnt[warp][bucket] : 0;
+    __syncwarp();
+    if (bucket >= 0 && rank == 0) scnt[warp][bucket] = base + __popc(peers);
+    __syncwarp();
+    if (MODE != 0 && bucket >= 0) {
+      const long long pos = offsets[slot(a, t, g, bucket)] - a.out_base + base + rank;
+      if (pos < a.out_cap) out[pos] = make_int2(bra, ket);
     }
-    if (__any_sync(0xffffffffu, beyond)) break;
+    scanned = j0 + 32;
+    if (MODE != 2 && __any_sync(0xffffffffu, beyond)) break;
   }
-  if (!WRITE && lane == 0)
-#pragma unroll
-    for (int k = 0; k < NBUCKET; ++k) counts[slot(a, t, g, k)] = cnt[k];
+  if (MODE == 0) {
+    for (int k = lane; k < NBUCKET; k += 32) counts[slot(a, t, g, k)] = scnt[warp][k];
+    if (a.cand && lane == 0) a.task_len[t] = min(scanned, jend);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1155,6 +1186,9 @@ struct tf_ctx {
   std::vector<int2> group_cls;                           // (bra class, ket class) of each group
   long long n_tasks = 0;
   long long list_budget = 1LL << 30;                     // quartets per list chunk (8 B each)
+  // screening record: one byte per candidate (bra task, ket) pair, when it fits
+  bool use_cand = false;
+  long long cand_budget = 12LL << 30;                    // bytes
   int shard_index = 0, shard_count = 1;                  // round-robin share of the bra tasks
   bool geometry_ready = false;
   // device
@@ -1168,7 +1202,9 @@ struct tf_ctx {
   tf::DBuf<tf::PrimPair> d_prim_full, d_prim_skip;
   tf::DBuf<int2> d_tasks, d_quartets;
   tf::DBuf<tf::CPUnit> d_units;
-  tf::DBuf<int> d_unit_group, d_group_task0;
+  tf::DBuf<int> d_unit_group, d_group_task0, d_task_len;
+  tf::DBuf<unsigned char> d_cand;
+  tf::DBuf<long long> d_task_cand_off;
   tf::DBuf<long long> d_counts, d_offsets, d_group_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
   tf::DBuf<unsigned char> d_scan_tmp;
@@ -1257,6 +1293,21 @@ static int build_tasks(tf_ctx* c) {
     }
   c->group_task0.push_back((int)tasks.size());
   c->n_tasks = (long long)tasks.size();
+  // candidate kets per task (all that a task may examine), for the screening record
+  std::vector<long long> cand_off(tasks.size() + 1, 0);
+  for (size_t t = 0; t < tasks.size(); ++t) {
+    const CPUnit& u = c->units[tasks[t].x];
+    cand_off[t + 1] = cand_off[t] + (u.p1 == u.p2 ? tasks[t].y + 1 : u.n_ket);
+  }
+  c->use_cand = false;
+  if (cand_off.back() <= c->cand_budget && c->d_cand.reserve(std::max<long long>(cand_off.back(), 1)) == cudaSuccess &&
+      c->d_task_cand_off.reserve(cand_off.size()) == cudaSuccess &&
+      c->d_task_len.reserve(std::max<size_t>(tasks.size(), 1)) == cudaSuccess) {
+    TF_CUDA(cudaMemcpyAsync(c->d_task_cand_off.p, cand_off.data(), cand_off.size() * sizeof(long long),
+                            cudaMemcpyHostToDevice, c->stream));
+    c->use_cand = true;
+  }
+  cudaGetLastError();
   const size_t ng = c->group_cls.size();
   TF_CUDA(c->d_units.reserve(std::max<size_t>(c->units.size(), 1)));
   TF_CUDA(c->d_unit_group.reserve(std::max<size_t>(c->unit_group.size(), 1)));
@@ -1538,11 +1589,12 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   kernels++;
   la = ListArgs{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
                 c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_pairs.p,  c->d_mols.p,  c->d_pmax.p,
-                c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX};
-  const long long thr_list = 256;
+                c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX,
+                c->use_cand ? c->d_cand.p : nullptr, c->d_task_cand_off.p, c->d_task_len.p};
+  const long long thr_list = LIST_THREADS;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   const long long nslots = c->n_tasks * NBUCKET;
-  k_quartets<false><<<grid_list, (unsigned)thr_list, 0, s>>>(la, c->d_counts.p, nullptr, nullptr);
+  k_quartets<0><<<grid_list, (unsigned)thr_list, 0, s>>>(la, c->d_counts.p, nullptr, nullptr);
   kernels++;
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
@@ -1597,9 +1649,10 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
   if (rc) return rc;
   ListArgs lw = la;
   lw.out_cap = c->graph_cap;
-  const long long thr_list = 256;
+  const long long thr_list = LIST_THREADS;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
-  k_quartets<true><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
+  if (c->use_cand) k_quartets<2><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
+  else k_quartets<1><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
   kernels++;
   const int ng = (int)c->group_cls.size();
   // class schedule: the class launches are spread over sched_streams branches of
@@ -1799,7 +1852,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     drop_graph(c);
     c->graph_cap = 0;
   }
-  const long long thr_list = 256;
+  const long long thr_list = LIST_THREADS;
   for (size_t ci = 0; ci + 1 < chunk.size(); ++ci) {
     const int g0 = chunk[ci], g1 = chunk[ci + 1];
     const long long base = goff[3 * g0], nq = goff[3 * (g1 - 1) + 2] - base;
@@ -1810,7 +1863,10 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       lw.out_base = base;
       const unsigned grid_w =
           (unsigned)std::max<long long>(1, ((lw.n_tasks - lw.t_base) * 32 + thr_list - 1) / thr_list);
-      k_quartets<true><<<grid_w, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
+      if (c->use_cand)
+        k_quartets<2><<<grid_w, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
+      else
+        k_quartets<1><<<grid_w, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
       kernels++;
     }
     for (int g = g0; g < g1; ++g) {
