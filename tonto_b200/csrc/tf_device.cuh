@@ -28,6 +28,36 @@
 namespace tf {
 
 // ---------------------------------------------------------------------------
+// Reciprocal and reciprocal square root by Newton-Raphson iteration, seeded by
+// the PTX approximate instructions rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64
+// (about 20 correct bits).  Each step squares the relative error:
+//   1/x:       y <- y + y (1 - x y)
+//   1/sqrt(x): y <- y + y (1/2 - (x/2) y^2)
+// so two steps reach the double-precision rounding level (a few ulp; checked
+// against IEEE division and square root by tests/fast_math_check.cu).  Used for
+// the exponent sums, rho, the Boys-function ratio and 1/x of the asymptotic
+// rules: positive normal numbers far from the overflow range.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double h = 0.5 * x;
+  double e = fma(-h * y, y, 0.5);
+  y = fma(y, e, y);
+  e = fma(-h * y, y, 0.5);
+  return fma(y, e, y);
+}
+
+// ---------------------------------------------------------------------------
 // compile-time helpers
 // ---------------------------------------------------------------------------
 template <int... Is, class F>
@@ -181,8 +211,8 @@ __device__ __forceinline__ void rys_eval(double x, double (&u)[N], double (&w)[N
       if (f < N) u[f] = v; else w[f - N] = v;
     }
   } else {
-    const double ix = 1.0 / x;
-    const double isx = sqrt(ix);
+    const double ix = rcp_nr(x);
+    const double isx = rsqrt_nr(x);
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       u[i] = tf_rys_hroot2[HOFF + i] * ix;
@@ -230,8 +260,8 @@ struct RysSmem {
         }
     } else {
       constexpr int HOFF = rys_hoffset(N);
-      const double ix = 1.0 / x;
-      const double isx = sqrt(ix);
+      const double ix = rcp_nr(x);
+      const double isx = rsqrt_nr(x);
 #pragma unroll
       for (int i = 0; i < N; ++i) {
         u[i] = tf_rys_hroot2[HOFF + i] * ix;
@@ -275,12 +305,11 @@ struct RysSmem<1> {
       a = fma(d, a, f01.x);
       b = fma(d, b, f01.y);
       w[0] = a;
-      u[0] = b / a;
+      u[0] = b * rcp_nr(a);
     } else {
       constexpr int HOFF = rys_hoffset(1);
-      const double ix = 1.0 / x;
-      u[0] = tf_rys_hroot2[HOFF] * ix;
-      w[0] = tf_rys_hweight[HOFF] * sqrt(ix);
+      u[0] = tf_rys_hroot2[HOFF] * rcp_nr(x);
+      w[0] = tf_rys_hweight[HOFF] * rsqrt_nr(x);
     }
   }
 };
@@ -364,14 +393,14 @@ __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp,
         if (ik < nkp) load_ket(ik);
       }
       const double eta = k0.w, half_einv = k1.w;
-      const double inv = 1.0 / (zeta + eta);
+      const double inv = rcp_nr(zeta + eta);
       const double rho = zeta * eta * inv;
       const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
       const double xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
       double u[NR], w[NR];
       if (rys_smem) RysSmem<NR>::eval(rys_smem, xx, u, w);
       else rys_eval<NR>(xx, u, w);
-      const double scale = bcc * kcc * sqrt(rho);
+      const double scale = bcc * kcc * (rho * rsqrt_nr(rho));
       const double r_z = eta * inv;     // rho / zeta
       const double r_e = zeta * inv;    // rho / eta
 #pragma unroll

@@ -189,11 +189,11 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         b0 = ld4(bp + ib, 0); b1 = ld4(bp + ib, 1);
         k0 = ld4(kp + ik, 0); k1 = ld4(kp + ik, 1);
         const double bcc = __ldg(&bp[ib].cc) * TWOPI5ON2, kcc = __ldg(&kp[ik].cc);
-        inv = 1.0 / (b0.w + k0.w);
+        inv = rcp_nr(b0.w + k0.w);
         const double rho = b0.w * k0.w * inv;
         const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
         rys_eval<NR>(rho * (QPx * QPx + QPy * QPy + QPz * QPz), u, w);
-        scale = bcc * kcc * sqrt(rho);
+        scale = bcc * kcc * (rho * rsqrt_nr(rho));
         r_z = k0.w * inv;
         r_e = b0.w * inv;
       }

@@ -65,7 +65,7 @@ __device__ int warp_quartet(const WarpQuartet& q, const PrimPair* __restrict__ b
       const double4 k1 = ld4(kp + ik, 1);
       const double kcc = __ldg(&kp[ik].cc);
       const double zeta = b0.w, eta = k0.w;
-      const double inv = 1.0 / (zeta + eta);
+      const double inv = rcp_nr(zeta + eta);
       const double rho = zeta * eta * inv;
       const double QP[3] = {k0.x - b0.x, k0.y - b0.y, k0.z - b0.z};
       const double xx = rho * (QP[0] * QP[0] + QP[1] * QP[1] + QP[2] * QP[2]);
@@ -77,7 +77,7 @@ __device__ int warp_quartet(const WarpQuartet& q, const PrimPair* __restrict__ b
         case 4: { double uu[4], ww[4]; rys_eval<4>(xx, uu, ww); for (int i = 0; i < 4; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
         default: { double uu[5], ww[5]; rys_eval<5>(xx, uu, ww); for (int i = 0; i < 5; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
       }
-      const double scale = bcc * kcc * sqrt(rho);
+      const double scale = bcc * kcc * (rho * rsqrt_nr(rho));
       const double r_z = eta * inv, r_e = zeta * inv;
       __syncwarp();
       // 2D tables: lane -> (direction, root)
