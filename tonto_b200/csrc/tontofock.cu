@@ -411,13 +411,18 @@ struct JKArgs {
 #ifndef TF_JK_MINB
 #define TF_JK_MINB 1
 #endif
-template <int LA, int LB, int LC, int LD>
+// Resident blocks per SM the compiler must allow (bounds the registers per thread).
+// Variant 0 leaves the registers to the compiler (one-root classes: 5 blocks);
+// variant 1 asks for more resident warps (6 blocks for one root, 4 otherwise),
+// at the price of fewer registers.  The autotuner times both per class.
+template <int LA, int LB, int LC, int LD, int V>
 constexpr int jk_min_blocks() {
-  return Quartet<LA, LB, LC, LD>::NROOT == 1 ? TF_JK_MINB_N1 : TF_JK_MINB;
+  return Quartet<LA, LB, LC, LD>::NROOT == 1 ? (V ? 6 : TF_JK_MINB_N1) : (V ? 4 : TF_JK_MINB);
 }
+constexpr int JK_VARIANTS = 2;
 
-template <int LA, int LB, int LC, int LD, typename T>
-__global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD>()) k_jk(JKArgs a) {
+template <int LA, int LB, int LC, int LD, typename T, int V>
+__global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(JKArgs a) {
   using Q = Quartet<LA, LB, LC, LD>;
   using RS = RysSmem<Q::NROOT>;
   extern __shared__ double rys_tab[];
@@ -1226,6 +1231,7 @@ struct tf_ctx {
   // class schedule (autotuned): graph branches and the branch of each class pair
   int sched_streams = 1;
   std::vector<int> sched_stream_of;
+  std::vector<int> cls_variant;                          // launch-bound variant of each class pair's kernel
   std::vector<cudaStream_t> side;                        // branch streams besides the context stream
   cudaEvent_t fork_ev = nullptr;
   std::vector<cudaEvent_t> join_ev;
@@ -1293,6 +1299,7 @@ static int build_tasks(tf_ctx* c) {
     }
   c->group_task0.push_back((int)tasks.size());
   c->n_tasks = (long long)tasks.size();
+  c->cls_variant.resize(c->group_cls.size(), 0);
   // candidate kets per task (all that a task may examine), for the screening record
   std::vector<long long> cand_off(tasks.size() + 1, 0);
   for (size_t t = 0; t < tasks.size(); ++t) {
@@ -1470,13 +1477,13 @@ static void class_l(int k, int& lh, int& ll) {
 
 // Launch set-up (shared-memory attribute, resident blocks per SM), done once per
 // kernel and before any graph capture: a zero-sized, range-less JKArgs only sets up.
-template <int LA, int LB, int LC, int LD, typename T>
+template <int LA, int LB, int LC, int LD, typename T, int V>
 static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {
-    cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T>, 128, smem);
+    cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T, V>, 128, smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   if (a.n <= 0 && !a.range) return;
@@ -1486,13 +1493,18 @@ static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   const int thr = 128;
   const long long full = (long long)nsm * blocks_per_sm;
   const long long blocks = a.range ? full : std::min<long long>((a.n + thr - 1) / thr, full);
-  k_jk<LA, LB, LC, LD, T><<<(unsigned)blocks, thr, smem, s>>>(a);
+  k_jk<LA, LB, LC, LD, T, V><<<(unsigned)blocks, thr, smem, s>>>(a);
 }
 
 template <int LA, int LB, int LC, int LD>
-static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32) {
-  if (fp32) launch_jk_t<LA, LB, LC, LD, float>(a, s);
-  else launch_jk_t<LA, LB, LC, LD, double>(a, s);
+static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
+  if (variant == 1) {
+    if (fp32) launch_jk_t<LA, LB, LC, LD, float, 1>(a, s);
+    else launch_jk_t<LA, LB, LC, LD, double, 1>(a, s);
+  } else {
+    if (fp32) launch_jk_t<LA, LB, LC, LD, float, 0>(a, s);
+    else launch_jk_t<LA, LB, LC, LD, double, 0>(a, s);
+  }
 }
 
 constexpr int GROUP_WPB = 4;
@@ -1530,11 +1542,11 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
 
 // fp32: evaluate the 2D recurrences and (e0|f0) sums in FP32 (thread-per-quartet
 // classes); roots, weights, transfers and the Fock accumulation stay FP64.
-static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStream_t s, bool fp32) {
+static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStream_t s, bool fp32, int variant = 0) {
   const int key = ((la * 3 + lb) * 3 + lc) * 3 + ld;
   switch (key) {
 #define TF_CASE(A, B, C, D) \
-  case ((A * 3 + B) * 3 + C) * 3 + D: launch_jk<A, B, C, D>(a, s, fp32); return TF_OK;
+  case ((A * 3 + B) * 3 + C) * 3 + D: launch_jk<A, B, C, D>(a, s, fp32, variant); return TF_OK;
     TF_CASE(0, 0, 0, 0)
     TF_CASE(1, 0, 0, 0) TF_CASE(1, 0, 1, 0)
     TF_CASE(1, 1, 0, 0) TF_CASE(1, 1, 1, 0)
@@ -1674,11 +1686,11 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
              nullptr, nullptr, nullptr, want};
     JKArgs a32 = a;
     a32.range = c->d_group_offsets.p + 3 * g + 1;
-    rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false);
+    rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false, c->cls_variant[g]);
     if (rc != TF_OK) return rc;
     kernels++;
     if (mixed) {
-      rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, sg, true);
+      rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, sg, true, c->cls_variant[g]);
       if (rc != TF_OK) return rc;
       kernels++;
     }
@@ -1784,7 +1796,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
         class_l(c->group_cls[g].y, l2h, l2l);
         const JKArgs none{};
         for (int fp32 = 0; fp32 < 2; ++fp32) {
-          const int rc = dispatch_jk(l1h, l1l, l2h, l2l, none, s, fp32 != 0);
+          const int rc = dispatch_jk(l1h, l1l, l2h, l2l, none, s, fp32 != 0, c->cls_variant[g]);
           if (rc != TF_OK) return rc;
         }
       }
@@ -1882,12 +1894,12 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
       a32.n = goff[3 * g + 2] - goff[3 * g + 1];
       if (a.n > 0) {
-        rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false);
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false, c->cls_variant[g]);
         if (rc != TF_OK) return rc;
         kernels++;
       }
       if (a32.n > 0) {
-        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true);
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true, c->cls_variant[g]);
         if (rc != TF_OK) return rc;
         kernels++;
       }
@@ -2115,14 +2127,37 @@ int tf_autotune(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, 
   if (!c->fork_ev) TF_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
   const bool use_graph = c->use_graph;
   tf_tune res{};
-  // class-pair times from a class-by-class build
+  const int ng = (int)c->group_cls.size();
+  // launch-bound variant of each class pair's kernel: class-by-class builds with
+  // every class on one variant (the first of two warms the kernels up), then per
+  // class the faster variant
   c->use_graph = false;
   drop_graph(c);
+  std::vector<std::vector<double>> tv(JK_VARIANTS, std::vector<double>(ng, 0.0));
+  for (int v = 0; v < JK_VARIANTS; ++v) {
+    std::fill(c->cls_variant.begin(), c->cls_variant.end(), v);
+    for (int rep = 0; rep < 2; ++rep) {
+      rc = build_jk_device(c, dP, dJ, dK, flags);
+      if (rc) { c->use_graph = use_graph; return rc; }
+    }
+    for (int g = 0; g < ng; ++g) {
+      float ms = 0.f;
+      TF_CUDA(cudaEventElapsedTime(&ms, c->cls_ev[2 * g], c->cls_ev[2 * g + 1]));
+      tv[v][g] = ms;
+    }
+  }
+  for (int g = 0; g < ng; ++g) {
+    int best_v = 0;
+    for (int v = 1; v < JK_VARIANTS; ++v)
+      if (tv[v][g] < tv[best_v][g] * 0.98) best_v = v;
+    c->cls_variant[g] = best_v;
+    if (best_v) res.variant_classes++;
+  }
+  // class-pair times from a class-by-class build with the chosen variants
   rc = build_jk_device(c, dP, dJ, dK, flags);
   c->use_graph = use_graph;
   if (rc) return rc;
   res.direct_ms = c->stats.build_ms;
-  const int ng = (int)c->group_cls.size();
   std::vector<double> t(ng, 0.0);
   for (int g = 0; g < ng; ++g) {
     float ms = 0.f;

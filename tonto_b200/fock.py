@@ -61,11 +61,11 @@ class Stats(ctypes.Structure):
 
 class Tune(ctypes.Structure):
     _fields_ = [("streams", ctypes.c_int), ("candidates", ctypes.c_int), ("ms", ctypes.c_double * 8),
-                ("direct_ms", ctypes.c_double)]
+                ("direct_ms", ctypes.c_double), ("variant_classes", ctypes.c_int)]
 
     def as_dict(self):
         return {"streams": self.streams, "candidates": self.candidates, "direct_ms": self.direct_ms,
-                "ms": [self.ms[i] for i in range(self.candidates)]}
+                "ms": [self.ms[i] for i in range(self.candidates)], "variant_classes": self.variant_classes}
 
 
 class ClassStats(ctypes.Structure):
