@@ -24,7 +24,8 @@ struct GroupCfg {
   static constexpr int G = Q::NF;
   static constexpr int QPW = 32 / G;
   static constexpr int NR = Q::NROOT, D1 = Q::LAB + 1, D2 = Q::LCD + 1;
-  static constexpr int T2D = 3 * NR * D1 * D2;
+  static constexpr int TS = (D1 * D2) | 1;     // one 2D table, odd stride (fewer bank conflicts)
+  static constexpr int T2D = 3 * NR * TS;
   static constexpr int ket_level(int k) {   // size after building d level k+1
     return Q::NE * (ncart_upto(LC + LD - k - 1) - ncart_upto(LC - 1)) * ncart(k + 1);
   }
@@ -130,6 +131,47 @@ struct GroupArgs {
   int want;                     // bit 0 J, bit 1 K
 };
 
+// Rys nodes and weights of a lane group's primitive quartet: the 2 N polynomial
+// pieces (u_1..u_N, w_1..w_N at the interval of x) are spread over the group's
+// G lanes, each evaluated once, then exchanged with shuffles, instead of every
+// lane of the group evaluating all of them.  x is uniform within a group; every
+// lane of the warp takes part.  gbase: the group's first lane.
+template <int N, int G>
+__device__ __forceinline__ void group_rys(double x, int gl, int gbase, double (&u)[N], double (&w)[N]) {
+  constexpr int NF2 = 2 * N, PER = (NF2 + G - 1) / G;
+  constexpr int XMAX = rys_xmax(N), OFF = rys_offset(N), HOFF = rys_hoffset(N);
+  const bool tab = x < (double)XMAX;
+  const int j = tab ? (int)x : 0;
+  const double s = x - (double)j;
+  double val[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int f = gl + q * G;
+    double v = 0.0;
+    if (tab && f < NF2) {
+      const double* cf = tf_rys_coef + OFF + j * (NF2 * TF_RYS_NCOEF) + f * TF_RYS_NCOEF;
+      v = __ldg(cf + TF_RYS_DEG);
+#pragma unroll
+      for (int k = TF_RYS_DEG - 1; k >= 0; --k) v = fma(v, s, __ldg(cf + k));
+    }
+    val[q] = v;
+  }
+#pragma unroll
+  for (int f = 0; f < NF2; ++f) {
+    const double v = __shfl_sync(0xffffffffu, val[f / G], gbase + f % G);
+    if (f < N) u[f] = v;
+    else w[f - N] = v;
+  }
+  if (!tab) {
+    const double ix = rcp_nr(x), isx = rsqrt_nr(x);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      u[i] = tf_rys_hroot2[HOFF + i] * ix;
+      w[i] = tf_rys_hweight[HOFF + i] * isx;
+    }
+  }
+}
+
 __constant__ unsigned char c_gcomp[3][NCOMP_ALL];
 __constant__ unsigned char c_gidx[(LCOMP + 1) * (LCOMP + 1) * (LCOMP + 1)];
 
@@ -137,7 +179,7 @@ template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
   using C = GroupCfg<LA, LB, LC, LD>;
   using Q = typename C::Q;
-  constexpr int G = C::G, QPW = C::QPW, NR = C::NR, D1 = C::D1, D2 = C::D2, TS = D1 * D2;
+  constexpr int G = C::G, QPW = C::QPW, NR = C::NR, D1 = C::D1, D2 = C::D2, TS = C::TS;
   extern __shared__ double smem[];
   __shared__ SmemComp sc;
   for (int i = threadIdx.x; i < NCOMP_ALL; i += blockDim.x) {
@@ -184,7 +226,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
       double u[NR], w[NR];
       double4 b0 = make_double4(0, 0, 0, 1), b1 = make_double4(0, 0, 0, 0), k0 = make_double4(0, 0, 0, 1),
               k1 = make_double4(0, 0, 0, 0);
-      double inv = 0.0, r_z = 0.0, r_e = 0.0, scale = 0.0;
+      double inv = 0.0, r_z = 0.0, r_e = 0.0, scale = 0.0, xx = 0.0;
       if (v) {
         b0 = ld4(bp + ib, 0); b1 = ld4(bp + ib, 1);
         k0 = ld4(kp + ik, 0); k1 = ld4(kp + ik, 1);
@@ -192,11 +234,12 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         inv = rcp_nr(b0.w + k0.w);
         const double rho = b0.w * k0.w * inv;
         const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
-        rys_eval<NR>(rho * (QPx * QPx + QPy * QPy + QPz * QPz), u, w);
+        xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
         scale = bcc * kcc * (rho * rsqrt_nr(rho));
         r_z = k0.w * inv;
         r_e = b0.w * inv;
       }
+      group_rys<NR, G>(xx, gl, lane - (in_group ? gl : 0), u, w);
       __syncwarp();
       if (v) {
         for (int task = gl; task < 3 * NR; task += G) {
