@@ -25,6 +25,8 @@ Optional modes (none changes the converged answer):
 
 from __future__ import annotations
 
+import dataclasses
+
 import time
 from dataclasses import dataclass, field
 from typing import Callable, List, Optional
@@ -89,6 +91,14 @@ class RHF:
         self.dev = torch.device("cuda", device)
         self.fb = builder or FockBuilder(mol, schwarz_cutoff=schwarz_cutoff, device=device,
                                          mixed_fp32_cut=mixed_fp32_cut)
+        self._one_electron()
+        self.n_occ = mol.n_electrons // 2
+        self.diis_keep = diis_keep
+        n = mol.n_bf
+        self._J = torch.empty((n, n), dtype=torch.float64, device=self.dev)
+        self._K = torch.empty((n, n), dtype=torch.float64, device=self.dev)
+
+    def _one_electron(self):
         S, T, V = self.fb.one_electron()
         self.S = torch.tensor(np.ascontiguousarray(S), dtype=torch.float64, device=self.dev)
         self.T = torch.tensor(np.ascontiguousarray(T), dtype=torch.float64, device=self.dev)
@@ -96,12 +106,18 @@ class RHF:
         self.H = self.T + self.V
         e, U = torch.linalg.eigh(self.S)
         self.X = (U / torch.sqrt(e)) @ U.T
-        self.n_occ = mol.n_electrons // 2
-        self.e_nuc = mol.nuclear_repulsion()
-        self.diis_keep = diis_keep
-        n = mol.n_bf
-        self._J = torch.empty((n, n), dtype=torch.float64, device=self.dev)
-        self._K = torch.empty((n, n), dtype=torch.float64, device=self.dev)
+        self.e_nuc = self.mol.nuclear_repulsion()
+
+    def set_geometry(self, xyz_bohr) -> None:
+        """Move the atoms (same atoms and basis), as Tonto's Hirshfeld-atom refinement
+        does between SCFs (molecule.har.foo:352-491): the library rebuilds the pair
+        data and Schwarz bounds (tf_set_geometry), the one-electron matrices are
+        recomputed, and the next run may start from the previous density."""
+        xyz = np.asarray(xyz_bohr, dtype=np.float64).reshape(self.mol.n_atom, 3)
+        self.mol = dataclasses.replace(self.mol, xyz=xyz)
+        self.fb.set_geometry(xyz)
+        self.fb.mol = self.mol
+        self._one_electron()
 
     def density(self, F: torch.Tensor):
         e, C = torch.linalg.eigh(self.X.T @ F @ self.X)
