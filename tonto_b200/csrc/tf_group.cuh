@@ -53,6 +53,108 @@ __device__ __forceinline__ int sc_idx(const SmemComp& s, int x, int y, int z) {
   return s.idx[(x * (LCOMP + 1) + y) * (LCOMP + 1) + z];
 }
 
+// Index plan of the horizontal transfers of one class, built at compile time from
+// the component tables: for every produced element of every level (ket levels
+// first, then bra levels) the two source positions and the direction, packed as
+// s1 | s2 << 13 | dir << 26, so that a lane does one table load per element
+// instead of the component-table lookups.
+template <int LA, int LB, int LC, int LD>
+struct HrrPlan {
+  using Q = Quartet<LA, LB, LC, LD>;
+  static constexpr int ket_tot(int k) {
+    return Q::NE * (ncart_upto(LC + LD - k - 1) - ncart_upto(LC - 1)) * ncart(k + 1);
+  }
+  static constexpr int bra_tot(int k) {
+    return (ncart_upto(LA + LB - k - 1) - ncart_upto(LA - 1)) * ncart(k + 1) * Q::NC * Q::ND;
+  }
+  static constexpr int ket_off(int k) { int o = 0; for (int i = 0; i < k; ++i) o += ket_tot(i); return o; }
+  static constexpr int bra_off(int k) {
+    int o = ket_off(LD);
+    for (int i = 0; i < k; ++i) o += bra_tot(i);
+    return o;
+  }
+  static constexpr int N = bra_off(LB) > 0 ? bra_off(LB) : 1;
+  int code[N];
+};
+
+template <int LA, int LB, int LC, int LD>
+constexpr HrrPlan<LA, LB, LC, LD> make_hrr_plan() {
+  using P = HrrPlan<LA, LB, LC, LD>;
+  using Q = Quartet<LA, LB, LC, LD>;
+  P p{};
+  const int FF = ncart_upto(LC - 1), FE = ncart_upto(LA - 1);
+  for (int k = 0; k < LD; ++k) {
+    const int NCR = ncart_upto(LC + LD - k) - FF, NY = ncart(k);
+    const int NCN = ncart_upto(LC + LD - k - 1) - FF, NYN = ncart(k + 1);
+    for (int t = 0; t < P::ket_tot(k); ++t) {
+      const int e = t / (NCN * NYN), rem = t - e * (NCN * NYN), c = rem / NYN, y1 = rem - c * NYN;
+      const int gy = ncart_upto(k) + y1;           // global index of the level-(k+1) component
+      const int px = CT.x[gy], py = CT.y[gy], pz = CT.z[gy];
+      const int dir = px > 0 ? 0 : (py > 0 ? 1 : 2);
+      const int y0 = CT.idx[px - (dir == 0)][py - (dir == 1)][pz - (dir == 2)];
+      const int g = FF + c;
+      const int ax = CT.x[g] + (dir == 0), ay = CT.y[g] + (dir == 1), az = CT.z[g] + (dir == 2);
+      const int gp = ncart_upto(ax + ay + az - 1) + CT.idx[ax][ay][az] - FF;
+      const int s1 = (e * NCR + gp) * NY + y0, s2 = (e * NCR + c) * NY + y0;
+      p.code[P::ket_off(k) + t] = s1 | (s2 << 13) | (dir << 26);
+    }
+  }
+  const int NCD = Q::NC * Q::ND;
+  for (int k = 0; k < LB; ++k) {
+    const int NBY = ncart(k), NAN_ = ncart_upto(LA + LB - k - 1) - FE, NBN = ncart(k + 1);
+    for (int t = 0; t < P::bra_tot(k); ++t) {
+      const int a = t / (NBN * NCD), rem = t - a * (NBN * NCD), b1 = rem / NCD, r = rem - b1 * NCD;
+      const int gb = ncart_upto(k) + b1;
+      const int px = CT.x[gb], py = CT.y[gb], pz = CT.z[gb];
+      const int dir = px > 0 ? 0 : (py > 0 ? 1 : 2);
+      const int b0 = CT.idx[px - (dir == 0)][py - (dir == 1)][pz - (dir == 2)];
+      const int g = FE + a;
+      const int ax = CT.x[g] + (dir == 0), ay = CT.y[g] + (dir == 1), az = CT.z[g] + (dir == 2);
+      const int gp = ncart_upto(ax + ay + az - 1) + CT.idx[ax][ay][az] - FE;
+      const int s1 = (gp * NBY + b0) * NCD + r, s2 = (a * NBY + b0) * NCD + r;
+      p.code[P::bra_off(k) + t] = s1 | (s2 << 13) | (dir << 26);
+    }
+  }
+  return p;
+}
+
+template <int LA, int LB, int LC, int LD>
+__device__ const HrrPlan<LA, LB, LC, LD> g_hrr_plan = make_hrr_plan<LA, LB, LC, LD>();
+
+// Horizontal transfers of one group's block in shared memory, from the index plan.
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ double* group_hrr_plan(double* src, double* dst, const double* Rab, const double* Rcd,
+                                                  int gl) {
+  using P = HrrPlan<LA, LB, LC, LD>;
+  constexpr int G = GroupCfg<LA, LB, LC, LD>::G;
+  const int* code = g_hrr_plan<LA, LB, LC, LD>.code;
+  static_for<LD>([&](auto kk) {
+    constexpr int k = decltype(kk)::value;
+    constexpr int TOT = P::ket_tot(k), OFF = P::ket_off(k);
+    for (int t = gl; t < TOT; t += G) {
+      const int cd = __ldg(code + OFF + t);
+      const int dir = cd >> 26;
+      const double R = dir == 0 ? Rcd[0] : (dir == 1 ? Rcd[1] : Rcd[2]);
+      dst[t] = src[cd & 0x1fff] + R * src[(cd >> 13) & 0x1fff];
+    }
+    __syncwarp();
+    double* tmp = src; src = dst; dst = tmp;
+  });
+  static_for<LB>([&](auto kk) {
+    constexpr int k = decltype(kk)::value;
+    constexpr int TOT = P::bra_tot(k), OFF = P::bra_off(k);
+    for (int t = gl; t < TOT; t += G) {
+      const int cd = __ldg(code + OFF + t);
+      const int dir = cd >> 26;
+      const double R = dir == 0 ? Rab[0] : (dir == 1 ? Rab[1] : Rab[2]);
+      dst[t] = src[cd & 0x1fff] + R * src[(cd >> 13) & 0x1fff];
+    }
+    __syncwarp();
+    double* tmp = src; src = dst; dst = tmp;
+  });
+  return src;
+}
+
 // Horizontal transfers of one group's block in shared memory.  On entry `src`
 // holds es[e][f]; on exit the returned pointer holds (ab|cd) as
 // [a][b][c*ND + d].  `gl` is the lane within the group, `G` the group size.
@@ -304,7 +406,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
     const double Rab[3] = {b.Rx, b.Ry, b.Rz};
     const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
     // lanes outside every group start beyond all element loops (they only keep the warp in step)
-    const double* I = group_hrr<LA, LB, LC, LD>(B0, B1, sc, Rab, Rcd, in_group ? gl : 0x40000000);
+    const double* I = group_hrr_plan<LA, LB, LC, LD>(B0, B1, Rab, Rcd, in_group ? gl : 0x40000000);
     if (act) {
       const MolInfo mi = a.mols[b.mol];
       const int n = mi.n_cart;
