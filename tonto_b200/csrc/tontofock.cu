@@ -517,6 +517,14 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
     // (twice for an unrestricted build: alpha and beta densities)
     auto digest_k = [&](const double* __restrict__ P, double* __restrict__ Km) {
       double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
+      double Kbc[Q::NB][Q::NC], Kbd[Q::NB][Q::ND];
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c) Kbc[ib][c] = 0.0;
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d) Kbd[ib][d] = 0.0;
+      }
 #pragma unroll
       for (int ib = 0; ib < Q::NB; ++ib) {
 #pragma unroll
@@ -552,20 +560,22 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
 #pragma unroll
         for (int ib = 0; ib < Q::NB; ++ib) {
 #pragma unroll
-          for (int c = 0; c < Q::NC; ++c) {
-            double s = 0.0;
+          for (int c = 0; c < Q::NC; ++c)
 #pragma unroll
-            for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pad[d];
-            atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
-          }
+            for (int d = 0; d < Q::ND; ++d) Kbc[ib][c] += I[ia][ib][c * Q::ND + d] * Pad[d];
 #pragma unroll
-          for (int d = 0; d < Q::ND; ++d) {
-            double s = 0.0;
+          for (int d = 0; d < Q::ND; ++d)
 #pragma unroll
-            for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pac[c];
-            atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
-          }
+            for (int c = 0; c < Q::NC; ++c) Kbd[ib][d] += I[ia][ib][c * Q::ND + d] * Pac[c];
         }
+      }
+      // K(bc), K(bd): summed over the a components first, one atomic per element
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c) atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * Kbc[ib][c]);
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d) atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * Kbd[ib][d]);
       }
     };
     if (active && (a.want & 2)) {
