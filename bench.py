@@ -431,7 +431,7 @@ def main():
                        "between timed builds", "parallelism": f"round-robin bra pairs x{world} + NCCL all-reduce"
                        if world > 1 else "single GPU",
                        "class_schedule": {"graph_branches": tune["streams"],
-                                          "more_warps_classes": tune["variant_classes"],
+                                          "non_default_kernel_variants": tune["variant_classes"],
                                           "autotune_ms": [round(v, 3) for v in tune["ms"]]}},
             "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(st["kernels"]) * args.steps,
             "e2e": e2e,

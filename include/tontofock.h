@@ -178,13 +178,14 @@ typedef struct tf_tune {
   int candidates;                    /* schedules timed (1 .. max_streams branches) */
   double ms[8];                      /* best graph build time of each candidate */
   double direct_ms;                  /* the class-by-class build used for the class times */
-  int variant_classes;               /* class pairs whose kernel runs the more-warps variant */
+  int variant_classes;               /* class pairs whose kernel runs a variant other than the default */
 } tf_tune;
 
 /* Autotuner for the kernels and the class schedule of graph builds.  Class-by-class
  * builds of the density dP (device arrays as tf_build_jk_device) time each class
- * pair's kernel in two launch-bound variants (registers left to the compiler, or
- * more resident warps) and keep the faster per class pair; a further build gives
+ * pair's kernel in four variants (registers left to the compiler or more resident
+ * warps; exchange atomics per lane or summed first over lanes that hit the same
+ * element) and keep the fastest per class pair; a further build gives
  * each class pair's device time; then for 1 .. max_streams (<= 8) graph branches the class pairs
  * are assigned longest first to the least-loaded branch, each schedule is
  * captured and timed over three builds, and the fastest is kept for this

@@ -417,9 +417,11 @@ struct JKArgs {
 // at the price of fewer registers.  The autotuner times both per class.
 template <int LA, int LB, int LC, int LD, int V>
 constexpr int jk_min_blocks() {
-  return Quartet<LA, LB, LC, LD>::NROOT == 1 ? (V ? 6 : TF_JK_MINB_N1) : (V ? 4 : TF_JK_MINB);
+  return Quartet<LA, LB, LC, LD>::NROOT == 1 ? ((V & 1) ? 6 : TF_JK_MINB_N1) : ((V & 1) ? 4 : TF_JK_MINB);
 }
-constexpr int JK_VARIANTS = 2;
+// Variant bits: 1 = more resident warps (see above); 2 = K atomics of lanes that hit
+// the same element summed first (segmented warp sums, bra-uniform warps).
+constexpr int JK_VARIANTS = 4;
 
 template <int LA, int LB, int LC, int LD, typename T, int V>
 __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(JKArgs a) {
@@ -515,6 +517,39 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
     // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
     // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
     // (twice for an unrestricted build: alpha and beta densities)
+    // Variant bit 2: the K rows a and b are the same for all lanes of a bra-uniform
+    // warp, and lanes whose kets share the c (or d) shell add to the same K
+    // elements.  Such lanes are neighbours (pair-id order), so each run of equal
+    // keys is summed with a segmented warp scan and added once, by its last lane.
+    constexpr bool SEG = (V & 2) != 0;
+    int segc = lane, segd = lane;
+    bool tailc = true, taild = true;
+    if constexpr (SEG) {
+      const int keyc = uni ? oc : -1 - lane, keyd = uni ? od : -1 - lane;
+      const unsigned lt_mask = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+      // (every lane executes both shuffles: none may be skipped by a short-circuit)
+      const int upc = __shfl_up_sync(0xffffffffu, keyc, 1), upd = __shfl_up_sync(0xffffffffu, keyd, 1);
+      const unsigned headc = __ballot_sync(0xffffffffu, lane == 0 || keyc != upc);
+      const unsigned headd = __ballot_sync(0xffffffffu, lane == 0 || keyd != upd);
+      segc = 31 - __clz(headc & lt_mask);
+      segd = 31 - __clz(headd & lt_mask);
+      tailc = lane == 31 || ((headc >> (lane + 1)) & 1u);
+      taild = lane == 31 || ((headd >> (lane + 1)) & 1u);
+    }
+    auto kadd = [&](double* addr, double v, int seg, bool tail) {
+      if constexpr (SEG) {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const double t = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane - o >= seg) v += t;
+        }
+        if (tail && v != 0.0) atomicAdd(addr, v);
+      } else {
+        atomicAdd(addr, v);
+      }
+    };
+#define TF_KADD_C(addr, v) kadd((addr), (v), segc, tailc)
+#define TF_KADD_D(addr, v) kadd((addr), (v), segd, taild)
     auto digest_k = [&](const double* __restrict__ P, double* __restrict__ Km) {
       double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
       double Kbc[Q::NB][Q::NC], Kbd[Q::NB][Q::ND];
@@ -546,7 +581,7 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
           for (int ib = 0; ib < Q::NB; ++ib)
 #pragma unroll
             for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pbd[ib][d];
-          atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
+          TF_KADD_C(Km + (size_t)(oa + ia) * n + oc + c, f * s);
         }
 #pragma unroll
         for (int d = 0; d < Q::ND; ++d) {
@@ -555,7 +590,7 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
           for (int ib = 0; ib < Q::NB; ++ib)
 #pragma unroll
             for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pbc[ib][c];
-          atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
+          TF_KADD_D(Km + (size_t)(oa + ia) * n + od + d, f * s);
         }
 #pragma unroll
         for (int ib = 0; ib < Q::NB; ++ib) {
@@ -573,15 +608,18 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
 #pragma unroll
       for (int ib = 0; ib < Q::NB; ++ib) {
 #pragma unroll
-        for (int c = 0; c < Q::NC; ++c) atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * Kbc[ib][c]);
+        for (int c = 0; c < Q::NC; ++c) TF_KADD_C(Km + (size_t)(ob + ib) * n + oc + c, f * Kbc[ib][c]);
 #pragma unroll
-        for (int d = 0; d < Q::ND; ++d) atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * Kbd[ib][d]);
+        for (int d = 0; d < Q::ND; ++d) TF_KADD_D(Km + (size_t)(ob + ib) * n + od + d, f * Kbd[ib][d]);
       }
     };
-    if (active && (a.want & 2)) {
+    // with segmented sums every lane takes part (idle lanes add f = 0)
+    if ((SEG || active) && (a.want & 2)) {
       digest_k(a.P + mi.cmat, a.K + mi.cmat);
       if (a.P2) digest_k(a.P2 + mi.cmat, a.K2 + mi.cmat);
     }
+#undef TF_KADD_C
+#undef TF_KADD_D
   }
   // primitive-quartet counter (per class, one atomic per warp)
 #pragma unroll
@@ -1506,14 +1544,19 @@ static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   k_jk<LA, LB, LC, LD, T, V><<<(unsigned)blocks, thr, smem, s>>>(a);
 }
 
+template <int LA, int LB, int LC, int LD, int V>
+static void launch_jk_v(const JKArgs& a, cudaStream_t s, bool fp32) {
+  if (fp32) launch_jk_t<LA, LB, LC, LD, float, V>(a, s);
+  else launch_jk_t<LA, LB, LC, LD, double, V>(a, s);
+}
+
 template <int LA, int LB, int LC, int LD>
 static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
-  if (variant == 1) {
-    if (fp32) launch_jk_t<LA, LB, LC, LD, float, 1>(a, s);
-    else launch_jk_t<LA, LB, LC, LD, double, 1>(a, s);
-  } else {
-    if (fp32) launch_jk_t<LA, LB, LC, LD, float, 0>(a, s);
-    else launch_jk_t<LA, LB, LC, LD, double, 0>(a, s);
+  switch (variant) {
+    case 1: launch_jk_v<LA, LB, LC, LD, 1>(a, s, fp32); break;
+    case 2: launch_jk_v<LA, LB, LC, LD, 2>(a, s, fp32); break;
+    case 3: launch_jk_v<LA, LB, LC, LD, 3>(a, s, fp32); break;
+    default: launch_jk_v<LA, LB, LC, LD, 0>(a, s, fp32); break;
   }
 }
 
