@@ -66,9 +66,13 @@ def pair_list(atoms: np.ndarray) -> List[Tuple[int, int]]:
     return out
 
 
-def descriptors(atoms: np.ndarray, frames, pairs) -> np.ndarray:
+def d_in(env_k: int) -> int:
+    return 1 + 9 + 1 + env_k * 10
+
+
+def descriptors(atoms: np.ndarray, frames, pairs, env_k: int = ENV_K) -> np.ndarray:
     n = len(atoms)
-    X = np.zeros((len(pairs), D_IN), dtype=np.float64)
+    X = np.zeros((len(pairs), d_in(env_k)), dtype=np.float64)
     for k, (v, w) in enumerate(pairs):
         R = frames[v]
         Ov = atoms[v, 0]
@@ -82,7 +86,7 @@ def descriptors(atoms: np.ndarray, frames, pairs) -> np.ndarray:
             centre = 0.5 * (Ov + atoms[w, 0])
         others = [u for u in range(n) if u != v and u != w]
         others.sort(key=lambda u: float(np.linalg.norm(atoms[u, 0] - centre)))
-        for j, u in enumerate(others[:ENV_K]):
+        for j, u in enumerate(others[:env_k]):
             base = 11 + 10 * j
             f[base:base + 9] = ((atoms[u] - Ov) @ R.T).ravel()
             f[base + 9] = fc(float(np.linalg.norm(atoms[u, 0] - centre)))
@@ -166,6 +170,7 @@ class MLP:
         self.v = [torch.zeros_like(p) for p in self.params]
         self.step_count = 0
         self.d_in, self.d_out, self.width = d_in, d_out, width
+        self.env_k = (d_in - 11) // 10            # environment waters in the descriptor
         self.x_mean = np.zeros(d_in)
         self.x_std = np.ones(d_in)
         self.y_mean = np.zeros(d_out)
@@ -275,7 +280,7 @@ def learned_density(mol: Molecule, model: MLP, P_mono_local: np.ndarray) -> np.n
     """Initial density of a water cluster from the network."""
     ws, frames, A, atoms = cluster_geometry(mol)
     pairs = pair_list(atoms)
-    X = descriptors(atoms, frames, pairs)
+    X = descriptors(atoms, frames, pairs, model.env_k)
     Y = model.predict(X)
     return assemble(mol, A, pairs, Y, P_mono_local)
 
@@ -284,7 +289,7 @@ def learned_densities(mols: List[Molecule], model: MLP, P_mono_local: np.ndarray
     """Initial densities of many clusters, one network evaluation over all their pairs."""
     geo = [cluster_geometry(m) for m in mols]
     pairs = [pair_list(g[3]) for g in geo]
-    X = np.concatenate([descriptors(g[3], g[1], p) for g, p in zip(geo, pairs)])
+    X = np.concatenate([descriptors(g[3], g[1], p, model.env_k) for g, p in zip(geo, pairs)])
     Y = model.predict(X)
     out, k = [], 0
     for m, g, p in zip(mols, geo, pairs):

@@ -42,7 +42,7 @@ def cluster_sizes(n_clusters: int, lo: int, hi: int, seed: int) -> np.ndarray:
     return np.random.default_rng(seed).integers(lo, hi + 1, size=n_clusters)
 
 
-def generate(n_train: int, P_mono: np.ndarray, device: int = 0, log=print):
+def generate(n_train: int, P_mono: np.ndarray, device: int = 0, log=print, env_k: int = LG.ENV_K):
     import torch
     from .scf import RHF
     Xs, Ys = [], []
@@ -55,7 +55,7 @@ def generate(n_train: int, P_mono: np.ndarray, device: int = 0, log=print):
         r = rhf.run(P0=P0, conv=1e-8, diis_tol=1e-5)
         ws, frames, A, atoms = LG.cluster_geometry(mol)
         pairs = LG.pair_list(atoms)
-        Xs.append(LG.descriptors(atoms, frames, pairs))
+        Xs.append(LG.descriptors(atoms, frames, pairs, env_k))
         Ys.append(LG.local_blocks(mol, r.P.cpu().numpy(), A, pairs, P_mono))
         rhf.fb.close()
         if (i + 1) % 100 == 0:
@@ -141,6 +141,7 @@ def main():
     ap.add_argument("--data", default=None, help="cache of the generated training set (.npz)")
     ap.add_argument("--report", default=None, help="write the evaluation summary (JSON)")
     ap.add_argument("--eval-only", action="store_true")
+    ap.add_argument("--env-k", type=int, default=LG.ENV_K, help="environment waters in the pair descriptor")
     args = ap.parse_args()
     P_mono = monomer_density()
     if args.eval_only:
@@ -151,7 +152,7 @@ def main():
             z = np.load(args.data)
             X, Y = z["X"], z["Y"]
         else:
-            X, Y = generate(args.n_train, P_mono)
+            X, Y = generate(args.n_train, P_mono, env_k=args.env_k)
             if args.data:
                 np.savez_compressed(args.data, X=X, Y=Y)
         print(f"training set: {X.shape[0]} pair blocks from {args.n_train} clusters ({time.time() - t0:.0f} s)")
