@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libtontofock.so")
 PEAK_LIB = os.path.join(HERE, "libtf_peak.so")
 
 SOURCES = ["tontofock.cu", "tf_mlp.cu"]
-DEPS = ["tontofock.cu", "tf_mlp.cu", "tf_device.cuh", "tf_warp.cuh", "tf_group.cuh", "rys_tables.inc", "boys_table.inc",
+DEPS = ["tontofock.cu", "tf_mlp.cu", "tf_device.cuh", "tf_warp.cuh", "tf_group.cuh", "rys_tables.inc", "boys_table.inc", "boys2_table.inc",
         os.path.join("..", "..", "include", "tontofock.h"), os.path.join("..", "..", "include", "tontofock_guess.h")]
 
 

@@ -24,6 +24,7 @@
 #define TF_RYS_CONST __device__ const
 #include "rys_tables.inc"
 #include "boys_table.inc"
+#include "boys2_table.inc"
 
 namespace tf {
 
@@ -313,6 +314,68 @@ struct RysSmem<1> {
     }
   }
 };
+
+#ifndef TF_RYS2_MOMENTS
+#define TF_RYS2_MOMENTS 1
+#endif
+#if TF_RYS2_MOMENTS
+// Two roots: the Gauss rule of the moments F_0..F_3 (gen_boys_table.py): u_1, u_2
+// are the roots of u^2 + a u + b, the monic polynomial orthogonal to 1 and u,
+//   a = (F0 F3 - F1 F2) / (F1^2 - F0 F2),  b = (F2^2 - F1 F3) / (F1^2 - F0 F2),
+// taken as q = (sqrt(a^2 - 4b) - a) / 2 (a < 0: no cancellation), u_1 = q,
+// u_2 = b / q; w_1 = (F0 u_2 - F1) / (u_2 - u_1), w_2 = F0 - w_1.  F0..F3 by the
+// 8-term Taylor step from a 1/8 grid of F_0..F_10: six 16-byte loads instead of 24.
+template <>
+struct RysSmem<2> {
+  static constexpr int SIZE = TF_BOYS2_NPTS * TF_BOYS2_NM;
+  static __device__ __forceinline__ void load(double* t) {
+    for (int q = threadIdx.x; q < SIZE; q += blockDim.x) t[q] = tf_boys2_grid[q];
+  }
+  static __device__ __forceinline__ void eval(const double* __restrict__ t, double x, double (&u)[2], double (&w)[2]) {
+    static_assert(TF_BOYS_NTERM == 8 && TF_BOYS2_NM == 12 && TF_BOYS2_XMAX == 50, "grid for the two-point rule");
+    if (x < (double)TF_BOYS2_XMAX) {
+      const int k = (int)(x * (double)TF_BOYS_H_INV + 0.5);
+      const double d = (double)k * (1.0 / TF_BOYS_H_INV) - x;
+      const double2* g = reinterpret_cast<const double2*>(t + k * TF_BOYS2_NM);
+      double f[12];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const double2 v = g[q];
+        f[2 * q] = v.x;
+        f[2 * q + 1] = v.y;
+      }
+      const double dj[8] = {0.0, d, d * 0.5, d * (1.0 / 3.0), d * 0.25, d * 0.2, d * (1.0 / 6.0), d * (1.0 / 7.0)};
+      double m[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {              // F_r = f_r + d (f_{r+1} + d/2 (... + d/7 f_{r+7}))
+        double v = f[r + 7];
+#pragma unroll
+        for (int j = 7; j >= 1; --j) v = fma(dj[j], v, f[r + j - 1]);
+        m[r] = v;
+      }
+      const double r = rcp_nr(m[1] * m[1] - m[0] * m[2]);
+      const double a = (m[0] * m[3] - m[1] * m[2]) * r;
+      const double b = (m[2] * m[2] - m[1] * m[3]) * r;
+      const double disc = fma(a, a, -4.0 * b);
+      const double q = 0.5 * (disc * rsqrt_nr(disc) - a);
+      u[0] = q;
+      u[1] = b * rcp_nr(q);
+      const double w0 = (m[0] * u[1] - m[1]) * rcp_nr(u[1] - u[0]);
+      w[0] = w0;
+      w[1] = m[0] - w0;
+    } else {
+      constexpr int HOFF = rys_hoffset(2);
+      const double ix = rcp_nr(x);
+      const double isx = rsqrt_nr(x);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        u[i] = tf_rys_hroot2[HOFF + i] * ix;
+        w[i] = tf_rys_hweight[HOFF + i] * isx;
+      }
+    }
+  }
+};
+#endif
 
 // ---------------------------------------------------------------------------
 // One contracted shell quartet (LA LB | LC LD), LA >= LB, LC >= LD, in
