@@ -187,11 +187,10 @@ class Molecule:
         return int(np.sum(self.Z)) - self.charge
 
     def nuclear_repulsion(self) -> float:
-        e = 0.0
-        for i in range(self.n_atom):
-            for j in range(i):
-                e += self.Z[i] * self.Z[j] / float(np.linalg.norm(self.xyz[i] - self.xyz[j]))
-        return float(e)
+        Z = np.asarray(self.Z, dtype=np.float64)
+        d = np.sqrt(((self.xyz[:, None, :] - self.xyz[None, :, :]) ** 2).sum(-1))
+        i, j = np.tril_indices(self.n_atom, -1)
+        return float(np.sum(Z[i] * Z[j] / d[i, j]))
 
     def flat_arrays(self):
         """Flattened shell data in the C-ABI layout (see include/tontofock.h)."""

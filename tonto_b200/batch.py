@@ -105,12 +105,12 @@ class BatchRHF:
         for b in self.buckets:
             b.S = self._pad(b, [S[i] for i in b.ids])
             b.H = self._pad(b, [T[i] + V[i] for i in b.ids])
-            X = torch.zeros_like(b.S)
-            for k in range(b.m):
-                n = n_bf[b.ids[k]]
-                e, U = torch.linalg.eigh(b.S[k, :n, :n])
-                X[k, :n, :n] = (U / torch.sqrt(e)) @ U.T
-            b.X = X
+            # orthogonaliser X = L^-T from the Cholesky factor S = L L^T (padding: identity):
+            # X^T S X = 1, and the densities do not depend on which orthogonaliser is used
+            pad_eye = torch.diag_embed((~b.valid).to(torch.float64))
+            L = torch.linalg.cholesky(b.S + pad_eye)
+            eye = torch.eye(b.n, dtype=torch.float64, device=dev).expand(b.m, b.n, b.n)
+            b.X = torch.linalg.solve_triangular(L, eye, upper=False).transpose(1, 2).contiguous()
             b.n_occ = torch.tensor([self.mols[i].n_electrons // 2 for i in b.ids], device=dev)
             b.e_nuc = torch.tensor([self.mols[i].nuclear_repulsion() for i in b.ids], dtype=torch.float64,
                                    device=dev)
