@@ -258,6 +258,7 @@ struct ListArgs {
   const int* sorted;            // pair ids, grouped by (molecule, class), in I_max bands (see setup_pairs)
   const double* sorted_imax;
   const double* sorted_bmax;    // largest I_max of the position's band (non-increasing)
+  const int4* srec;             // screening record of each sorted position (see ScreenRec)
   const PairRec* pairs;
   const MolInfo* mols;
   const double* pmax;           // per-molecule n_shell x n_shell blocks
@@ -275,11 +276,17 @@ struct ListArgs {
   int* task_len;
 };
 
-__device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo& mi, const PairRec& b,
-                                                const PairRec& k, double Ib, double Ik) {
+// Screening record of a sorted pair position, 16 bytes read in list order (coalesced):
+// x = local shell hi | local shell lo << 16, y = local atom hi | local atom lo << 16,
+// z = primitive pairs without | with the pair cutoff << 16, w = pair id.
+__device__ __forceinline__ int lo16(int v) { return v & 0xffff; }
+__device__ __forceinline__ int hi16(int v) { return (int)((unsigned)v >> 16); }
+
+__device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo& mi, const int4 b, const int4 k,
+                                                double Ib, double Ik) {
   const double* pm = a.pmax + mi.pmax;
   const int ns = mi.n_shell;
-  const int sa = b.sh_hi - mi.shell0, sb = b.sh_lo - mi.shell0, sc = k.sh_hi - mi.shell0, sd = k.sh_lo - mi.shell0;
+  const int sa = lo16(b.x), sb = hi16(b.x), sc = lo16(k.x), sd = hi16(k.x);
   double m = fmax(pm[sa * ns + sb], pm[sc * ns + sd]);
   m = fmax(m, fmax(pm[sa * ns + sc], pm[sa * ns + sd]));
   m = fmax(m, fmax(pm[sb * ns + sc], pm[sb * ns + sd]));
@@ -287,10 +294,10 @@ __device__ __forceinline__ double quartet_bound(const ListArgs& a, const MolInfo
   return m * Ib * Ik;
 }
 
-__device__ __forceinline__ int cost_bucket(const PairRec& b, const PairRec& k) {
-  const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
-                        b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
-  const int npq = any_same ? b.n_full * k.n_full : b.n_skip * k.n_skip;
+__device__ __forceinline__ int cost_bucket(const int4 b, const int4 k) {
+  const int bh = lo16(b.y), bl = hi16(b.y), kh = lo16(k.y), kl = hi16(k.y);
+  const bool any_same = bh == bl || kh == kl || bh == kh || bh == kl || bl == kh || bl == kl;
+  const int npq = any_same ? lo16(b.z) * lo16(k.z) : hi16(b.z) * hi16(k.z);
   const int lg = npq > 0 ? 31 - __clz(npq) : 0;
   return lg < NCOST ? lg : NCOST - 1;
 }
@@ -329,11 +336,11 @@ __global__ void __launch_bounds__(LIST_THREADS) k_quartets(ListArgs a, long long
   const long long coff = a.cand ? a.cand_off[t] : 0;
   const int len = MODE == 2 ? a.task_len[t] : jend;
   double Ib = 0.0, pg = 0.0;
-  PairRec b{};
+  int4 b = make_int4(0, 0, 0, 0);
   MolInfo mi{};
   if (MODE != 2) {
     Ib = a.sorted_imax[cp.bra_off + i];
-    b = a.pairs[bra];
+    b = a.srec[cp.bra_off + i];
     mi = a.mols[cp.mol];
     pg = __longlong_as_double((long long)a.pglob[cp.mol]);
   }
@@ -352,8 +359,8 @@ __global__ void __launch_bounds__(LIST_THREADS) k_quartets(ListArgs a, long long
       if (!(Ib * a.sorted_bmax[cp.ket_off + j] * pg > a.cutoff)) {
         beyond = true;                           // bands are in decreasing I_max: nothing further survives
       } else if (Ib * Ik * pg > a.cutoff) {
-        ket = a.sorted[cp.ket_off + j];
-        const PairRec k = a.pairs[ket];
+        const int4 k = a.srec[cp.ket_off + j];
+        ket = k.w;
         const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
         if (bound > a.cutoff) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
       }
@@ -1257,6 +1264,7 @@ struct tf_ctx {
   tf::DBuf<tf::CPUnit> d_units;
   tf::DBuf<int> d_unit_group, d_group_task0, d_task_len;
   tf::DBuf<unsigned char> d_cand;
+  tf::DBuf<int4> d_srec;
   tf::DBuf<long long> d_task_cand_off;
   tf::DBuf<long long> d_counts, d_offsets, d_group_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
@@ -1501,6 +1509,20 @@ static int setup_pairs(tf_ctx* c) {
       for (; i < e; ++i) { sorted.push_back(v[i]); simax.push_back(c->pairs_h[v[i]].imax); sbmax.push_back(bm); }
     }
   }
+  std::vector<int4> srec(sorted.size());
+  for (size_t q = 0; q < sorted.size(); ++q) {
+    const PairRec& pr = c->pairs_h[sorted[q]];
+    const MolInfo& mi = c->mols[pr.mol];
+    const int sh = pr.sh_hi - mi.shell0, sl = pr.sh_lo - mi.shell0;
+    const int ah = pr.atom_hi - mi.atom0, al = pr.atom_lo - mi.atom0;
+    if (sh > 0xffff || sl > 0xffff || ah > 0xffff || al > 0xffff || pr.n_full > 0xffff || pr.n_skip > 0xffff) {
+      set_error("molecule too large for the screening records (65535 shells, atoms or primitive pairs)");
+      return TF_EUNSUPPORTED;
+    }
+    srec[q] = make_int4(sh | (sl << 16), ah | (al << 16), pr.n_full | (pr.n_skip << 16), sorted[q]);
+  }
+  TF_CUDA(c->d_srec.reserve(std::max<size_t>(srec.size(), 1)));
+  TF_CUDA(cudaMemcpyAsync(c->d_srec.p, srec.data(), srec.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(c->d_sorted.reserve(std::max<size_t>(sorted.size(), 1)));
   TF_CUDA(c->d_sorted_imax.reserve(std::max<size_t>(simax.size(), 1)));
   TF_CUDA(c->d_sorted_bmax.reserve(std::max<size_t>(sbmax.size(), 1)));
@@ -1653,7 +1675,8 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, dPb, c->d_pmax.p, c->d_pglob.p);
   kernels++;
   la = ListArgs{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
-                c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_pairs.p,  c->d_mols.p,  c->d_pmax.p,
+                c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_srec.p, c->d_pairs.p,  c->d_mols.p,
+                c->d_pmax.p,
                 c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX,
                 c->use_cand ? c->d_cand.p : nullptr, c->d_task_cand_off.p, c->d_task_len.p};
   const long long thr_list = LIST_THREADS;
