@@ -154,6 +154,30 @@ struct __align__(16) PairRec {
   double imax;               // Schwarz bound sqrt(max |(ab|ab)|)
 };
 
+// What the ERI kernels read of a shell pair, packed: rec[2 id] = {cart_hi, cart_lo,
+// full_off, skip_off}, rec[2 id + 1] = {atom_hi, atom_lo, n_full | n_skip << 16,
+// mol | (shell hi == shell lo) << 31} (32 bytes, one sector), and pairR[id] = (A - B, 0)
+// read only by classes whose transfers need it.
+struct PairJK {
+  int cart_hi, cart_lo, full_off, skip_off;
+  int atom_hi, atom_lo, n_full, n_skip, mol;
+  bool same;                 // both shells the same (coincidence factor 1/2)
+  double Rx, Ry, Rz;
+};
+
+__device__ __forceinline__ PairJK load_pair_jk(const int4* __restrict__ rec, const double2* __restrict__ pairR,
+                                               int id) {
+  const int4 x = __ldg(rec + 2 * id), y = __ldg(rec + 2 * id + 1);
+  PairJK p;
+  p.cart_hi = x.x; p.cart_lo = x.y; p.full_off = x.z; p.skip_off = x.w;
+  p.atom_hi = y.x; p.atom_lo = y.y;
+  p.n_full = y.z & 0xffff; p.n_skip = (int)((unsigned)y.z >> 16);
+  p.mol = y.w & 0x7fffffff; p.same = y.w < 0;
+  const double2 r0 = __ldg(pairR + 2 * id), r1 = __ldg(pairR + 2 * id + 1);
+  p.Rx = r0.x; p.Ry = r0.y; p.Rz = r1.x;
+  return p;
+}
+
 // Quartet range of a launch in a graph-captured build: list[range[0] - base,
 // range[1] - base), read on the device and clamped to the list capacity.
 __device__ __forceinline__ void resolve_range(const long long* range, long long base, long long cap,

@@ -227,6 +227,8 @@ struct GroupArgs {
   unsigned long long* prim_count;
   const long long* range;       // graph builds: see resolve_range
   long long base, cap;
+  const int4* jkrec;            // packed pair records (load_pair_jk)
+  const double2* pairR;
   const double* P2;             // unrestricted: beta density and its J, K (else null)
   double* J2;
   double* K2;
@@ -308,8 +310,8 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
     const long long t = base + (in_group ? g : 0);
     const bool act = in_group && t < nq;
     const int2 qd = act ? quartets[t] : make_int2(0, 0);
-    const PairRec b = a.pairs[qd.x];
-    const PairRec k = a.pairs[qd.y];
+    const PairJK b = load_pair_jk(a.jkrec, a.pairR, qd.x);
+    const PairJK k = load_pair_jk(a.jkrec, a.pairR, qd.y);
     const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
                           b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
     const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
@@ -411,8 +413,8 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
       const MolInfo mi = a.mols[b.mol];
       const int n = mi.n_cart;
       double f = 1.0;
-      if (b.sh_hi == b.sh_lo) f *= 0.5;
-      if (k.sh_hi == k.sh_lo) f *= 0.5;
+      if (b.same) f *= 0.5;
+      if (k.same) f *= 0.5;
       if (qd.x == qd.y) f *= 0.5;
       constexpr int NA = Q::NA, NB = Q::NB, NC = Q::NC, ND = Q::ND, NCD = NC * ND;
       const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;

@@ -403,6 +403,8 @@ struct JKArgs {
   // range read on the device and clamped to base + cap (quartets = list start)
   const long long* range;
   long long base, cap;
+  const int4* jkrec;            // packed pair records (load_pair_jk)
+  const double2* pairR;
   // unrestricted builds: the beta density and its J, K (else null); P, J, K above
   // are then the alpha ones.  want: bit 0 J, bit 1 K.
   const double* P2;
@@ -449,8 +451,8 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
     // take part in the warp reductions below
     const bool active = t < nq;
     const int2 qd = quartets[active ? t : nq - 1];
-    const PairRec b = a.pairs[qd.x];
-    const PairRec k = a.pairs[qd.y];
+    const PairJK b = load_pair_jk(a.jkrec, a.pairR, qd.x);
+    const PairJK k = load_pair_jk(a.jkrec, a.pairR, qd.y);
     const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
                           b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
     const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
@@ -459,8 +461,8 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
     const int nkp = any_same ? k.n_full : k.n_skip;
     if (active) nprim += (unsigned long long)nbp * nkp;
     double f = active ? 1.0 : 0.0;
-    if (b.sh_hi == b.sh_lo) f *= 0.5;
-    if (k.sh_hi == k.sh_lo) f *= 0.5;
+    if (b.same) f *= 0.5;
+    if (k.same) f *= 0.5;
     if (qd.x == qd.y) f *= 0.5;
     const double Rab[3] = {b.Rx, b.Ry, b.Rz};
     const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
@@ -1264,7 +1266,8 @@ struct tf_ctx {
   tf::DBuf<tf::CPUnit> d_units;
   tf::DBuf<int> d_unit_group, d_group_task0, d_task_len;
   tf::DBuf<unsigned char> d_cand;
-  tf::DBuf<int4> d_srec;
+  tf::DBuf<int4> d_srec, d_jkrec;
+  tf::DBuf<double2> d_pairR;
   tf::DBuf<long long> d_task_cand_off;
   tf::DBuf<long long> d_counts, d_offsets, d_group_offsets;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
@@ -1509,6 +1512,24 @@ static int setup_pairs(tf_ctx* c) {
       for (; i < e; ++i) { sorted.push_back(v[i]); simax.push_back(c->pairs_h[v[i]].imax); sbmax.push_back(bm); }
     }
   }
+  // packed pair records of the ERI kernels (load_pair_jk)
+  {
+    std::vector<int4> jr(2 * c->n_pairs);
+    std::vector<double2> pr2(2 * c->n_pairs);
+    for (long long p = 0; p < c->n_pairs; ++p) {
+      const PairRec& q = c->pairs_h[p];
+      if (q.n_full > 0xffff || q.n_skip > 0xffff) { set_error("too many primitive pairs in one shell pair"); return TF_EUNSUPPORTED; }
+      jr[2 * p] = make_int4(q.cart_hi, q.cart_lo, q.full_off, q.skip_off);
+      jr[2 * p + 1] = make_int4(q.atom_hi, q.atom_lo, q.n_full | (q.n_skip << 16),
+                                (int)((unsigned)q.mol | (q.sh_hi == q.sh_lo ? 0x80000000u : 0u)));
+      pr2[2 * p] = make_double2(q.Rx, q.Ry);
+      pr2[2 * p + 1] = make_double2(q.Rz, 0.0);
+    }
+    TF_CUDA(c->d_jkrec.reserve(std::max<size_t>(jr.size(), 1)));
+    TF_CUDA(c->d_pairR.reserve(std::max<size_t>(pr2.size(), 1)));
+    TF_CUDA(cudaMemcpy(c->d_jkrec.p, jr.data(), jr.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    TF_CUDA(cudaMemcpy(c->d_pairR.p, pr2.data(), pr2.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  }
   std::vector<int4> srec(sorted.size());
   for (size_t q = 0; q < sorted.size(); ++q) {
     const PairRec& pr = c->pairs_h[sorted[q]];
@@ -1610,7 +1631,7 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   const long long full = (long long)nsm * group_blocks_per_sm;
   const long long blocks = a.range ? full : std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
   GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count,
-              a.range, a.base, a.cap, a.P2, a.J2, a.K2, a.want};
+              a.range, a.base, a.cap, a.jkrec, a.pairR, a.P2, a.J2, a.K2, a.want};
   k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
   return TF_OK;
 }
@@ -1759,7 +1780,7 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
     cudaStream_t sg = si == 0 ? s : c->side[si - 1];
     JKArgs a{c->d_quartets.p, 0, c->d_pairs.p, c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p,
              c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap,
-             nullptr, nullptr, nullptr, want};
+             c->d_jkrec.p, c->d_pairR.p, nullptr, nullptr, nullptr, want};
     JKArgs a32 = a;
     a32.range = c->d_group_offsets.p + 3 * g + 1;
     rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false, c->cls_variant[g]);
@@ -1964,7 +1985,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       TF_CUDA(cudaEventRecord(c->cls_ev[2 * g], s));
       JKArgs a{c->d_quartets.p + (goff[3 * g] - base), goff[3 * g + 1] - goff[3 * g], c->d_pairs.p,
                c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p,
-               c->d_prim_count.p, nullptr, 0, LLONG_MAX,
+               c->d_prim_count.p, nullptr, 0, LLONG_MAX, c->d_jkrec.p, c->d_pairR.p,
                dPb ? c->d_PcB.p : nullptr, dPb ? c->d_JcB.p : nullptr, dPb ? c->d_KcB.p : nullptr, want};
       JKArgs a32 = a;
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
