@@ -330,7 +330,7 @@ def main():
     import numpy as np
     import torch
     import torch.distributed as dist
-    from tonto_b200.fock import FockBuilder
+    from tonto_b200.fock import TF_JK_MIXED, FockBuilder
     from tonto_b200.molecules import water_cluster
 
     torch.cuda.set_device(local)
@@ -371,8 +371,31 @@ def main():
             step()
             ev[k][1].record(stream)
             torch.cuda.synchronize(dev)
-    graph_builds = bool(fb.stats()["graph"])
+    st_timed = fb.stats()
+    graph_builds = bool(st_timed["graph"])
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    # the same builds with mixed precision (quartets with Schwarz x density bound
+    # below 1e-6 in FP32, FP64 roots, weights and accumulation), device-timed alike
+    mixed = None
+    if world == 1:
+        J64, K64 = J.clone(), K.clone()
+        for _ in range(2):
+            fb.make_r_JK_device(P, J, K, TF_JK_MIXED)
+        torch.cuda.synchronize(dev)
+        mev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            mev[k][0].record(stream)
+            fb.make_r_JK_device(P, J, K, TF_JK_MIXED)
+            mev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        mst = fb.stats()
+        m_ms = sum(a.elapsed_time(b) for a, b in mev) / args.steps
+        mixed = {"value": 1e3 / m_ms, "unit": "builds/s", "ms_per_step": m_ms,
+                 "fp32_quartet_fraction": mst["quartets_fp32"] / mst["quartets"],
+                 "max_abs_dJ_vs_fp64": float((J - J64).abs().max()), "max_abs_dK_vs_fp64": float((K - K64).abs().max())}
+        fb.make_r_JK_device(P, J, K)
+        torch.cuda.synchronize(dev)
     # per-class device times: builds launched class by class (events between the
     # launches), outside the timed region
     cls_acc = {}
@@ -433,8 +456,9 @@ def main():
                        "class_schedule": {"graph_branches": tune["streams"],
                                           "non_default_kernel_variants": tune["variant_classes"],
                                           "autotune_ms": [round(v, 3) for v in tune["ms"]]}},
-            "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(st["kernels"]) * args.steps,
+            "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(st_timed["kernels"]) * args.steps,
             "e2e": e2e,
+            "mixed_precision_builds": mixed,
             "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"], "flops": st["flops"],
                       "graph": graph_builds, "direct_build_ms": st_direct["build_ms"],
                       "direct_eri_ms": st_direct["eri_ms"]},
