@@ -189,7 +189,8 @@ typedef struct tf_tune {
  * each class pair's device time; then for 1 .. max_streams (<= 8) graph branches the class pairs
  * are assigned longest first to the least-loaded branch, each schedule is
  * captured and timed over three builds, and the fastest is kept for this
- * context's later graph builds.  Fills *out if not NULL.  Results do not depend
+ * context's later graph builds.  Contexts created later on the same device start
+ * from the kernel variants chosen here.  Fills *out if not NULL.  Results do not depend
  * on the schedule beyond summation order.  No reference counterpart. */
 int tf_autotune(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags, int max_streams, tf_tune* out);
 

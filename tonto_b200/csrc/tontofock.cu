@@ -30,6 +30,8 @@
 #include <numeric>
 #include <string>
 #include <vector>
+#include <mutex>
+#include <map>
 
 namespace tf {
 
@@ -1330,6 +1332,12 @@ __global__ void k_group_offsets(int n_groups, const int* __restrict__ group_task
   out[3 * g + 2] = offs[t1 * NBUCKET];
 }
 
+// Kernel variant of each class pair chosen by the last tf_autotune on a device; new
+// contexts on that device start from it (class pairs are enumerated alike in every
+// context).
+static std::mutex g_variant_mutex;
+static std::map<int, std::vector<int>> g_variant_cache;
+
 // Groups (class pairs p1 >= p2) of units (one per molecule having both classes);
 // tasks are (unit, bra position); with sharding this context keeps every
 // shard_count-th task (Tonto's round-robin parallel do).
@@ -1358,7 +1366,12 @@ static int build_tasks(tf_ctx* c) {
     }
   c->group_task0.push_back((int)tasks.size());
   c->n_tasks = (long long)tasks.size();
-  c->cls_variant.resize(c->group_cls.size(), 0);
+  c->cls_variant.assign(c->group_cls.size(), 0);
+  {                                    // start from the last autotuned choice on this device
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    const auto it = g_variant_cache.find(c->device);
+    if (it != g_variant_cache.end() && it->second.size() == c->cls_variant.size()) c->cls_variant = it->second;
+  }
   // candidate kets per task (all that a task may examine), for the screening record
   std::vector<long long> cand_off(tasks.size() + 1, 0);
   for (size_t t = 0; t < tasks.size(); ++t) {
@@ -2249,6 +2262,10 @@ int tf_autotune(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, 
       if (tv[v][g] < tv[best_v][g] * 0.98) best_v = v;
     c->cls_variant[g] = best_v;
     if (best_v) res.variant_classes++;
+  }
+  {                                    // later contexts on this device start from this choice
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    g_variant_cache[c->device] = c->cls_variant;
   }
   // class-pair times from a class-by-class build with the chosen variants
   rc = build_jk_device(c, dP, dJ, dK, flags);
