@@ -189,10 +189,9 @@ def time_to_scf(mol, fb, device):
         t0 = time.perf_counter()
         P0 = None
         fb_guess = None
-        if guess == "learned":
-            P_sup = torch.tensor(G.superposition_guess(mol, P_mono), device=rhf.dev)
+        if guess == "learned":            # the superposition guess only if the fallback needs it
             P0 = torch.tensor(LG.learned_density(mol, model, P_mono), device=rhf.dev)
-            fb_guess = lambda: P_sup  # noqa: E731
+            fb_guess = lambda: torch.tensor(G.superposition_guess(mol, P_mono), device=rhf.dev)  # noqa: E731
         t_guess = time.perf_counter() - t0
         r = rhf.run(P0=P0, conv=1e-9, diis_tol=1e-6, fallback=fb_guess, **kw)
         if ref is None:

@@ -6,8 +6,8 @@ the final cycles), its density change since the last cycle (incremental
 cycles; G is linear in the density), or nothing once converged (a zero change
 is screened out entirely by the density test).  Per molecule the loop is Tonto's
 usual_SCF with DIIS (keep 8), as in ``tonto_b200.scf``: cheap builds until the
-convergence test first passes, then full FP64 builds until it passes again after
-at least two of them.  A molecule whose DIIS error after ``fallback_after`` cycles
+DIIS error is within ``final_at`` times its tolerance (or the convergence test
+passes), then full FP64 builds until the test passes after at least two of them.  A molecule whose DIIS error after ``fallback_after`` cycles
 is not below its first cycle's restarts (once) from ``fallback(i)``.
 
 Everything between the builds runs on the device in batches: the molecules are
@@ -143,7 +143,7 @@ class BatchRHF:
 
     def run(self, P0: Optional[List[torch.Tensor]] = None, conv: float = 1e-9, diis_tol: float = 1e-6,
             max_iter: int = 100, incremental: bool = True, mixed: bool = False, rebuild_every: int = 16,
-            mixed_until: float = 1e-6, fp64_final: int = 2,
+            mixed_until: float = 1e-6, fp64_final: int = 2, final_at: float = 10.0,
             fallback: Optional[Callable[[int], torch.Tensor]] = None, fallback_after: int = 3,
             diis_keep: int = 8) -> List[SCFResult]:
         nm = len(self.mols)
@@ -233,7 +233,7 @@ class BatchRHF:
                 if state[i] == "final" and passed and n_final[i] >= min(fp64_final, it + 1):
                     done[i] = True
                     continue
-                if state[i] == "cheap" and passed:
+                if state[i] == "cheap" and (passed or (E_old[i] is not None and err_n < final_at * diis_tol)):
                     state[i] = "final"
                 E_old[i] = E[i]
                 have_prev[i] = True

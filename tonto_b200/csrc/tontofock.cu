@@ -239,8 +239,12 @@ __global__ void k_pmax(BatchArgs b, const double* __restrict__ P, const double* 
 // ---------------------------------------------------------------------------
 // kernels: quartet lists
 // ---------------------------------------------------------------------------
-constexpr int NCOST = 13;                  // log2 buckets of the primitive-quartet count
+// Cost buckets of the primitive-quartet count npq: npq itself below 8, then quarter
+// octaves (counts within a factor 1.19 share a bucket), so that the lanes of a warp
+// loop over nearly the same number of primitive quartets.
+constexpr int NCOST = 47;
 constexpr int NBUCKET = 2 * NCOST;         // FP64 buckets, then FP32 buckets
+static_assert(NBUCKET < 0xff, "bucket ids are recorded as bytes, 0xff = screened out");
 
 // One (class pair, molecule) unit of the list builder.  Units of the same class
 // pair are consecutive and form a group; the quartets of a group are one launch.
@@ -276,6 +280,9 @@ struct ListArgs {
   unsigned char* cand;
   const long long* cand_off;
   int* task_len;
+  // captured builds: the list length (written by the scan); a list longer than
+  // out_base + out_cap is not written at all (that build is redone), else null
+  const long long* list_total;
 };
 
 // Screening record of a sorted pair position, 16 bytes read in list order (coalesced):
@@ -300,8 +307,10 @@ __device__ __forceinline__ int cost_bucket(const int4 b, const int4 k) {
   const int bh = lo16(b.y), bl = hi16(b.y), kh = lo16(k.y), kl = hi16(k.y);
   const bool any_same = bh == bl || kh == kl || bh == kh || bh == kl || bl == kh || bl == kl;
   const int npq = any_same ? lo16(b.z) * lo16(k.z) : hi16(b.z) * hi16(k.z);
-  const int lg = npq > 0 ? 31 - __clz(npq) : 0;
-  return lg < NCOST ? lg : NCOST - 1;
+  if (npq < 8) return npq > 0 ? npq - 1 : 0;
+  const int lg = 31 - __clz(npq);                          // >= 3
+  const int bucket = 7 + (lg - 3) * 4 + ((npq >> (lg - 2)) & 3);
+  return bucket < NCOST ? bucket : NCOST - 1;
 }
 
 // Index of (task, bucket) in the count/offset arrays: group (class pair), then
@@ -327,6 +336,7 @@ __global__ void __launch_bounds__(LIST_THREADS) k_quartets(ListArgs a, long long
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long t = a.t_base + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (t >= a.n_tasks) return;                    // uniform over the warp
+  if (MODE != 0 && a.list_total && *a.list_total - a.out_base > a.out_cap) return;
   for (int k = lane; k < NBUCKET; k += 32) scnt[warp][k] = 0;
   __syncwarp();
   const int2 task = a.tasks[t];
@@ -473,7 +483,17 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
 
     // The lists are bra-major, so the lanes of a warp usually share the bra pair:
     // then J(ab) is summed over the warp and added once, and P(ab) is a broadcast.
+    // Otherwise the lanes of one bra are neighbours (a bra's kets of one cost bucket
+    // are consecutive) and J(ab) is summed over each run of equal bras by a segmented
+    // warp scan, then added by the run's last lane.
     const bool uni = __all_sync(0xffffffffu, qd.x == __shfl_sync(0xffffffffu, qd.x, 0));
+    const unsigned lt_mask = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+    // (every lane executes the shuffle: none may be skipped by a short-circuit)
+    const int upx = __shfl_up_sync(0xffffffffu, qd.x, 1);
+    const bool headx = lane == 0 || qd.x != upx;
+    const unsigned heada = __ballot_sync(0xffffffffu, headx);
+    const int sega = 31 - __clz(heada & lt_mask);
+    const bool taila = lane == 31 || ((heada >> (lane + 1)) & 1u);
     const MolInfo mi = a.mols[b.mol];
     const int n = mi.n_cart;
     const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
@@ -498,8 +518,13 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
-          } else if (active) {
-            atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+          } else {                       // idle lanes join the last run with s = 0
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const double t = __shfl_up_sync(0xffffffffu, s, o);
+              if (lane - o >= sega) s += t;
+            }
+            if (taila && s != 0.0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
           }
         }
       if (active) {
@@ -528,20 +553,18 @@ __global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(
     // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
     // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
     // (twice for an unrestricted build: alpha and beta densities)
-    // Variant bit 2: the K rows a and b are the same for all lanes of a bra-uniform
-    // warp, and lanes whose kets share the c (or d) shell add to the same K
-    // elements.  Such lanes are neighbours (pair-id order), so each run of equal
-    // keys is summed with a segmented warp scan and added once, by its last lane.
+    // Variant bit 2: the K rows a and b are the same for all lanes of one bra, and
+    // lanes whose kets share the c (or d) shell add to the same K elements.  Such
+    // lanes are neighbours (pair-id order), so each run of equal (bra, shell) keys
+    // is summed with a segmented warp scan and added once, by its last lane.
     constexpr bool SEG = (V & 2) != 0;
     int segc = lane, segd = lane;
     bool tailc = true, taild = true;
     if constexpr (SEG) {
-      const int keyc = uni ? oc : -1 - lane, keyd = uni ? od : -1 - lane;
-      const unsigned lt_mask = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
       // (every lane executes both shuffles: none may be skipped by a short-circuit)
-      const int upc = __shfl_up_sync(0xffffffffu, keyc, 1), upd = __shfl_up_sync(0xffffffffu, keyd, 1);
-      const unsigned headc = __ballot_sync(0xffffffffu, lane == 0 || keyc != upc);
-      const unsigned headd = __ballot_sync(0xffffffffu, lane == 0 || keyd != upd);
+      const int upc = __shfl_up_sync(0xffffffffu, oc, 1), upd = __shfl_up_sync(0xffffffffu, od, 1);
+      const unsigned headc = __ballot_sync(0xffffffffu, headx || oc != upc);
+      const unsigned headd = __ballot_sync(0xffffffffu, headx || od != upd);
       segc = 31 - __clz(headc & lt_mask);
       segd = 31 - __clz(headd & lt_mask);
       tailc = lane == 31 || ((headc >> (lane + 1)) & 1u);
@@ -1199,7 +1222,7 @@ struct DBuf {
 // Per-context host staging in pinned memory (group offsets and primitive counts
 // read back after a build; pinned so that a captured graph can copy into them).
 struct PinnedStage {
-  long long* goff = nullptr;                 // 3 per group
+  long long* goff = nullptr;                 // 3 per group, then the list length
   unsigned long long* pc = nullptr;          // tf::NQCLS
   size_t n_goff = 0;
   ~PinnedStage() {
@@ -1321,11 +1344,20 @@ static BatchArgs batch_args(tf_ctx* c) {
                    c->d_shell_nbf.p,  c->spherical};
 }
 
-// gather (start, FP32 start, end) of every group's quartet range
+// gather (start, FP32 start, end) of every group's quartet range, and the list
+// length at out[3 n_groups].  A list longer than cap (the buffer of a captured
+// build) gets empty ranges: that build's class launches do nothing, and the host,
+// seeing the length, redoes the build with a larger buffer.
 __global__ void k_group_offsets(int n_groups, const int* __restrict__ group_task0, const long long* __restrict__ offs,
-                                long long* __restrict__ out) {
+                                long long cap, long long* __restrict__ out) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_groups) return;
+  const long long total = offs[(long long)group_task0[n_groups] * NBUCKET];
+  if (g == 0) out[3 * n_groups] = total;
+  if (total > cap) {
+    out[3 * g] = out[3 * g + 1] = out[3 * g + 2] = 0;
+    return;
+  }
   const long long t0 = group_task0[g], t1 = group_task0[g + 1];
   out[3 * g] = offs[t0 * NBUCKET];
   out[3 * g + 1] = offs[t0 * NBUCKET + (long long)NCOST * (t1 - t0)];
@@ -1391,8 +1423,12 @@ static int build_tasks(tf_ctx* c) {
   TF_CUDA(c->d_units.reserve(std::max<size_t>(c->units.size(), 1)));
   TF_CUDA(c->d_unit_group.reserve(std::max<size_t>(c->unit_group.size(), 1)));
   TF_CUDA(c->d_group_task0.reserve(ng + 1));
-  TF_CUDA(c->d_group_offsets.reserve(3 * ng));
+  TF_CUDA(c->d_group_offsets.reserve(3 * ng + 1));
   TF_CUDA(c->d_tasks.reserve(std::max<size_t>(tasks.size(), 1)));
+  if ((long long)tasks.size() * NBUCKET + 1 > 0x7fffffffLL) {    // the count scan indexes with int
+    set_error("too many bra tasks for the quartet-list counts");
+    return TF_EUNSUPPORTED;
+  }
   TF_CUDA(c->d_counts.reserve(tasks.size() * NBUCKET + 1));
   TF_CUDA(c->d_offsets.reserve(tasks.size() * NBUCKET + 1));
   if (!c->units.empty()) {
@@ -1694,7 +1730,8 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
 // Density transform, pair maxima, quartet counts, their scan and the per-group
 // (start, FP32 start, end) offsets on the device: the part of a build shared by
 // the dynamic and the graph paths.
-static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool mixed, ListArgs& la, int& kernels) {
+static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool mixed, long long cap, ListArgs& la,
+                          int& kernels) {
   cudaStream_t s = c->stream;
   const BatchArgs bt = batch_args(c);
   const long long nc2 = c->cmat_off[c->n_mol], ns2 = c->pmax_off[c->n_mol];
@@ -1725,7 +1762,7 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   TF_CUDA(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1),
                                         s));
   const int ng = (int)c->group_cls.size();
-  k_group_offsets<<<(ng + 63) / 64, 64, 0, s>>>(ng, c->d_group_task0.p, c->d_offsets.p, c->d_group_offsets.p);
+  k_group_offsets<<<(ng + 63) / 64, 64, 0, s>>>(ng, c->d_group_task0.p, c->d_offsets.p, cap, c->d_group_offsets.p);
   kernels += 3;
   const long long nc = c->cmat_off[c->n_mol];
   TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc * sizeof(double), s));
@@ -1751,7 +1788,8 @@ static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, double* dJb, doub
   }
   TF_CUDA(cudaGetLastError());
   const int ng = (int)c->group_cls.size();
-  TF_CUDA(cudaMemcpyAsync(c->pin->goff, c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  TF_CUDA(cudaMemcpyAsync(c->pin->goff, c->d_group_offsets.p, (3 * ng + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
+                          s));
   TF_CUDA(cudaMemcpyAsync(c->pin->pc, c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                           s));
   return TF_OK;
@@ -1767,10 +1805,11 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
                               int& kernels) {
   cudaStream_t s = c->stream;
   ListArgs la;
-  int rc = enqueue_counts(c, dP, nullptr, mixed, la, kernels);
+  int rc = enqueue_counts(c, dP, nullptr, mixed, c->graph_cap, la, kernels);
   if (rc) return rc;
   ListArgs lw = la;
   lw.out_cap = c->graph_cap;
+  lw.list_total = c->d_offsets.p + c->n_tasks * NBUCKET;     // an overflowing list is not written
   const long long thr_list = LIST_THREADS;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   if (c->use_cand) k_quartets<2><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
@@ -1885,7 +1924,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     TF_CUDA(cudaEventCreate(&e));
     c->cls_ev.push_back(e);
   }
-  TF_CUDA(c->pin->reserve(3 * (size_t)ng));
+  TF_CUDA(c->pin->reserve(3 * (size_t)ng + 1));
   {
     size_t tmp_bytes = 0;
     const long long nslots = c->n_tasks * NBUCKET;
@@ -1930,17 +1969,18 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     TF_CUDA(cudaGraphLaunch(c->graph_exec, s));
     TF_CUDA(cudaEventRecord(c->ev2, s));
     TF_CUDA(cudaStreamSynchronize(s));
-    const long long total = ng > 0 ? c->pin->goff[3 * (ng - 1) + 2] : 0;
+    const long long total = c->pin->goff[3 * ng];
     if (total <= c->graph_cap) return finish_stats(c, c->graph_kernels, true);
     drop_graph(c);                          // list outgrew the buffer: redo this build dynamically
   }
   int kernels = 0;
   TF_CUDA(cudaEventRecord(c->ev0, s));
   ListArgs la;
-  int rc = enqueue_counts(c, dP, dPb, mixed, la, kernels);
+  int rc = enqueue_counts(c, dP, dPb, mixed, LLONG_MAX, la, kernels);
   if (rc) return rc;
-  std::vector<long long> goff(3 * ng);
-  TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, 3 * ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  std::vector<long long> goff(3 * ng + 1);
+  TF_CUDA(cudaMemcpyAsync(goff.data(), c->d_group_offsets.p, (3 * ng + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
+                          s));
   TF_CUDA(cudaStreamSynchronize(s));
   TF_CUDA(cudaEventRecord(c->ev1, s));
   const long long nq_total = ng > 0 ? goff[3 * (ng - 1) + 2] : 0;

@@ -137,17 +137,19 @@ class RHF:
             max_iter: int = 100, mixed: bool = False, fp64_final: int = 2, incremental: bool = False,
             rebuild_every: int = 16, guess_name: str = "core", mixed_until: float = 1e-6,
             fallback: Optional[Callable[[], torch.Tensor]] = None, fallback_after: int = 3,
-            shrink: Optional[float] = None, loose_max: float = 1e-9,
+            shrink: Optional[float] = None, loose_max: float = 1e-9, final_at: float = 10.0,
             verbose: bool = False) -> SCFResult:
         """Converge from P0 (default: core guess).
 
         With ``mixed`` or ``incremental`` the SCF runs in two states.  "cheap": Fock
         builds from the density change (incremental, a full rebuild every
         ``rebuild_every`` cycles) and, while |dE| >= ``mixed_until``, with FP32
-        quartets below the Schwarz x density cut.  Once the convergence test passes
-        in the cheap state, the SCF continues with full FP64 builds and stops when the
-        test passes again after at least ``fp64_final`` of them, so the reported energy
-        comes from full FP64 Fock matrices.
+        quartets below the Schwarz x density cut.  Once the DIIS error in the cheap
+        state is below ``final_at`` x ``diis_tol`` (or the convergence test passes), the
+        SCF continues with full FP64 builds and stops when the test passes after at
+        least ``fp64_final`` of them, so the reported energy comes from full FP64 Fock
+        matrices; with ``final_at`` > 1 those full builds fall on cycles the SCF needs
+        anyway instead of being added after convergence.
 
         ``fallback``: a callable giving a replacement density; used (once) if the DIIS
         error after ``fallback_after`` cycles is not below the first cycle's.
@@ -227,7 +229,7 @@ class RHF:
             if state == "final" and passed and n_final >= min(fp64_final, it + 1):
                 converged = True
                 break
-            if state == "cheap" and passed:
+            if state == "cheap" and (passed or (E_old is not None and err_n < final_at * diis_tol)):
                 state = "final"
             if it >= max_iter:
                 break
