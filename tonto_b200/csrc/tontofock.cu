@@ -432,10 +432,10 @@ struct JKArgs {
 #ifndef TF_JK_MINB
 #define TF_JK_MINB 1
 #endif
-// Resident blocks per SM the compiler must allow (bounds the registers per thread).
-// Variant 0 leaves the registers to the compiler (one-root classes: 5 blocks);
-// variant 1 asks for more resident warps (6 blocks for one root, 4 otherwise),
-// at the price of fewer registers.  The autotuner times both per class.
+// Resident warps per SM, in units of four (bounds the registers per thread).
+// Variant 0 leaves the registers to the compiler (one-root classes: 20 warps);
+// variant 1 asks for more resident warps (24 for one root, 16 otherwise), at the
+// price of fewer registers.  The autotuner times both per class.
 template <int LA, int LB, int LC, int LD, int V>
 constexpr int jk_min_blocks() {
   return Quartet<LA, LB, LC, LD>::NROOT == 1 ? ((V & 1) ? 6 : TF_JK_MINB_N1) : ((V & 1) ? 4 : TF_JK_MINB);
@@ -443,9 +443,19 @@ constexpr int jk_min_blocks() {
 // Variant bits: 1 = more resident warps (see above); 2 = K atomics of lanes that hit
 // the same element summed first (segmented warp sums, bra-uniform warps).
 constexpr int JK_VARIANTS = 4;
+// Threads per block: the resident warps of an SM form one block, so the SM holds
+// one copy of the shared Rys/Boys grid and leaves the rest of its shared storage to
+// the L1 cache, which serves the bra primitive records every iteration re-reads
+// (measured on (H2O)32, (ps|ss): L1 hit rate 42% -> 62%, 14.8 -> 13.7 ms against
+// five blocks of 128 threads).  A variant with no register bound uses up to 255
+// registers: 256 threads per SM.
+template <int LA, int LB, int LC, int LD, int V>
+constexpr int jk_threads() {
+  return jk_min_blocks<LA, LB, LC, LD, V>() == 1 ? 256 : 128 * jk_min_blocks<LA, LB, LC, LD, V>();
+}
 
 template <int LA, int LB, int LC, int LD, typename T, int V>
-__global__ void __launch_bounds__(128, jk_min_blocks<LA, LB, LC, LD, V>()) k_jk(JKArgs a) {
+__global__ void __launch_bounds__(jk_threads<LA, LB, LC, LD, V>(), 1) k_jk(JKArgs a) {
   using Q = Quartet<LA, LB, LC, LD>;
   using RS = RysSmem<Q::NROOT>;
   extern __shared__ double rys_tab[];
@@ -1620,17 +1630,24 @@ static void class_l(int k, int& lh, int& ll) {
 template <int LA, int LB, int LC, int LD, typename T, int V>
 static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
+  constexpr int thr = jk_threads<LA, LB, LC, LD, V>();
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {
     cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T, V>, 128, smem);
+    {                                  // shared storage for one block, the rest to L1
+      int dev = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+      const int pct = per_sm > 0 ? std::min(100, (int)((smem + 2048) * 100 / per_sm) + 1) : 100;
+      cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T, V>, thr, smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   if (a.n <= 0 && !a.range) return;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int thr = 128;
   const long long full = (long long)nsm * blocks_per_sm;
   const long long blocks = a.range ? full : std::min<long long>((a.n + thr - 1) / thr, full);
   k_jk<LA, LB, LC, LD, T, V><<<(unsigned)blocks, thr, smem, s>>>(a);
