@@ -183,7 +183,7 @@ typedef struct tf_tune {
 
 /* Autotuner for the kernels and the class schedule of graph builds.  Class-by-class
  * builds of the density dP (device arrays as tf_build_jk_device) time each class
- * pair's kernel in four variants (registers left to the compiler or more resident
+ * pair's kernel in its variants (registers left to the compiler or more resident
  * warps; exchange atomics per lane or summed first over lanes that hit the same
  * element) and keep the fastest per class pair; a further build gives
  * each class pair's device time; then for 1 .. max_streams (<= 8) graph branches the class pairs
@@ -193,6 +193,12 @@ typedef struct tf_tune {
  * from the kernel variants chosen here.  Fills *out if not NULL.  Results do not depend
  * on the schedule beyond summation order.  No reference counterpart. */
 int tf_autotune(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags, int max_streams, tf_tune* out);
+
+/* Run every class pair's thread kernel in one variant (0 .. 3, as tf_autotune
+ * numbers them: bit 0 more resident warps, bit 1 exchange atomics summed over lanes
+ * first) until the next tf_autotune or tf_set_kernel_variant.
+ * Results do not depend on it beyond summation order.  No reference counterpart. */
+int tf_set_kernel_variant(tf_ctx* ctx, int variant);
 
 /* Restrict this context's builds to shard `index` of `count`: every count-th bra
  * shell-pair task, as one MPI rank of Tonto's round-robin parallel do

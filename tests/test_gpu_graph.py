@@ -86,3 +86,25 @@ def test_autotuned_schedule_keeps_results(cuda_ok, oracle_mod):
         torch.cuda.synchronize()
         assert fb.stats()["graph"] == 1
         assert np.max(np.abs(J.cpu().numpy().T - Jr)) < 1e-11 and np.max(np.abs(K.cpu().numpy().T - Kr)) < 1e-11
+
+
+@pytest.mark.gpu
+def test_every_kernel_variant_matches_oracle(cuda_ok, oracle_mod):
+    """Each kernel variant the autotuner may choose (tf_set_kernel_variant 0 .. 3)
+    gives the oracle's J and K; an out-of-range variant is refused."""
+    from tonto_b200.fock import FockBuilder
+    mol = water_cluster(3, seed=8)
+    n = mol.n_bf
+    rng = np.random.default_rng(12)
+    A = rng.normal(size=(n, n)) * 0.05
+    P = A + A.T
+    Jr, Kr = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12).jk(P)
+    fb = FockBuilder(mol, schwarz_cutoff=1e-12)
+    for v in range(4):
+        fb.set_kernel_variant(v)
+        for _ in range(2):                       # first build direct, second from the graph
+            J, K = fb.make_r_JK(P)
+            assert np.max(np.abs(J - Jr)) < 1e-11 and np.max(np.abs(K - Kr)) < 1e-11, v
+    from tonto_b200.fock import TontoFockError
+    with pytest.raises(TontoFockError):
+        fb.set_kernel_variant(4)

@@ -433,104 +433,125 @@ __device__ __forceinline__ double4 ld4(const PrimPair* p, int half) {
 #define TF_PRIM_UNROLL 1
 #endif
 constexpr int kPrimUnroll = TF_PRIM_UNROLL;
+constexpr int PPS = sizeof(PrimPair) / sizeof(double2);         // 5 16-byte loads per record
 
+// The loaded part of a primitive-pair record: (Px, Py), (Pz, zeta), (cc, 1/(2 zeta)),
+// and (PAx, PAy), (PAz, -) only where the recurrences need P - A.
+struct PrimRegs {
+  double2 P, Z, C, A0, A1;
+};
+
+template <bool NEED_PA>
+__device__ __forceinline__ PrimRegs load_prim(const double2* __restrict__ q, int i) {
+  PrimRegs r;
+  r.P = __ldg(q + i * PPS);
+  r.Z = __ldg(q + i * PPS + 1);
+  r.C = __ldg(q + i * PPS + 2);
+  if constexpr (NEED_PA) {
+    r.A0 = __ldg(q + i * PPS + 3);
+    r.A1 = __ldg(q + i * PPS + 4);
+  } else {
+    r.A0 = r.A1 = make_double2(0.0, 0.0);
+  }
+  return r;
+}
+
+// One primitive quartet: Rys nodes and weights, the 2D recurrences and the
+// (e0|f0) products, added to esfs with weight `wmask`.
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void prim_quartet(const PrimRegs& B, const PrimRegs& K, double wmask,
+                                             T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
+                                             const double* __restrict__ rys_smem) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
+  const double bcc = B.C.x * TWOPI5ON2, kcc = K.C.x;
+  const double zeta = B.Z.y, half_zinv = B.C.y;
+  const double eta = K.Z.y, half_einv = K.C.y;
+  const double inv = rcp_nr(zeta + eta);
+  const double rho = zeta * eta * inv;
+  const double QPx = K.P.x - B.P.x, QPy = K.P.y - B.P.y, QPz = K.Z.x - B.Z.x;
+  const double xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
+  double u[NR], w[NR];
+  if (rys_smem) RysSmem<NR>::eval(rys_smem, xx, u, w);
+  else rys_eval<NR>(xx, u, w);
+  const double scale = bcc * kcc * (rho * rsqrt_nr(rho)) * wmask;
+  const double r_z = eta * inv;     // rho / zeta
+  const double r_e = zeta * inv;    // rho / eta
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const double t2 = u[r];
+    const double t2_rz = t2 * r_z, t2_re = t2 * r_e;
+    const T B10 = T((1.0 - t2_rz) * half_zinv);
+    const T B01 = T((1.0 - t2_re) * half_einv);
+    const T B00 = T(0.5 * t2 * inv);
+    const T wt = T(w[r] * scale);
+    T I[3][D1][D2];
+    const double PA[3] = {B.A0.x, B.A0.y, B.A1.x};
+    const double QC[3] = {K.A0.x, K.A0.y, K.A1.x};
+    const double QP[3] = {QPx, QPy, QPz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T c00 = T(PA[d] + t2_rz * QP[d]);
+      const T d00 = T(QC[d] - t2_re * QP[d]);
+      I[d][0][0] = (d == 2) ? wt : T(1);
+      if (D1 > 1) I[d][1][0] = c00 * I[d][0][0];
+#pragma unroll
+      for (int e = 1; e + 1 < D1; ++e) I[d][e + 1][0] = c00 * I[d][e][0] + T(e) * B10 * I[d][e - 1][0];
+#pragma unroll
+      for (int f = 0; f + 1 < D2; ++f) {
+#pragma unroll
+        for (int e = 0; e < D1; ++e) {
+          T v = d00 * I[d][e][f];
+          if (f > 0) v += T(f) * B01 * I[d][e][f - 1];
+          if (e > 0) v += T(e) * B00 * I[d][e - 1][f];
+          I[d][e][f + 1] = v;
+        }
+      }
+    }
+    static_for<Q::NE>([&](auto e) {
+      constexpr int ge = Q::FE + decltype(e)::value;
+      static_for<Q::NF>([&](auto f) {
+        constexpr int gf = Q::FF + decltype(f)::value;
+        esfs[decltype(e)::value][decltype(f)::value] +=
+            I[0][gx(ge)][gx(gf)] * I[1][gy(ge)][gy(gf)] * I[2][gz(ge)][gz(gf)];
+      });
+    });
+  }
+}
+
+// One flat loop over the nbp x nkp primitive quartets: lanes with the same count but
+// different (nbp, nkp) splits stay converged.  Kets are the outer index and bras the
+// inner one: the lanes of a warp share the bra pair (bra-major lists), so the
+// per-iteration bra loads are warp-wide broadcasts and each lane's ket record is
+// read once per ket primitive, one iteration ahead.  (Two primitive quartets per
+// iteration as independent chains measured no faster on (H2O)32.)
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void accumulate_esfs(const PrimPair* __restrict__ bp, int nbp,
                                                 const PrimPair* __restrict__ kp, int nkp,
                                                 T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
                                                 const double* __restrict__ rys_smem = nullptr) {
   using Q = Quartet<LA, LB, LC, LD>;
-  constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
+  constexpr bool BPA = Q::LAB > 0, KPA = Q::LCD > 0;
 #pragma unroll
   for (int e = 0; e < Q::NE; ++e)
 #pragma unroll
     for (int f = 0; f < Q::NF; ++f) esfs[e][f] = T(0);
-
-  // one flat loop over the nbp x nkp primitive quartets: lanes with the same count
-  // but different (nbp, nkp) splits stay converged.  Kets are the outer index and
-  // bras the inner one: the lanes of a warp share the bra pair (bra-major lists),
-  // so the per-iteration bra loads are warp-wide broadcasts and each lane's ket
-  // record is read once per ket primitive.  P - A and 1/(2 zeta) only where needed.
   const int npq = nbp * nkp;
-  int ib = 0, ik = 0;
+  if (npq <= 0) return;
   const double2* bq = reinterpret_cast<const double2*>(bp);
   const double2* kq = reinterpret_cast<const double2*>(kp);
-  constexpr int PPS = sizeof(PrimPair) / sizeof(double2);       // 5
-  double2 kP, kZ, kC, kA0 = make_double2(0.0, 0.0), kA1 = make_double2(0.0, 0.0);
-  auto load_ket = [&](int i) {
-    kP = __ldg(kq + i * PPS); kZ = __ldg(kq + i * PPS + 1); kC = __ldg(kq + i * PPS + 2);
-    if constexpr (Q::LCD > 0) { kA0 = __ldg(kq + i * PPS + 3); kA1 = __ldg(kq + i * PPS + 4); }
-  };
-  if (npq > 0) load_ket(0);
+  int ib = 0, ik = 0;
+  PrimRegs kc = load_prim<KPA>(kq, 0);
 #pragma unroll(kPrimUnroll)
   for (int p = 0; p < npq; ++p) {
-    {
-      const double2 bP = __ldg(bq + ib * PPS), bZ = __ldg(bq + ib * PPS + 1), bC = __ldg(bq + ib * PPS + 2);
-      double2 bA0 = make_double2(0.0, 0.0), bA1 = make_double2(0.0, 0.0);
-      if constexpr (Q::LAB > 0) { bA0 = __ldg(bq + ib * PPS + 3); bA1 = __ldg(bq + ib * PPS + 4); }
-      const double4 b0 = make_double4(bP.x, bP.y, bZ.x, bZ.y);
-      const double4 b1 = make_double4(bA0.x, bA0.y, bA1.x, bC.y);
-      const double4 k0 = make_double4(kP.x, kP.y, kZ.x, kZ.y);
-      const double4 k1 = make_double4(kA0.x, kA0.y, kA1.x, kC.y);
-      const double bcc = bC.x * TWOPI5ON2, kcc = kC.x;
-      const double zeta = b0.w, half_zinv = b1.w;
-      if (++ib == nbp) {
-        ib = 0;
-        ++ik;
-        if (ik < nkp) load_ket(ik);
-      }
-      const double eta = k0.w, half_einv = k1.w;
-      const double inv = rcp_nr(zeta + eta);
-      const double rho = zeta * eta * inv;
-      const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
-      const double xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
-      double u[NR], w[NR];
-      if (rys_smem) RysSmem<NR>::eval(rys_smem, xx, u, w);
-      else rys_eval<NR>(xx, u, w);
-      const double scale = bcc * kcc * (rho * rsqrt_nr(rho));
-      const double r_z = eta * inv;     // rho / zeta
-      const double r_e = zeta * inv;    // rho / eta
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        const double t2 = u[r];
-        const double t2_rz = t2 * r_z, t2_re = t2 * r_e;
-        const T B10 = T((1.0 - t2_rz) * half_zinv);
-        const T B01 = T((1.0 - t2_re) * half_einv);
-        const T B00 = T(0.5 * t2 * inv);
-        const T wt = T(w[r] * scale);
-        T I[3][D1][D2];
-        const double PA[3] = {b1.x, b1.y, b1.z};
-        const double QC[3] = {k1.x, k1.y, k1.z};
-        const double QP[3] = {QPx, QPy, QPz};
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const T c00 = T(PA[d] + t2_rz * QP[d]);
-          const T d00 = T(QC[d] - t2_re * QP[d]);
-          I[d][0][0] = (d == 2) ? wt : T(1);
-          if (D1 > 1) I[d][1][0] = c00 * I[d][0][0];
-#pragma unroll
-          for (int e = 1; e + 1 < D1; ++e) I[d][e + 1][0] = c00 * I[d][e][0] + T(e) * B10 * I[d][e - 1][0];
-#pragma unroll
-          for (int f = 0; f + 1 < D2; ++f) {
-#pragma unroll
-            for (int e = 0; e < D1; ++e) {
-              T v = d00 * I[d][e][f];
-              if (f > 0) v += T(f) * B01 * I[d][e][f - 1];
-              if (e > 0) v += T(e) * B00 * I[d][e - 1][f];
-              I[d][e][f + 1] = v;
-            }
-          }
-        }
-        static_for<Q::NE>([&](auto e) {
-          constexpr int ge = Q::FE + decltype(e)::value;
-          static_for<Q::NF>([&](auto f) {
-            constexpr int gf = Q::FF + decltype(f)::value;
-            esfs[decltype(e)::value][decltype(f)::value] +=
-                I[0][gx(ge)][gx(gf)] * I[1][gy(ge)][gy(gf)] * I[2][gz(ge)][gz(gf)];
-          });
-        });
-      }
+    const PrimRegs b = load_prim<BPA>(bq, ib);
+    const PrimRegs k = kc;
+    if (++ib == nbp) {
+      ib = 0;
+      ++ik;
+      if (ik < nkp) kc = load_prim<KPA>(kq, ik);
     }
+    prim_quartet<LA, LB, LC, LD, T>(b, k, 1.0, esfs, rys_smem);
   }
 }
 

@@ -435,13 +435,13 @@ struct JKArgs {
 // Resident warps per SM, in units of four (bounds the registers per thread).
 // Variant 0 leaves the registers to the compiler (one-root classes: 20 warps);
 // variant 1 asks for more resident warps (24 for one root, 16 otherwise), at the
-// price of fewer registers.  The autotuner times both per class.
+// price of fewer registers.  The autotuner times the variants per class.
 template <int LA, int LB, int LC, int LD, int V>
 constexpr int jk_min_blocks() {
   return Quartet<LA, LB, LC, LD>::NROOT == 1 ? ((V & 1) ? 6 : TF_JK_MINB_N1) : ((V & 1) ? 4 : TF_JK_MINB);
 }
 // Variant bits: 1 = more resident warps (see above); 2 = K atomics of lanes that hit
-// the same element summed first (segmented warp sums, bra-uniform warps).
+// the same element summed first (segmented warp sums over lanes of one bra).
 constexpr int JK_VARIANTS = 4;
 // Threads per block: the resident warps of an SM form one block, so the SM holds
 // one copy of the shared Rys/Boys grid and leaves the rest of its shared storage to
@@ -1661,7 +1661,7 @@ static void launch_jk_v(const JKArgs& a, cudaStream_t s, bool fp32) {
 
 template <int LA, int LB, int LC, int LD>
 static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
-  switch (variant) {
+  switch (variant & 3) {
     case 1: launch_jk_v<LA, LB, LC, LD, 1>(a, s, fp32); break;
     case 2: launch_jk_v<LA, LB, LC, LD, 2>(a, s, fp32); break;
     case 3: launch_jk_v<LA, LB, LC, LD, 3>(a, s, fp32); break;
@@ -2266,6 +2266,13 @@ int tf_set_schwarz_cutoff(tf_ctx* c, double cutoff) {
 int tf_set_list_budget(tf_ctx* c, long long quartets) {
   if (!c || quartets <= 0) { tf::set_error("bad list budget"); return TF_EINVAL; }
   c->list_budget = quartets;
+  return TF_OK;
+}
+
+int tf_set_kernel_variant(tf_ctx* c, int variant) {
+  if (!c || variant < 0 || variant >= tf::JK_VARIANTS) { tf::set_error("bad kernel variant"); return TF_EINVAL; }
+  std::fill(c->cls_variant.begin(), c->cls_variant.end(), variant);
+  tf::drop_graph(c);                   // captured launches hold the old kernels
   return TF_OK;
 }
 
