@@ -194,8 +194,12 @@ def main():
         for r, W in herm[n]:
             r2.append(float(r ** 2).hex())
             ww.append(float(W).hex())
-    lines.append("TF_RYS_CONST double tf_rys_hroot2[%d] = {%s};" % (ht, ", ".join(r2)))
-    lines.append("TF_RYS_CONST double tf_rys_hweight[%d] = {%s};" % (ht, ", ".join(ww)))
+    # the small asymptotic tables may live in a faster memory space than the large one
+    lines.append("#ifndef TF_RYS_SMALL_CONST")
+    lines.append("#define TF_RYS_SMALL_CONST TF_RYS_CONST")
+    lines.append("#endif")
+    lines.append("TF_RYS_SMALL_CONST double tf_rys_hroot2[%d] = {%s};" % (ht, ", ".join(r2)))
+    lines.append("TF_RYS_SMALL_CONST double tf_rys_hweight[%d] = {%s};" % (ht, ", ".join(ww)))
     with open(args.out, "w") as fh:
         fh.write("\n".join(lines) + "\n")
     with open(args.golden, "w") as fh:

@@ -22,6 +22,9 @@
 #include <type_traits>
 
 #define TF_RYS_CONST __device__ const
+// the asymptotic-rule tables in the constant bank: read at compile-time indices,
+// they become immediate operands instead of global loads
+#define TF_RYS_SMALL_CONST __constant__ const
 #include "rys_tables.inc"
 #include "boys_table.inc"
 #include "boys2_table.inc"
