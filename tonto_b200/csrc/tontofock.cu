@@ -1465,6 +1465,12 @@ static int setup_pairs(tf_ctx* c) {
   c->pair_cls.clear();
   c->mol_pair0.assign(c->n_mol + 1, 0);
   long long full_tot = 0;
+  {
+    long long np_all = 0;
+    for (int m = 0; m < c->n_mol; ++m) np_all += (long long)c->mols[m].n_shell * (c->mols[m].n_shell + 1) / 2;
+    c->pairs_h.reserve(np_all);
+    c->pair_cls.reserve(np_all);
+  }
   for (int m = 0; m < c->n_mol; ++m) {
     const MolInfo& mi = c->mols[m];
     c->mol_pair0[m] = (long long)c->pairs_h.size();
@@ -1555,14 +1561,19 @@ static int setup_pairs(tf_ctx* c) {
   std::vector<std::vector<int>> lists((size_t)c->n_mol * NPAIRCLS);
   for (long long p = 0; p < c->n_pairs; ++p)
     lists[(size_t)c->pairs_h[p].mol * NPAIRCLS + c->pair_cls[p]].push_back((int)p);
-  auto band = [&](int p) {
+  std::vector<int> band_of(c->n_pairs);               // half-decade band of each pair, computed once
+  for (long long p = 0; p < c->n_pairs; ++p) {
     const double v = c->pairs_h[p].imax;
-    return v > 0.0 ? (int)std::floor(2.0 * std::log10(v)) : -1000000;
-  };
+    band_of[p] = v > 0.0 ? (int)std::floor(2.0 * std::log10(v)) : -1000000;
+  }
+  auto band = [&](int p) { return band_of[p]; };
+  sorted.reserve(c->n_pairs);
+  simax.reserve(c->n_pairs);
+  sbmax.reserve(c->n_pairs);
   for (size_t q = 0; q < lists.size(); ++q) {
     auto& v = lists[q];
     std::sort(v.begin(), v.end(), [&](int x, int y) {
-      const int bx = band(x), by = band(y);
+      const int bx = band_of[x], by = band_of[y];
       return bx != by ? bx > by : x < y;
     });
     c->cls_off[q] = (int)sorted.size();

@@ -95,26 +95,21 @@ def solid_harmonics(l: int) -> np.ndarray:
 
 
 def cart_rotation(l: int, R: np.ndarray) -> np.ndarray:
-    """C[c, c'] with m_c(R r) = sum_c' C[c, c'] m_c'(r) for the degree-l monomials."""
+    """C[c, c'] with m_c(R r) = sum_c' C[c, c'] m_c'(r) for the degree-l monomials:
+    the product of a copies of row 0, b of row 1 and c of row 2 of R, expanded (the
+    outer product of those rows, summed into the monomials its index tuples give)."""
     comps = cart_components(l)
+    if l == 0:
+        return np.ones((1, 1))
     idx = {c: i for i, c in enumerate(comps)}
+    tgt = np.array([idx[tuple(kk.count(d) for d in range(3))] for kk in itertools.product(range(3), repeat=l)])
     C = np.zeros((len(comps), len(comps)))
     for i, (a, b, c) in enumerate(comps):
-        # product of a copies of row 0, b of row 1, c of row 2 of R, expanded
         rows = [0] * a + [1] * b + [2] * c
-        poly = {(0, 0, 0): 1.0}
-        for r in rows:
-            new = {}
-            for mono, v in poly.items():
-                for k in range(3):
-                    if R[r, k] != 0.0:
-                        m2 = list(mono)
-                        m2[k] += 1
-                        m2 = tuple(m2)
-                        new[m2] = new.get(m2, 0.0) + v * R[r, k]
-            poly = new
-        for mono, v in poly.items():
-            C[i, idx[mono]] += v
+        T = R[rows[0]]
+        for r in rows[1:]:
+            T = np.multiply.outer(T, R[r])
+        C[i] = np.bincount(tgt, weights=T.ravel(), minlength=len(comps))
     return C
 
 
@@ -173,7 +168,9 @@ def water_ao_ranges(mol: Molecule) -> List[Tuple[int, int]]:
 
 
 def water_ao_rotation(mol: Molecule, w: Tuple[int, int, int], R: np.ndarray) -> np.ndarray:
-    blocks = [shell_rotation(s.l, R, mol.spherical) for s in mol.shells if s.atom in w]
+    by_l = {}                                       # one rotation block per angular momentum
+    blocks = [by_l.setdefault(s.l, shell_rotation(s.l, R, mol.spherical)) if s.l not in by_l else by_l[s.l]
+              for s in mol.shells if s.atom in w]
     n = sum(b.shape[0] for b in blocks)
     A = np.zeros((n, n))
     k = 0

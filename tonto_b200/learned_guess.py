@@ -57,12 +57,15 @@ def cluster_geometry(mol: Molecule):
 
 
 def pair_list(atoms: np.ndarray) -> List[Tuple[int, int]]:
+    """Every water with itself, then the pairs (v < w) whose O atoms are closer than
+    PAIR_CUTOFF, in row order."""
     n = len(atoms)
     out = [(v, v) for v in range(n)]
-    for v in range(n):
-        for w in range(v + 1, n):
-            if np.linalg.norm(atoms[w, 0] - atoms[v, 0]) < PAIR_CUTOFF:
-                out.append((v, w))
+    if n > 1:
+        O = atoms[:, 0]
+        d = np.linalg.norm(O[None, :, :] - O[:, None, :], axis=2)
+        vs, ws = np.nonzero(np.triu(d < PAIR_CUTOFF, k=1))
+        out.extend(zip(vs.tolist(), ws.tolist()))
     return out
 
 
@@ -70,26 +73,49 @@ def d_in(env_k: int) -> int:
     return 1 + 9 + 1 + env_k * 10
 
 
+def _fc(r: np.ndarray) -> np.ndarray:
+    return np.where(r < RC, 0.5 * (np.cos(np.pi * r / RC) + 1.0), 0.0)
+
+
 def descriptors(atoms: np.ndarray, frames, pairs, env_k: int = ENV_K) -> np.ndarray:
+    """Per pair (v, w), in the local frame R_v of water v with O_v at the origin:
+    [v == w], the three atoms of w and fc(|O_w - O_v|) (v != w), then the env_k
+    waters u != v, w nearest to the pair centre (O_v, or the O-O midpoint; ties by
+    index) with their three atoms and fc(distance to the centre); missing
+    neighbours stay zero.  All pairs of a cluster at once."""
     n = len(atoms)
     X = np.zeros((len(pairs), d_in(env_k)), dtype=np.float64)
-    for k, (v, w) in enumerate(pairs):
-        R = frames[v]
-        Ov = atoms[v, 0]
-        f = X[k]
-        if v == w:
-            f[0] = 1.0
-            centre = Ov
-        else:
-            f[1:10] = ((atoms[w] - Ov) @ R.T).ravel()
-            f[10] = fc(float(np.linalg.norm(atoms[w, 0] - Ov)))
-            centre = 0.5 * (Ov + atoms[w, 0])
-        others = [u for u in range(n) if u != v and u != w]
-        others.sort(key=lambda u: float(np.linalg.norm(atoms[u, 0] - centre)))
-        for j, u in enumerate(others[:env_k]):
-            base = 11 + 10 * j
-            f[base:base + 9] = ((atoms[u] - Ov) @ R.T).ravel()
-            f[base + 9] = fc(float(np.linalg.norm(atoms[u, 0] - centre)))
+    if not pairs:
+        return X
+    P = len(pairs)
+    pv = np.array([p[0] for p in pairs])
+    pw = np.array([p[1] for p in pairs])
+    Rv = np.asarray(frames, dtype=np.float64)[pv]                    # (P, 3, 3), rows = local axes
+    O = atoms[:, 0]
+    Ov = O[pv]
+    same = pv == pw
+    diff = ~same
+
+    def local(u):                                                    # (atoms[u] - O_v) @ R_v^T, flattened
+        return np.einsum("pak,pjk->paj", atoms[u] - Ov[:, None, :], Rv).reshape(P, 9)
+
+    X[same, 0] = 1.0
+    X[diff, 1:10] = local(pw)[diff]
+    X[diff, 10] = _fc(np.linalg.norm(O[pw] - Ov, axis=1))[diff]
+    centre = np.where(same[:, None], Ov, 0.5 * (Ov + O[pw]))
+    dist = np.linalg.norm(O[None, :, :] - centre[:, None, :], axis=2)  # (P, n)
+    masked = dist.copy()
+    rows = np.arange(P)
+    masked[rows, pv] = np.inf
+    masked[rows, pw] = np.inf
+    order = np.argsort(masked, axis=1, kind="stable")
+    n_others = n - np.where(same, 1, 2)
+    for j in range(min(env_k, n)):
+        ok = j < n_others
+        u = order[:, j]
+        base = 11 + 10 * j
+        X[ok, base:base + 9] = local(u)[ok]
+        X[ok, base + 9] = _fc(dist[rows, u])[ok]
     return X
 
 
