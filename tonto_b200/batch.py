@@ -93,13 +93,12 @@ class BatchRHF:
         self.buckets = [_Bucket(ids, n_bf, dev) for ids in cuts if ids]
         # concatenated <-> padded index maps (the matrices are symmetric)
         self.off = [int(v) for v in self.fb.offsets]
-        for b in self.buckets:
+        for b in self.buckets:                    # built on the device
             idx = []
             for k, i in enumerate(b.ids):
-                n = n_bf[i]
-                rr, cc = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
-                idx.append((k * b.n * b.n + rr * b.n + cc).ravel())
-            b.pad_idx = torch.tensor(np.concatenate(idx), device=dev)
+                r = torch.arange(n_bf[i], device=dev)
+                idx.append((k * b.n * b.n + r[:, None] * b.n + r[None, :]).reshape(-1))
+            b.pad_idx = torch.cat(idx)
             b.cat_idx = torch.cat([torch.arange(self.off[i], self.off[i + 1], device=dev) for i in b.ids])
         S, T, V = self.fb.one_electron()
         for b in self.buckets:
