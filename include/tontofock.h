@@ -139,7 +139,8 @@ int tf_build_jk_uhf(tf_ctx* ctx, const double* Pa, const double* Pb, double* Ja,
                     double* Kb, int flags);
 
 /* The same on device arrays (the context's concatenated molecule blocks), ordered
- * on `stream` (NULL: the context's own stream). */
+ * after the caller's earlier work on `stream` and before its later work, as
+ * tf_build_jk_device. */
 int tf_build_jk_uhf_device(tf_ctx* ctx, const double* dPa, const double* dPb, double* dJa, double* dJb,
                            double* dKa, double* dKb, int flags, void* stream);
 
@@ -162,6 +163,13 @@ int tf_set_schwarz_cutoff(tf_ctx* ctx, double cutoff);
  * No reference counterpart (the reference keeps no quartet lists). */
 int tf_set_list_budget(tf_ctx* ctx, long long quartets);
 
+/* Device memory for the screening record (one byte per candidate bra-ket pair,
+ * default 12 GiB): when the candidates fit, the counting pass records its
+ * screening and the list write only compacts the record; otherwise the list write
+ * screens again.  bytes = 0 always screens twice.  Results do not depend on it.
+ * No reference counterpart. */
+int tf_set_screen_record_budget(tf_ctx* ctx, long long bytes);
+
 /* CUDA-graph builds (default on).  After a first build has sized the quartet
  * list, each build is one captured graph (density transform, screening, list,
  * every class launch with its quartet range read on the device, Fock
@@ -181,7 +189,8 @@ typedef struct tf_tune {
   int variant_classes;               /* class pairs whose kernel runs a variant other than the default */
 } tf_tune;
 
-/* Autotuner for the kernels and the class schedule of graph builds.  Class-by-class
+/* Autotuner for the kernels and the class schedule of graph builds.  It first waits
+ * for all earlier work on the device; then class-by-class
  * builds of the density dP (device arrays as tf_build_jk_device) time each class
  * pair's kernel in its variants (registers left to the compiler or more resident
  * warps; exchange atomics per lane or summed first over lanes that hit the same
@@ -211,8 +220,11 @@ int tf_set_shard(tf_ctx* ctx, int index, int count);
  * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*. */
 int tf_build_jk(tf_ctx* ctx, const double* P, double* J, double* K, int flags);
 
-/* Same, on device arrays (n_bf*n_bf doubles each) on the CUDA stream `stream`
- * (a cudaStream_t, or NULL for the context's own stream).  Asynchronous. */
+/* Same, on device arrays (n_bf*n_bf doubles each).  `stream` is the caller's
+ * cudaStream_t (NULL is CUDA's legacy default stream): the build runs on the
+ * context's own stream, ordered after the caller's earlier work on `stream` (so
+ * dP may still be being written there) and before its later work; the call
+ * returns when the build has finished. */
 int tf_build_jk_device(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags, void* stream);
 
 /* F = Hcore + J - K/2 from P (host arrays).  Replaces make_r_Fock_mx. */

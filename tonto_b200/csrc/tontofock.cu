@@ -2283,6 +2283,17 @@ int tf_set_list_budget(tf_ctx* c, long long quartets) {
   return TF_OK;
 }
 
+int tf_set_screen_record_budget(tf_ctx* c, long long bytes) {
+  if (!c || bytes < 0) { tf::set_error("bad screening-record budget"); return TF_EINVAL; }
+  int rc = tf::set_device(c);
+  if (rc) return rc;
+  c->cand_budget = bytes;
+  const std::vector<int> keep = c->cls_variant;
+  rc = tf::build_tasks(c);             // decides whether the record is used
+  if (rc == TF_OK && keep.size() == c->cls_variant.size()) c->cls_variant = keep;
+  return rc;
+}
+
 int tf_set_kernel_variant(tf_ctx* c, int variant) {
   if (!c || variant < 0 || variant >= tf::JK_VARIANTS) { tf::set_error("bad kernel variant"); return TF_EINVAL; }
   std::fill(c->cls_variant.begin(), c->cls_variant.end(), variant);
@@ -2304,6 +2315,7 @@ int tf_autotune(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, 
   if (!c || !dP || !dJ || !dK || max_streams < 1 || max_streams > 8) { set_error("bad argument"); return TF_EINVAL; }
   int rc = set_device(c);
   if (rc) return rc;
+  TF_CUDA(cudaDeviceSynchronize());    // dP may still be being written on any of the caller's streams
   while ((int)c->side.size() < max_streams - 1) {
     cudaStream_t x;
     cudaEvent_t e;
@@ -2412,8 +2424,10 @@ int tf_build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int 
   if (!c || !dP || !dJ || !dK) { set_error("null argument"); return TF_EINVAL; }
   int rc = set_device(c);
   if (rc) return rc;
+  // NULL is the legacy default stream, which the context's non-blocking stream does
+  // not synchronise with: it is ordered explicitly like any other caller stream
   cudaStream_t user = static_cast<cudaStream_t>(stream);
-  if (user && user != c->stream) {
+  if (user != c->stream) {
     // order the context stream after the caller's work, and the caller's after ours
     cudaEvent_t e;
     TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -2451,8 +2465,8 @@ int tf_build_jk_uhf_device(tf_ctx* c, const double* dPa, const double* dPb, doub
   if (!c || !dPa || !dPb || !dJa || !dJb || !dKa || !dKb) { set_error("null argument"); return TF_EINVAL; }
   int rc = set_device(c);
   if (rc) return rc;
-  cudaStream_t user = static_cast<cudaStream_t>(stream);
-  if (user && user != c->stream) {
+  cudaStream_t user = static_cast<cudaStream_t>(stream);   // NULL: the legacy default stream
+  if (user != c->stream) {
     cudaEvent_t e;
     TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TF_CUDA(cudaEventRecord(e, user));

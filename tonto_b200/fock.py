@@ -95,6 +95,7 @@ def load_library(path: Optional[str] = None):
     L.tf_set_schwarz_cutoff.argtypes = [vp, d]
     L.tf_set_list_budget.argtypes = [vp, ctypes.c_longlong]
     L.tf_set_kernel_variant.argtypes = [vp, ctypes.c_int]
+    L.tf_set_screen_record_budget.argtypes = [vp, ctypes.c_longlong]
     L.tf_set_graph.argtypes = [vp, i]
     L.tf_build_jk_uhf.argtypes = [vp, P(d), P(d), P(d), P(d), P(d), P(d), i]
     L.tf_build_jk_uhf_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, i, vp]
@@ -184,6 +185,10 @@ class FockBuilder:
     def set_list_budget(self, quartets: int):
         """Largest quartet-list chunk (entries of 8 bytes) a build keeps on the device."""
         _check(load_library().tf_set_list_budget(self.h, int(quartets)))
+
+    def set_screen_record_budget(self, n_bytes: int):
+        """Device bytes for the screening record (0: the list write screens again)."""
+        _check(load_library().tf_set_screen_record_budget(self.h, int(n_bytes)))
 
     def set_kernel_variant(self, variant: int):
         """Run every class pair's kernel in one variant (0 .. 3; see tf_set_kernel_variant)."""
