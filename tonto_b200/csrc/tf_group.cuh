@@ -325,12 +325,6 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
 #pragma unroll
     for (int e = 0; e < Q::NE; ++e) es[e] = 0.0;
     int ib = 0, ik = 0;
-    // bras are the outer index: the bra record stays in registers while the kets run
-    // (five 16-byte loads per record, each field once)
-    const double2* bq = reinterpret_cast<const double2*>(bp);
-    const double2* kq = reinterpret_cast<const double2*>(kp);
-    PrimRegs B{};
-    if (npq > 0) B = load_prim<true>(bq, 0);
     for (int p = 0; p < maxnpq; ++p) {
       const bool v = p < npq;
       double u[NR], w[NR];
@@ -338,12 +332,9 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
               k1 = make_double4(0, 0, 0, 0);
       double inv = 0.0, r_z = 0.0, r_e = 0.0, scale = 0.0, xx = 0.0;
       if (v) {
-        const PrimRegs K = load_prim<true>(kq, ik);
-        b0 = make_double4(B.P.x, B.P.y, B.Z.x, B.Z.y);
-        b1 = make_double4(B.A0.x, B.A0.y, B.A1.x, B.C.y);
-        k0 = make_double4(K.P.x, K.P.y, K.Z.x, K.Z.y);
-        k1 = make_double4(K.A0.x, K.A0.y, K.A1.x, K.C.y);
-        const double bcc = B.C.x * TWOPI5ON2, kcc = K.C.x;
+        b0 = ld4(bp + ib, 0); b1 = ld4(bp + ib, 1);
+        k0 = ld4(kp + ik, 0); k1 = ld4(kp + ik, 1);
+        const double bcc = __ldg(&bp[ib].cc) * TWOPI5ON2, kcc = __ldg(&kp[ik].cc);
         inv = rcp_nr(b0.w + k0.w);
         const double rho = b0.w * k0.w * inv;
         const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
@@ -406,11 +397,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
           });
         }
       }
-      if (++ik == nkp) {
-        ik = 0;
-        ++ib;
-        if (p + 1 < npq) B = load_prim<true>(bq, ib);
-      }
+      if (++ik == nkp) { ik = 0; ++ib; }
     }
     __syncwarp();
     if (act) {
