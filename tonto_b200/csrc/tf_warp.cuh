@@ -1,14 +1,16 @@
-// tf_warp.cuh — warp-cooperative shell quartets for the high angular momentum
-// classes, whose (e0|f0) block (up to 31 x 31 for (dd|dd)) does not fit one
-// thread's registers.  One warp computes one contracted quartet:
+// tf_warp.cuh — warp-cooperative shell quartets with runtime angular momenta, used
+// for the Schwarz diagonal (ab|ab) of the pair classes above the thread kernels
+// (the (e0|f0) block, up to 31 x 31 for (dd|dd), does not fit one thread's
+// registers; the J/K builds of those classes use the lane-group kernels of
+// tf_group.cuh).  One warp computes one contracted quartet:
 //   * every lane evaluates the Rys nodes/weights of the primitive quartet
 //     (warp-uniform table reads);
 //   * lanes (direction, root) build the 2D recurrence tables in shared memory;
 //   * lanes own (e, f) elements of the (e0|f0) block and accumulate them in
 //     shared memory across primitive quartets;
 //   * the horizontal transfers and the digestion run with lanes over elements.
-// Angular momenta are runtime values here (compiled once), so the same code
-// also gives the Schwarz diagonal (ab|ab) of every pair class.
+// Angular momenta are runtime values here (compiled once), so one kernel serves
+// every pair class.
 #pragma once
 #include "tf_device.cuh"
 

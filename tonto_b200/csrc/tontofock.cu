@@ -675,90 +675,9 @@ __global__ void __launch_bounds__(jk_threads<LA, LB, LC, LD, V>(), 1) k_jk(JKArg
 }
 
 // ---------------------------------------------------------------------------
-// kernel: warp-cooperative quartets (high angular momentum classes)
+// kernel: Schwarz bounds of the classes above the thread kernels (one warp per pair)
 // ---------------------------------------------------------------------------
 constexpr int WARPS_PER_BLOCK = 2;
-
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int la, int lb, int lc, int ld) {
-  extern __shared__ double smem_all[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  double* sm = smem_all + wib * W_SMEM;
-  const WarpQuartet q = wq_make(la, lb, lc, ld);
-  const long long nwarps = (long long)gridDim.x * WARPS_PER_BLOCK;
-  unsigned long long nprim = 0;
-  const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
-  for (long long t = (long long)blockIdx.x * WARPS_PER_BLOCK + wib; t < a.n; t += nwarps) {
-    const int2 qd = a.quartets[t];
-    const PairRec b = a.pairs[qd.x];
-    const PairRec k = a.pairs[qd.y];
-    const MolInfo mi = a.mols[b.mol];
-    const int n = mi.n_cart;
-    const double* __restrict__ P = a.P + mi.cmat;
-    double* __restrict__ Jm = a.J + mi.cmat;
-    double* __restrict__ Km = a.K + mi.cmat;
-    const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
-                          b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
-    const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
-    const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
-    const int nbp = any_same ? b.n_full : b.n_skip;
-    const int nkp = any_same ? k.n_full : k.n_skip;
-    double f = 1.0;
-    if (b.sh_hi == b.sh_lo) f *= 0.5;
-    if (k.sh_hi == k.sh_lo) f *= 0.5;
-    if (qd.x == qd.y) f *= 0.5;
-    const double Rab[3] = {b.Rx, b.Ry, b.Rz};
-    const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
-    double* I = nullptr;
-    const int np = warp_quartet(q, bp, nbp, kp, nkp, Rab, Rcd, sm, I);
-    if (lane == 0) nprim += (unsigned long long)np;
-    const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
-    const int ncd = nc * nd;
-    for (int e = lane; e < na * nb; e += 32) {          // J(ab)
-      const int ia = e / nb, ib = e % nb;
-      double s = 0.0;
-      for (int c = 0; c < nc; ++c)
-        for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
-      atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, f * s);
-    }
-    for (int e = lane; e < ncd; e += 32) {              // J(cd)
-      const int c = e / nd, d = e % nd;
-      double s = 0.0;
-      for (int ia = 0; ia < na; ++ia)
-        for (int ib = 0; ib < nb; ++ib) s += I[(ia * nb + ib) * ncd + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ib);
-      atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
-    }
-    for (int e = lane; e < na * nc; e += 32) {          // K(ac) = sum_bd I P(bd)
-      const int ia = e / nc, c = e % nc;
-      double s = 0.0;
-      for (int ib = 0; ib < nb; ++ib)
-        for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
-      atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
-    }
-    for (int e = lane; e < na * nd; e += 32) {          // K(ad) = sum_bc I P(bc)
-      const int ia = e / nd, d = e % nd;
-      double s = 0.0;
-      for (int ib = 0; ib < nb; ++ib)
-        for (int c = 0; c < nc; ++c) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
-      atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
-    }
-    for (int e = lane; e < nb * nc; e += 32) {          // K(bc) = sum_ad I P(ad)
-      const int ib = e / nc, c = e % nc;
-      double s = 0.0;
-      for (int ia = 0; ia < na; ++ia)
-        for (int d = 0; d < nd; ++d) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
-      atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
-    }
-    for (int e = lane; e < nb * nd; e += 32) {          // K(bd) = sum_ac I P(ac)
-      const int ib = e / nd, d = e % nd;
-      double s = 0.0;
-      for (int ia = 0; ia < na; ++ia)
-        for (int c = 0; c < nc; ++c) s += I[(ia * nb + ib) * ncd + c * nd + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
-      atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
-    }
-    __syncwarp();
-  }
-  if (lane == 0 && nprim) atomicAdd(a.prim_count + qclass_id(la, lb, lc, ld), nprim);
-}
 
 // Schwarz bound of any pair class with the warp path (one warp per pair).
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int* __restrict__ ids, int n,
@@ -2174,8 +2093,6 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
         cudaMemcpyToSymbol(c_cidx, g_tables.cidx, sizeof(g_tables.cidx)) != cudaSuccess ||
         cudaMemcpyToSymbol(c_gcomp, g_tables.comp, sizeof(g_tables.comp)) != cudaSuccess ||
         cudaMemcpyToSymbol(c_gidx, g_tables.cidx, sizeof(g_tables.cidx)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_jk_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess ||
         cudaFuncSetAttribute(k_schwarz_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              WARPS_PER_BLOCK * W_SMEM * (int)sizeof(double)) != cudaSuccess) {
       delete c; set_error("constant upload"); return TF_ECUDA;
