@@ -87,7 +87,7 @@ class Oracle:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h:
+        if h and lib is not None:            # (module globals may be gone at interpreter exit)
             lib().oracle_destroy(h)
             self.h = None
 

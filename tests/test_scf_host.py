@@ -1,0 +1,81 @@
+"""The SCF driver's control flow on CPU tensors, with the oracle's J/K standing in for
+the CUDA builder: the cheap state (incremental builds of the density change), the
+switch to full FP64 builds near convergence (final_at), the two final full builds, and
+the fall-back to a second guess.  The converged energy must not depend on any of it."""
+
+import types
+
+import numpy as np
+import pytest
+import torch
+
+from tonto_b200.molecules import water_cluster
+from tonto_b200.scf import RHF
+
+
+class OracleBuilder:
+    """The slice of FockBuilder that RHF uses, computed by the oracle (all flags give
+    FP64; TF_JK_DELTA needs nothing, J and K being linear in the density)."""
+
+    def __init__(self, oracle_mod, mol):
+        self.o = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
+        self.options = types.SimpleNamespace(eri_schwarz_cutoff=1e-12)
+        self.builds = 0
+
+    def one_electron(self):
+        return self.o.one_electron()
+
+    def make_r_JK_device(self, P, J, K, flags=0):
+        Jn, Kn = self.o.jk(P.numpy())
+        J.copy_(torch.from_numpy(np.ascontiguousarray(Jn)))
+        K.copy_(torch.from_numpy(np.ascontiguousarray(Kn)))
+        self.builds += 1
+
+    def set_schwarz_cutoff(self, cut):
+        pass
+
+
+@pytest.fixture(scope="module")
+def water2(oracle_mod):
+    mol = water_cluster(2, seed=1)
+    ref = oracle_mod.scf(mol, conv=1e-9, diis_tol=1e-6)
+    return mol, ref
+
+
+def test_plain_run_matches_the_oracle_scf(oracle_mod, water2):
+    mol, ref = water2
+    rhf = RHF(mol, device=torch.device("cpu"), builder=OracleBuilder(oracle_mod, mol))
+    r = rhf.run(conv=1e-9, diis_tol=1e-6)
+    assert r.converged and abs(r.energy - ref["E"]) < 1e-9
+    assert r.builds == r.iterations + 1
+    assert all(h[4] == "fp64" for h in r.history)
+
+
+def test_incremental_run_ends_with_full_fp64_builds(oracle_mod, water2):
+    mol, ref = water2
+    cpu = torch.device("cpu")
+    plain = RHF(mol, device=cpu, builder=OracleBuilder(oracle_mod, mol)).run(conv=1e-9, diis_tol=1e-6)
+    fast = RHF(mol, device=cpu, builder=OracleBuilder(oracle_mod, mol)).run(
+        conv=1e-9, diis_tol=1e-6, mixed=True, incremental=True)
+    assert fast.converged and abs(fast.energy - ref["E"]) < 1e-9
+    kinds = [h[4] for h in fast.history]
+    assert kinds[0] == "mixed" and any(k.endswith("+delta") for k in kinds)
+    assert kinds[-2:] == ["fp64", "fp64"]                      # the last two builds full FP64
+    # the switch comes once the DIIS error is within final_at x tolerance, so the
+    # final builds fall on cycles the plain SCF needs as well
+    first_full = kinds.index("fp64", 1)
+    assert fast.history[first_full - 1][3] < 10.0 * 1e-6
+    assert fast.builds <= plain.builds + 1
+
+
+def test_fallback_replaces_a_guess_that_does_not_converge(oracle_mod, water2):
+    mol, ref = water2
+    rhf = RHF(mol, device=torch.device("cpu"), builder=OracleBuilder(oracle_mod, mol))
+    n = mol.n_bf
+    # a zero density commutes with the core Fock matrix (DIIS error 0), so the error can
+    # only grow from the first cycle: the fall-back must replace it
+    bad = torch.zeros((n, n), dtype=torch.float64)
+    good = rhf.core_guess()
+    r = rhf.run(P0=bad, conv=1e-9, diis_tol=1e-6, fallback=lambda: good, fallback_after=1)
+    assert r.fell_back
+    assert r.converged and abs(r.energy - ref["E"]) < 1e-9

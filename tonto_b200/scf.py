@@ -38,6 +38,11 @@ from .basis import Molecule
 from .fock import TF_JK_DELTA, TF_JK_FULL, TF_JK_MIXED, FockBuilder
 
 
+def _sync(dev: torch.device) -> None:
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
+
+
 @dataclass
 class SCFResult:
     energy: float
@@ -88,7 +93,7 @@ class RHF:
     def __init__(self, mol: Molecule, schwarz_cutoff: float = 1e-12, device: int = 0, diis_keep: int = 8,
                  mixed_fp32_cut: float = 1e-6, builder: Optional[FockBuilder] = None):
         self.mol = mol
-        self.dev = torch.device("cuda", device)
+        self.dev = device if isinstance(device, torch.device) else torch.device("cuda", device)
         self.fb = builder or FockBuilder(mol, schwarz_cutoff=schwarz_cutoff, device=device,
                                          mixed_fp32_cut=mixed_fp32_cut)
         self._one_electron()
@@ -160,7 +165,7 @@ class RHF:
         while the Fock error it admits stays well below the current error; the final
         full FP64 builds always use the context's own cutoff.
         """
-        torch.cuda.synchronize(self.dev)
+        _sync(self.dev)
         t0 = time.perf_counter()
         tight = self.fb.options.eri_schwarz_cutoff
         P = self.core_guess() if P0 is None else P0.to(self.dev, torch.float64).contiguous()
@@ -240,7 +245,7 @@ class RHF:
             it += 1
         if shrink is not None:
             self.fb.set_schwarz_cutoff(tight)
-        torch.cuda.synchronize(self.dev)
+        _sync(self.dev)
         return SCFResult(energy=E, converged=converged, iterations=it, builds=builds,
                          seconds=time.perf_counter() - t0, build_seconds=build_s, P=P, history=hist,
                          guess=guess_name, fell_back=fell_back)
@@ -269,7 +274,7 @@ class UHF(RHF):
 
     def run(self, conv: float = 1e-9, diis_tol: float = 1e-6, max_iter: int = 200, flags: int = TF_JK_FULL,
             verbose: bool = False) -> SCFResult:
-        torch.cuda.synchronize(self.dev)
+        _sync(self.dev)
         t0 = time.perf_counter()
         Pa = self.spin_density(self.H, self.n_alpha)
         Pb = self.spin_density(self.H, self.n_beta)
@@ -302,7 +307,7 @@ class UHF(RHF):
             Pa = self.spin_density(Fx[:n], self.n_alpha)
             Pb = self.spin_density(Fx[n:], self.n_beta)
             it += 1
-        torch.cuda.synchronize(self.dev)
+        _sync(self.dev)
         res = SCFResult(energy=E, converged=converged, iterations=it, builds=it + 1,
                         seconds=time.perf_counter() - t0, build_seconds=0.0, P=Pa + Pb, history=hist)
         res.Pa, res.Pb = Pa, Pb
