@@ -33,7 +33,7 @@ import torch
 
 from .basis import Molecule
 from .fock import TF_JK_DELTA, TF_JK_FULL, TF_JK_MIXED, BatchFockBuilder
-from .scf import SCFResult
+from .scf import SCFResult, _sync
 
 
 class _Bucket:
@@ -78,13 +78,13 @@ def purify(Fo: torch.Tensor, valid: torch.Tensor, n_occ: torch.Tensor, tol: floa
 
 class BatchRHF:
     def __init__(self, mols: List[Molecule], schwarz_cutoff: float = 1e-12, device: int = 0,
-                 mixed_fp32_cut: float = 1e-6, n_buckets: int = 4):
+                 mixed_fp32_cut: float = 1e-6, n_buckets: int = 4, builder=None):
         self.mols = list(mols)
         nm = len(self.mols)
-        self.dev = torch.device("cuda", device)
+        self.dev = device if isinstance(device, torch.device) else torch.device("cuda", device)
         dev = self.dev
-        self.fb = BatchFockBuilder(self.mols, schwarz_cutoff=schwarz_cutoff, device=device,
-                                   mixed_fp32_cut=mixed_fp32_cut)
+        self.fb = builder or BatchFockBuilder(self.mols, schwarz_cutoff=schwarz_cutoff, device=device,
+                                              mixed_fp32_cut=mixed_fp32_cut)
         n_bf = [m.n_bf for m in self.mols]
         self.n_bf = n_bf
         order = sorted(range(nm), key=lambda i: n_bf[i])
@@ -147,7 +147,7 @@ class BatchRHF:
             diis_keep: int = 8) -> List[SCFResult]:
         nm = len(self.mols)
         dev = self.dev
-        torch.cuda.synchronize(dev)
+        _sync(dev)
         t0 = time.perf_counter()
         bk = self.buckets
         for b in bk:
@@ -255,7 +255,7 @@ class BatchRHF:
                 b.P[k, :n, :n] = fallback(i).to(dev, torch.float64)
                 b.count[k] = 0
             it += 1
-        torch.cuda.synchronize(dev)
+        _sync(dev)
         secs = time.perf_counter() - t0
         out = []
         for i in range(nm):
