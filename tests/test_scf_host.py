@@ -79,3 +79,22 @@ def test_fallback_replaces_a_guess_that_does_not_converge(oracle_mod, water2):
     r = rhf.run(P0=bad, conv=1e-9, diis_tol=1e-6, fallback=lambda: good, fallback_after=1)
     assert r.fell_back
     assert r.converged and abs(r.energy - ref["E"]) < 1e-9
+
+
+class OracleUBuilder(OracleBuilder):
+    """Adds the unrestricted build (make_u_JK_direct) from the oracle."""
+
+    def make_u_JK_device(self, Pa, Pb, Ja, Jb, Ka, Kb, flags=0):
+        out = self.o.jk_uhf(Pa.numpy(), Pb.numpy())
+        for t, a in zip((Ja, Jb, Ka, Kb), out):
+            t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+
+
+def test_uhf_driver_matches_the_oracle_uhf(oracle_mod):
+    from tonto_b200.molecules import from_angstrom
+    from tonto_b200.scf import UHF
+    oh = from_angstrom([8, 1], np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 0.97]]), "cc-pVDZ", True)
+    ref = oracle_mod.uhf_scf(oh, 5, 4, conv=1e-9, diis_tol=1e-6)
+    u = UHF(oh, multiplicity=2, device=torch.device("cpu"), builder=OracleUBuilder(oracle_mod, oh))
+    r = u.run(conv=1e-9, diis_tol=1e-6)
+    assert r.converged and abs(r.energy - ref["E"]) < 1e-9
