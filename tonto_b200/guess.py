@@ -25,7 +25,7 @@ from typing import List, Tuple
 
 import numpy as np
 
-from .basis import Molecule, n_cart
+from .basis import Molecule
 
 
 # ---------------------------------------------------------------------------
