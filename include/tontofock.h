@@ -32,7 +32,8 @@
  *
  * Errors: every int-returning call returns TF_OK (0) or a negative TF_E* code;
  * tf_error_string() gives a message.  No exception or exit crosses the ABI.
- * Device waits inside the library are bounded and report TF_ETIMEOUT.
+ * The library's kernels never wait on one another (no device-side spin waits);
+ * TF_ETIMEOUT is reserved for a bounded wait and not returned by this version.
  *
  * Threading: one caller thread per context.  Contexts are independent; each is
  * bound to the CUDA device given in tf_options.device.
@@ -72,7 +73,8 @@ typedef struct tf_basis {
   const double* xyz;            /* [n_atom][3], bohr */
   int n_shell;
   const int* shell_atom;        /* [n_shell] atom of each shell */
-  const int* shell_l;           /* [n_shell] angular momentum (0..3 supported) */
+  const int* shell_l;           /* [n_shell] angular momentum (s, p, d: 0..2; higher l is refused
+                                   with TF_EUNSUPPORTED) */
   const int* shell_nprim;       /* [n_shell] primitives per shell */
   const int* shell_first_bf;    /* [n_shell] first basis function (Tonto order) */
   const double* exponents;      /* [sum nprim] primitive exponents, shell after shell */
