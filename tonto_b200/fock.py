@@ -234,12 +234,14 @@ class FockBuilder:
         return J, K
 
     def make_r_JK_device(self, P, J, K, flags: int = TF_JK_FULL, stream=None):
-        """J, K on device (torch CUDA float64 tensors of shape (n_bf, n_bf)); asynchronous
-        on ``stream`` (a torch.cuda.Stream, default: the current stream)."""
+        """J, K on device (torch CUDA float64 tensors of shape (n_bf, n_bf) on the context's
+        GPU), ordered after the earlier work on ``stream`` (a torch.cuda.Stream, default: the
+        current stream) and before its later work; returns when the build has finished."""
         import torch
         for t in (P, J, K):
             if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == self.n_bf ** 2):
                 raise ValueError("device J/K tensors must be contiguous float64 CUDA (n_bf, n_bf)")
+            self._on_device(t)
         s = stream if stream is not None else torch.cuda.current_stream(P.device)
         _check(load_library().tf_build_jk_device(self.h, ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(J.data_ptr()),
                                                  ctypes.c_void_p(K.data_ptr()), int(flags),
@@ -263,18 +265,27 @@ class FockBuilder:
         for t in (Pa, Pb, Ja, Jb, Ka, Kb):
             if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == self.n_bf ** 2):
                 raise ValueError("device tensors must be contiguous float64 CUDA (n_bf, n_bf)")
+            self._on_device(t)
         s = stream if stream is not None else torch.cuda.current_stream(Pa.device)
         ptr = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
         _check(load_library().tf_build_jk_uhf_device(self.h, ptr(Pa), ptr(Pb), ptr(Ja), ptr(Jb), ptr(Ka), ptr(Kb),
                                                      int(flags), ctypes.c_void_p(s.cuda_stream)))
 
     def make_r_Fock_mx(self, P: np.ndarray, H: np.ndarray) -> np.ndarray:
+        """F = H + J - K/2 for the density P and core Hamiltonian H (host arrays):
+        MOLECULE.FOCK:make_r_Fock_mx."""
         n = self.n_bf
         Pf = np.asfortranarray(P, dtype=np.float64)
         Hf = np.asfortranarray(H, dtype=np.float64)
+        if Pf.shape != (n, n) or Hf.shape != (n, n):
+            raise ValueError(f"P and H must be {n}x{n}")
         F = np.empty((n, n), order="F")
         _check(load_library().tf_build_fock(self.h, _dp(Pf), _dp(Hf), _dp(F)))
         return F
+
+    def _on_device(self, t):
+        if t.device.index != self.options.device:
+            raise ValueError(f"tensor on {t.device}, context on cuda:{self.options.device}")
 
     def class_stats(self) -> list:
         """Per-class (la lb|lc ld) figures of the last build."""
@@ -333,7 +344,12 @@ class BatchFockBuilder(FockBuilder):
     def make_r_JK_batched(self, Ps, flags: int = TF_JK_FULL):
         """J, K per molecule from host densities Ps[i] (n_bf_i x n_bf_i)."""
         n = len(self.mols)
+        if len(Ps) != n:
+            raise ValueError(f"{n} densities expected")
         Pf = [np.asfortranarray(P, dtype=np.float64) for P in Ps]
+        for P, nb in zip(Pf, self.n_bf_per_mol):
+            if P.shape != (nb, nb):
+                raise ValueError(f"density of shape {P.shape}, molecule has {nb} functions")
         Js = [np.empty_like(p, order="F") for p in Pf]
         Ks = [np.empty_like(p, order="F") for p in Pf]
         arr = lambda lst: (ctypes.POINTER(ctypes.c_double) * n)(*[_dp(a) for a in lst])  # noqa: E731
@@ -347,6 +363,7 @@ class BatchFockBuilder(FockBuilder):
         for t in (P, J, K):
             if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == tot):
                 raise ValueError("batched device arrays must be contiguous float64 CUDA of the concatenated size")
+            self._on_device(t)
         s = stream if stream is not None else torch.cuda.current_stream(P.device)
         _check(load_library().tf_build_jk_device(self.h, ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(J.data_ptr()),
                                                  ctypes.c_void_p(K.data_ptr()), int(flags),
