@@ -20,7 +20,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -43,9 +42,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-scf", action="store_true", help="skip the time-to-SCF measurement")
-    ap.add_argument("--batch-mols", type=int, default=64,
+    ap.add_argument("--batch-mols", type=int, default=256,
                     help="clusters of the batch time-to-SCF measurement (0: skip; 256: the full batch)")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the oracle build (CPU baseline, parity, FLOP counts)")
     ap.add_argument("--no-alkane", action="store_true", help="skip the C40H82 mixed-precision measurement")
     ap.add_argument("--waters", type=int, default=N_WATER,
                     help="cluster size (default 32: the benchmark workload; smaller sizes for profiling)")
@@ -151,21 +150,43 @@ def core_density_torch(mol, fb, dev):
 
 
 # ---------------------------------------------------------------------------
-# CPU restatement timed on a bounded round-robin sample
+# CPU restatement: one full build, timed, and the checker of the GPU build
 # ---------------------------------------------------------------------------
-def cpu_sample(mol, P_np, target_s: float):
+GPU_FLOP_CATEGORIES = ("pair", "roots", "vrr", "form", "hrr", "digest")
+
+
+def oracle_full_build(mol, P_np):
+    """One full oracle J/K build of the workload on all host cores: its wall time (the
+    CPU baseline), its J and K (the per-element check of the GPU build) and its exact
+    per-class counts of quartets, primitive quartets and FLOPs (the roofline's
+    algorithmic work)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     oracle.build()
     orc = oracle.Oracle(mol, schwarz_cutoff=SCHWARZ)
     cores = os.cpu_count() or 1
-    # calibrate on every 128th bra pair (enough work items to load all cores evenly),
-    # then choose the stride so that one sample takes about target_s
-    stride = 128
-    t = orc.jk_sample(P_np, stride, 0, cores)
-    est_full = t * stride
-    stride = max(1, int(math.floor(est_full / target_s)))
-    return orc, stride, cores
+    orc.counts(reset=True)
+    J, K = orc.jk(P_np, n_threads=cores)
+    t_loop, t_call = orc.last_times()
+    cnt = orc.counts().reshape(625, 2)
+    fl = orc.flops(reset=True).reshape(625, 8)
+    cats = list(oracle.Oracle.FLOP_CATEGORIES)
+    sym = "spdfg"
+    classes = {}
+    for q in range(625):
+        if cnt[q, 0] > 0:
+            l = (q // 125, (q // 25) % 5, (q // 5) % 5, q % 5)
+            name = "(%s%s|%s%s)" % tuple(sym[v] for v in l)
+            classes[name] = {"quartets": float(cnt[q, 0]), "prim_quartets": float(cnt[q, 1]),
+                             "flops": {c: float(fl[q, i]) for i, c in enumerate(cats)}}
+    return {"seconds": t_call, "loop_seconds": t_loop, "cores": cores, "J": J, "K": K, "classes": classes}
+
+
+def gpu_flops(cls: dict) -> float:
+    """Counted FLOPs of the categories the GPU kernels perform per quartet (the
+    positioned ket pairs are made once per geometry and the spherical transform once
+    per build on the GPU, so those categories are left out)."""
+    return sum(cls["flops"][c] for c in GPU_FLOP_CATEGORIES)
 
 
 def time_to_scf(mol, fb, device):
@@ -284,10 +305,33 @@ def time_to_scf_batch(n_mol: int, device: int):
             "speedup": round(t_plain / t_batch, 3)}
 
 
+def config_dict(n_bf: int, world: int) -> dict:
+    """The workload description both arms print (identical for the same N)."""
+    return {"workload": WORKLOAD, "n_bf": n_bf, "schwarz_cutoff": SCHWARZ,
+            "l2": "GPU arm: flushed (256 MB write) between timed builds",
+            "parallelism": f"round-robin bra pairs x{world} + NCCL all-reduce" if world > 1 else "single GPU"}
+
+
+def host_cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args, rank, world):
+    """The reference's CPU J/K build on the host cores: the oracle's restatement of
+    make_r_JK_direct (the Foo/Fortran reference does not build here).  Step k runs the
+    bra shell pairs ab = k mod K (one rank of Tonto's round-robin parallel do over K
+    ranks), so the K timed steps together compute every quartet of one build exactly
+    once; one build's time is the sum of their quartet-loop times plus the fixed
+    per-call work (density maxima, per-thread accumulators, their sum, fold and
+    reflect) once.  ms_per_step is the wall time of one step (1/K of a build)."""
     if rank != 0:
         return
-    import numpy as np
     from tonto_b200.molecules import water_cluster
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -297,23 +341,28 @@ def run_reference(args, rank, world):
     S, T, V = orc.one_electron()
     P, _, _ = oracle.density_from_fock(T + V, oracle.orthogonaliser(S), mol.n_electrons // 2)
     cores = os.cpu_count() or 1
-    t = orc.jk_sample(P, 1024, 0, cores)
-    stride = max(1, int(math.ceil(t * 1024 / 2.0)))      # ~2 s of CPU work per step
+    K = max(1, args.steps)
     for w in range(args.warmup):
-        orc.jk_sample(P, stride, w % stride, cores)
-    times = []
+        orc.jk_sample_times(P, K, w % K, cores)
+    loops, totals = [], []
     for k in range(args.steps):
-        times.append(orc.jk_sample(P, stride, (args.warmup + k) % stride, cores) * stride)
-    mean = sum(times) / len(times)
-    value = 1.0 / mean
+        t_loop, t_call = orc.jk_sample_times(P, K, k, cores)
+        loops.append(t_loop)
+        totals.append(t_call)
+    fixed = statistics.median(t - l for t, l in zip(totals, loops))
+    t_build = sum(loops) + fixed
+    value = 1.0 / t_build
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "schwarz_cutoff": SCHWARZ, "n_bf": mol.n_bf},
-            "cpu_baseline": {"value": value, "unit": "builds/s", "cores": cores, "kind": "port",
-                             "sample": f"Tonto's round-robin outer shell-pair loop, 1/{stride} of the bra pairs "
-                                       f"per step (rank r of {stride}), scaled by {stride}; the reference itself "
-                                       f"does not build here (Foo/Fortran, no gfortran or Java)"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(totals) * 1e3,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(mol.n_bf, world),
+            "build_seconds": t_build,
+            "cpu_baseline": {"value": value, "unit": "builds/s", "cores": cores, "cpu": host_cpu_model(),
+                             "kind": "port",
+                             "sample": f"oracle (C++ restatement of make_r_JK_direct; the Foo/Fortran reference does "
+                                       f"not build here) on {cores} threads: step k = bra pairs ab = k mod {K}, the "
+                                       f"{K} steps together one full build ({t_build:.2f} s: quartet loops "
+                                       f"{sum(loops):.2f} s + fixed per-call work {fixed:.3f} s once)"},
             "e2e": {"value": value, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -421,17 +470,35 @@ def main():
     value = args.steps / (total_ms * 1e-3)
     st = fb.stats()
 
+    # the oracle's full build of the same density: CPU baseline, per-element check of
+    # the GPU J and K, and the exact per-class FLOP counts of the roofline (rank 0)
+    orc_res = None
+    if rank == 0 and not args.no_cpu:
+        orc_res = oracle_full_build(mol, np.asfortranarray(P.cpu().numpy()))
+
     # dominant kernel by device time
-    dom_cls, (dom_ms, dom_flops, dom_n, _, _) = max(cls_acc.items(), key=lambda kv: kv[1][0])
-    achieved = dom_flops / (dom_ms * 1e-3) / 1e12
+    dom_cls, (dom_ms, dom_model, dom_n, _, _) = max(cls_acc.items(), key=lambda kv: kv[1][0])
     tkern, traffic = traffic_from_profile()
     if tkern != dom_cls:
         traffic = None          # the committed capture is of another kernel
-    roofline = {"bound": "fp64_pipe", "kernel": f"k_jk {dom_cls}", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": (achieved / peak) if peak else None,
-                "traffic": traffic, "peak_source": "measured on this GPU: FP64 FMA loop (tf_peak_fma)",
-                "all_classes_achieved": (st_direct["flops"] / (st_direct["eri_ms"] * 1e-3) / 1e12)
-                if st_direct["eri_ms"] else None}
+    roofline = {"bound": "fp64_pipe", "kernel": f"k_jk {dom_cls}", "peak": peak, "unit": "TFLOP/s",
+                "traffic": traffic, "peak_source": "measured on this GPU: FP64 FMA loop (tf_peak_fma), of measured"}
+    if orc_res is not None and dom_cls in orc_res["classes"]:
+        fl = gpu_flops(orc_res["classes"][dom_cls])
+        achieved = fl / (dom_ms * 1e-3) / 1e12
+        all_fl = sum(gpu_flops(v) for v in orc_res["classes"].values())
+        eri_ms = sum(v[0] / v[2] for v in cls_acc.values())
+        roofline.update({"achieved": achieved, "frac": (achieved / peak) if peak else None,
+                         "flops_per_launch": fl, "launch_ms": dom_ms,
+                         "flops_counted_by": "oracle: exact count of the restated reference algorithm over the "
+                                             "same screened quartets (categories " + ", ".join(GPU_FLOP_CATEGORIES) +
+                                             "; ket pair set-up and per-quartet spherical transforms left out: "
+                                             "the GPU does those once per geometry and once per build)",
+                         "all_classes_achieved": all_fl / (eri_ms * 1e-3) / 1e12})
+    else:                       # no oracle run: the library's per-class model
+        achieved = dom_model / (dom_ms * 1e-3) / 1e12
+        roofline.update({"achieved": achieved, "frac": (achieved / peak) if peak else None,
+                         "flops_counted_by": "library model (no oracle run)"})
 
     # e2e through the C ABI with host buffers
     e2e = None
@@ -445,25 +512,35 @@ def main():
         e2e = {"value": args.steps / e2e_s, "unit": "builds/s", "h2d_bytes_per_step": 8 * n * n,
                "d2h_bytes_per_step": 16 * n * n}
 
+    cfg = config_dict(n, world)
+    if args.waters != N_WATER:
+        cfg["workload"] = f"(H2O){args.waters} cc-pVDZ (profiling case)"
     line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.waters == N_WATER else f"(H2O){args.waters} cc-pVDZ (profiling case)",
-                       "n_bf": n, "schwarz_cutoff": SCHWARZ, "l2": "flushed (256 MB write) "
-                       "between timed builds", "parallelism": f"round-robin bra pairs x{world} + NCCL all-reduce"
-                       if world > 1 else "single GPU",
-                       "class_schedule": {"graph_branches": tune["streams"],
-                                          "non_default_kernel_variants": tune["variant_classes"],
-                                          "autotune_ms": [round(v, 3) for v in tune["ms"]]}},
+            "config": cfg,
             "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(st_timed["kernels"]) * args.steps,
             "e2e": e2e,
+            "class_schedule": {"graph_branches": tune["streams"], "non_default_kernel_variants": tune["variant_classes"],
+                               "autotune_ms": [round(v, 3) for v in tune["ms"]]},
             "mixed_precision_builds": mixed,
-            "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"], "flops": st["flops"],
+            "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"],
                       "graph": graph_builds, "direct_build_ms": st_direct["build_ms"],
                       "direct_eri_ms": st_direct["eri_ms"]},
             "classes": {k: {"ms": round(v[0] / v[2], 3), "prim_quartets": v[3], "quartets": v[4],
-                            "tflops": round(v[1] / (v[0] * 1e-3) / 1e12, 3) if v[0] > 0 else None}
+                            "tflops_counted": round(gpu_flops(orc_res["classes"][k]) / (v[0] / v[2] * 1e-3) / 1e12, 3)
+                            if orc_res is not None and k in orc_res["classes"] and v[0] > 0 else None}
                         for k, v in sorted(cls_acc.items(), key=lambda kv: -kv[1][0])}}
+    if orc_res is not None:
+        Jg = J.cpu().numpy().T                      # device arrays hold column-major n x n
+        Kg = K.cpu().numpy().T
+        same_counts = all(k in orc_res["classes"] and orc_res["classes"][k]["quartets"] == v[4]
+                          and orc_res["classes"][k]["prim_quartets"] == v[3] for k, v in cls_acc.items()) and \
+            len(orc_res["classes"]) == len(cls_acc)
+        line["parity_vs_oracle"] = {"max_abs_dJ": float(np.max(np.abs(Jg - orc_res["J"]))),
+                                    "max_abs_dK": float(np.max(np.abs(Kg - orc_res["K"]))),
+                                    "tolerance": 1e-11, "class_counts_equal": bool(same_counts),
+                                    "density": "core-Hamiltonian guess of the GPU run (the same array both sides)"}
 
     if rank == 0 and world == 1 and not args.no_scf:
         line["time_to_scf"] = time_to_scf(mol, fb, local)
@@ -472,13 +549,12 @@ def main():
         if not args.no_alkane:
             line["mixed_precision_alkane"] = mixed_precision_alkane(local)
 
-    if rank == 0 and world == 1 and not args.no_cpu:
-        orc, stride, cores = cpu_sample(mol, np.asfortranarray(P.cpu().numpy()), target_s=15.0)
-        t = orc.jk_sample(np.asfortranarray(P.cpu().numpy()), stride, 0, cores)
-        line["cpu_baseline"] = {"value": 1.0 / (t * stride), "unit": "builds/s", "cores": cores, "kind": "port",
-                                "sample": f"oracle (C++ restatement of make_r_JK_direct), bra shell pairs "
-                                          f"ab = 0 mod {stride} (one rank of Tonto's round-robin parallel do), "
-                                          f"{t:.1f} s, scaled by {stride}"}
+    if orc_res is not None and world == 1:
+        line["cpu_baseline"] = {"value": 1.0 / orc_res["seconds"], "unit": "builds/s", "cores": orc_res["cores"],
+                                "cpu": host_cpu_model(), "kind": "port",
+                                "sample": f"one full build of the workload by the oracle (C++ restatement of "
+                                          f"make_r_JK_direct; the Foo/Fortran reference does not build here) on "
+                                          f"{orc_res['cores']} threads: {orc_res['seconds']:.2f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

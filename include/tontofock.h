@@ -219,7 +219,9 @@ int tf_set_kernel_variant(tf_ctx* ctx, int variant);
 int tf_set_shard(tf_ctx* ctx, int index, int count);
 
 /* J and K from the symmetric density P (host arrays, column-major n_bf x n_bf).
- * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*. */
+ * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*.  A density with a
+ * NaN or infinite element is refused with TF_EINVAL (J and K are then undefined);
+ * the check is made on the device during the build, at no extra pass. */
 int tf_build_jk(tf_ctx* ctx, const double* P, double* J, double* K, int flags);
 
 /* Same, on device arrays (n_bf*n_bf doubles each).  `stream` is the caller's
@@ -231,6 +233,18 @@ int tf_build_jk_device(tf_ctx* ctx, const double* dP, double* dJ, double* dK, in
 
 /* F = Hcore + J - K/2 from P (host arrays).  Replaces make_r_Fock_mx. */
 int tf_build_fock(tf_ctx* ctx, const double* P, const double* Hcore, double* F);
+
+/* The three host builds with the status returned through the last argument instead
+ * of the function value, for Fortran callers that must bind them as PURE
+ * subroutines: make_r_JK_direct / make_r_JK_engine (molecule.fock.foo:1235,1365),
+ * make_r_Fock_mx (:88) and make_u_JK_direct (:2360) are PURE, a PURE procedure may
+ * only call PURE procedures, and a PURE function may not have INTENT(OUT)
+ * arguments, so the binding is a PURE subroutine over these.
+ * *status receives what tf_build_jk / tf_build_fock / tf_build_jk_uhf return. */
+void tf_build_jk_f(tf_ctx* ctx, const double* P, double* J, double* K, int flags, int* status);
+void tf_build_fock_f(tf_ctx* ctx, const double* P, const double* Hcore, double* F, int* status);
+void tf_build_jk_uhf_f(tf_ctx* ctx, const double* Pa, const double* Pb, double* Ja, double* Jb, double* Ka,
+                       double* Kb, int flags, int* status);
 
 /* Many independent molecules in one launch sequence: P[i], J[i], K[i] are host
  * arrays of ctx[i]'s size.  All contexts must be on the same device. */
@@ -247,18 +261,29 @@ int tf_one_electron(tf_ctx* ctx, const double* Z, double* S, double* T, double* 
  * program whose host framework owns the GPU memory, or code running where
  * allocating would be forbidden or would stall the device.  No counterpart in
  * the reference (Tonto allocates freely on the host); this is an addition.
- *   basis: host arrays as for tf_ctx_create; Z: host nuclear charges;
- *   dS, dT, dV: caller-owned DEVICE arrays of n_bf*n_bf doubles (column-major);
- *   stream: cudaStream_t or NULL; the call is asynchronous on that stream.
+ *   basis: host arrays as for tf_ctx_create; Z: host nuclear charges.  They are
+ *          copied before the call returns (through a pageable staging area), so
+ *          the caller may overwrite or free them, pinned or not, on return;
+ *   dS, dT, dV: caller-owned DEVICE arrays of n_bf*n_bf doubles (column-major) on
+ *          the current device (anything else: TF_EINVAL);
+ *   stream: cudaStream_t or NULL; the kernels are asynchronous on that stream.
  * Limits: 256 atoms, 512 shells, 4096 primitives, 512 Cartesian functions
  * (hence n_bf <= 512); larger inputs return TF_EUNSUPPORTED.  All scratch lives
  * in one fixed array of about 6.4 MB in device memory, held by every GPU that
  * loads this library until the process exits.  The first call on a device looks
- * up that array's device address and uploads constant tables; make that first
- * call before any stream capture.  Every call on a device reuses the same array,
- * so calls whose work overlaps on the GPU (different streams, no ordering) race. */
+ * up that array's device address and uploads constant tables (under a lock, so
+ * threads may race to it); make that first call before any stream capture.
+ * Every call on a device reuses the same array, so calls whose work overlaps on
+ * the GPU (different streams, no ordering) race; calls in order on one stream
+ * do not. */
 int tf_one_electron_noalloc(const tf_basis* basis, const double* Z, double* dS, double* dT, double* dV,
                             void* stream);
+
+/* Failure injection for tests: the countdown-th device allocation made after this
+ * call (by any context) fails as an out-of-memory would, so every allocation path's
+ * error return (TF_ENOMEM, context left usable or cleanly destroyed) can be tested
+ * without exhausting a shared GPU.  0 turns it off.  No reference counterpart. */
+int tf_debug_fail_alloc(int countdown);
 
 /* Statistics of the last build on this context. */
 int tf_last_stats(const tf_ctx* ctx, tf_stats* stats);

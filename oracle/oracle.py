@@ -53,6 +53,8 @@ def lib():
         L.oracle_jk_sample.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_long, ctypes.c_int, ctypes.c_long,
                                        ctypes.c_long]
         L.oracle_counts.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+        L.oracle_flops.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+        L.oracle_last_times.argtypes = [ctypes.c_void_p, dp]
         L.oracle_jk_uhf.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, ctypes.c_int]
         L.oracle_spherical_matrix.argtypes = [ctypes.c_int, dp]
         L.oracle_spherical_matrix.restype = ctypes.c_int
@@ -112,13 +114,37 @@ class Oracle:
         return np.ascontiguousarray(J), np.ascontiguousarray(K)
 
     def jk_sample(self, P: np.ndarray, stride: int, offset: int = 0, n_threads: int = 0) -> float:
-        """Time the outer loop over ab = offset, offset+stride, ... (seconds)."""
+        """Time the outer loop over ab = offset, offset+stride, ... (seconds, whole call)."""
         Pf = np.asfortranarray(P, dtype=np.float64)
         J = np.zeros((self.n_bf, self.n_bf), order="F")
         K = np.zeros((self.n_bf, self.n_bf), order="F")
         t = time.perf_counter()
         lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(stride), int(offset))
         return time.perf_counter() - t
+
+    def jk_sample_times(self, P: np.ndarray, stride: int, offset: int = 0, n_threads: int = 0):
+        """(loop seconds, whole-call seconds) of the bra pairs ab = offset, offset+stride, ...:
+        the shell-quartet loop of that share alone, and the call with its fixed work (density
+        maxima, per-thread accumulators, their sum, fold and reflect), which one full build
+        does once whatever the share."""
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        J = np.zeros((self.n_bf, self.n_bf), order="F")
+        K = np.zeros((self.n_bf, self.n_bf), order="F")
+        lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(stride), int(offset))
+        return self.last_times()
+
+    def last_times(self):
+        out = np.zeros(2)
+        lib().oracle_last_times(self.h, _dp(out))
+        return float(out[0]), float(out[1])
+
+    def flops(self, reset: bool = False) -> np.ndarray:
+        """Counted FLOPs of the J/K calls so far, shape (5, 5, 5, 5, 8): per (la lb|lc ld)
+        class, the categories set-up, pair terms, roots, recurrences, (e0|f0) sums,
+        transfers, spherical transform, digestion."""
+        out = np.zeros(625 * 8)
+        lib().oracle_flops(self.h, _dp(out), int(reset))
+        return out.reshape(5, 5, 5, 5, 8)
 
     def jk_shard(self, P: np.ndarray, rank: int, n_ranks: int, n_threads: int = 0):
         """Partial J, K of the bra pairs ab = rank, rank + n_ranks, ... (one rank of
@@ -137,7 +163,11 @@ class Oracle:
         lib().oracle_jk_uhf(self.h, _dp(Pa), _dp(Pb), *[_dp(x) for x in out], int(n_threads))
         return tuple(np.ascontiguousarray(x) for x in out)
 
+    FLOP_CATEGORIES = ("setup", "pair", "roots", "vrr", "form", "hrr", "spherical", "digest")
+
     def counts(self, reset: bool = False) -> np.ndarray:
+        """Contracted and primitive quartets computed so far, shape (5, 5, 5, 5, 2).
+        reset clears these and the FLOP counters."""
         out = np.zeros(625 * 2)
         lib().oracle_counts(self.h, _dp(out), int(reset))
         return out.reshape(5, 5, 5, 5, 2)

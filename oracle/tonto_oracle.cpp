@@ -39,6 +39,7 @@
 #include <vector>
 #include <algorithm>
 #include <array>
+#include <chrono>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -152,9 +153,30 @@ void build_spherical() {
 }
 
 // ---------------------------------------------------------------------------
+// FLOP counter: every floating-point +, -, *, /, sqrt and exp the code below
+// executes for a shell quartet is tallied (one each) by category, per thread;
+// jk_impl files the tally of each quartet under its (la lb|lc ld) class.
+// ---------------------------------------------------------------------------
+enum FlopCat {
+  F_SETUP = 0,   // positioned ket primitive pairs of the quartet (set_cd_new)
+  F_PAIR,        // per primitive quartet: rho, P-Q, x, prefactor (make_esfs_XX)
+  F_ROOTS,       // Rys nodes and weights (get_weights)
+  F_VRR,         // per root: recurrence coefficients, the 2D recurrences, weight
+  F_FORM,        // (e0|f0) sums over roots and primitive quartets (form_esfs)
+  F_HRR,         // horizontal transfers (transfer_cd, transfer_ab)
+  F_SPH,         // Cartesian -> spherical of the integral block (change_to_spherical)
+  F_DIGEST,      // J, K digestion (molecule.fock.foo:1322-1338)
+  F_NCAT
+};
+// (the hot loops count into locals and add here once per call)
+thread_local double tl_flops[F_NCAT];
+inline void add_flops(int cat, double n) { tl_flops[cat] += n; }
+
+// ---------------------------------------------------------------------------
 // Rys nodes (t^2) and weights from the generated tables (rys.foo:89-134 role)
 // ---------------------------------------------------------------------------
-inline void rys_roots(int n, double x, double* u, double* w) {
+// Returns the FLOPs spent.
+inline int rys_roots(int n, double x, double* u, double* w) {
   if (x < tf_rys_xmax[n]) {
     int j = (int)x;
     double s = x - j;
@@ -165,12 +187,14 @@ inline void rys_roots(int n, double x, double* u, double* w) {
       for (int k = TF_RYS_DEG - 1; k >= 0; --k) v = v * s + cf[k];
       if (f < n) u[f] = v; else w[f - n] = v;
     }
+    return 1 + 2 * n * TF_RYS_DEG * 2;
   } else {
     double ix = 1.0 / x, isx = std::sqrt(ix);
     for (int i = 0; i < n; ++i) {
       u[i] = tf_rys_hroot2[tf_rys_hoffset[n] + i] * ix;
       w[i] = tf_rys_hweight[tf_rys_hoffset[n] + i] * isx;
     }
+    return 2 + 2 * n;
   }
 }
 
@@ -242,6 +266,7 @@ void set_side(const Basis& B, const PairData& pr, bool skip, double pair_cutoff,
   s.zeta.clear(); s.zinv.clear(); s.cc.clear(); s.P.clear(); s.PA.clear();
   double AB[3] = {A[0] - Bp[0], A[1] - Bp[1], A[2] - Bp[2]};
   double r2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+  double fl_setup = 8.0;
   int np = (int)pr.zeta.size();
   for (int i = 0; i < np; ++i) {
     if (s.same_center && !skip) {
@@ -253,19 +278,25 @@ void set_side(const Basis& B, const PairData& pr, bool skip, double pair_cutoff,
     double inv = pr.zinv[i];
     double b_r2 = b * r2;
     double prefac = std::exp(-a * b_r2 * inv);
+    fl_setup += 5.0;                          // b r2, -a, * b_r2, * inv, exp
     if (skip && prefac < pair_cutoff) continue;
+    fl_setup += 1.0 + 3.0 * 5.0;              // prefactor; per axis (b B + a A) inv, P - At
     s.zeta.push_back(pr.zeta[i]); s.zinv.push_back(inv); s.cc.push_back(prefac * pr.cc[i]);
     for (int k = 0; k < 3; ++k) {
       double P = (b * Bp[k] + a * A[k]) * inv;
       s.P.push_back(P); s.PA.push_back(P - At[k]);
     }
   }
+  add_flops(F_SETUP, fl_setup);
 }
 
 // ---------------------------------------------------------------------------
 // Instrumented counters (per (l_a l_b | l_c l_d) class, canonical ordering)
 // ---------------------------------------------------------------------------
-struct ClassCount { double quartets = 0, prim_quartets = 0; };
+struct ClassCount {
+  double quartets = 0, prim_quartets = 0;
+  double flops[F_NCAT] = {};
+};
 
 // ---------------------------------------------------------------------------
 // (e0|f0) by Rys quadrature (make_esfs_XX + form_esfs)
@@ -288,8 +319,15 @@ long make_esfs(const Side& ab, const Side& cd, Work& W) {
   W.Iz.assign((size_t)n_sum * d12, 0.0);
   W.u.resize(n_roots); W.w.resize(n_roots);
   int i = 0;
+  // recurrence work of one root, one axis (the loops below, counted once)
+  double vrr_axis = 4.0 + 4.0 * std::max(0, dim1 - 2);
+  for (int f = 0; f + 1 < dim2; ++f)
+    for (int e = 0; e < dim1; ++e) vrr_axis += 1.0 + (f > 0 ? 3.0 : 0.0) + (e > 0 ? 3.0 : 0.0);
+  const double vrr_root = 8.0 + 3.0 * vrr_axis + d12;
+  double fl_pair = 0.0, fl_roots = 0.0;
   for (int k = 0; k < nab; ++k) {
     double ab_cc = ab.cc[k] * TWOPI5ON2, zeta = ab.zeta[k], zinv = ab.zinv[k], half_zinv = 0.5 * zinv;
+    fl_pair += 2.0;
     const double* P = &ab.P[3 * k]; const double* PA = &ab.PA[3 * k];
     for (int j = 0; j < ncd; ++j) {
       double cd_cc = cd.cc[j], eta = cd.zeta[j], einv = cd.zinv[j];
@@ -298,8 +336,9 @@ long make_esfs(const Side& ab, const Side& cd, Work& W) {
       double rho_zinv = rho * zinv, rho_einv = rho * einv, half_einv = 0.5 * einv;
       double QP[3] = {Q[0] - P[0], Q[1] - P[1], Q[2] - P[2]};
       double xx = rho * (QP[0] * QP[0] + QP[1] * QP[1] + QP[2] * QP[2]);
-      rys_roots(n_roots, xx, W.u.data(), W.w.data());
+      fl_roots += rys_roots(n_roots, xx, W.u.data(), W.w.data());
       double scale = ab_cc * cd_cc * std::sqrt(rho);
+      fl_pair += 18.0;                        // rho (3), rho/zeta, rho/eta, 1/(2 eta), Q-P (3), x (6), scale (3)
       for (int n = 0; n < n_roots; ++n, ++i) {
         double t2 = W.u[n];
         double wt = W.w[n] * scale;
@@ -333,6 +372,10 @@ long make_esfs(const Side& ab, const Side& cd, Work& W) {
   const int ff = g_first[cd.l_max], lf = g_first[cd.l_sum + 1];
   const int ne = le - fe, nf = lf - ff;
   W.esfs.assign((size_t)ne * nf, 0.0);
+  add_flops(F_PAIR, fl_pair);
+  add_flops(F_ROOTS, fl_roots);
+  add_flops(F_VRR, (double)n_sum * vrr_root);
+  add_flops(F_FORM, 3.0 * ne * nf * (double)n_sum);
   for (int f = 0; f < nf; ++f) {
     const Comp& cf_ = g_comp[ff + f];
     for (int e = 0; e < ne; ++e) {
@@ -377,6 +420,7 @@ void hrr(int l_hi, int l_lo, const double* R, const double* G, int nrest, std::v
         for (int r = 0; r < nrest; ++r) o[r] = a[r] + R[dir] * b[r];
       }
     }
+    add_flops(F_HRR, 2.0 * nrest * (double)nx_new * ny_new);
     t1.swap(t2);
     ny = ny_new;
   }
@@ -420,6 +464,7 @@ void to_spherical(int la, int lb, int lc, int ld, const std::vector<double>& C, 
   int l4[4] = {la, lb, lc, ld};
   int dims[4] = {ncart(la), ncart(lb), ncart(lc), ncart(ld)};
   S = C;
+  double fl_sph = 0.0;
   for (int idx = 0; idx < 4; ++idx) {
     int l = l4[idx];
     if (l < 2) continue;
@@ -434,6 +479,7 @@ void to_spherical(int la, int lb, int lc, int ld, const std::vector<double>& C, 
         double v = S[(((size_t)d * dims[2] + c) * dims[1] + b) * dims[0] + a];
         if (v == 0.0) continue;
         int i = id[idx];
+        fl_sph += 2.0 * nsph;
         for (int m = 0; m < nsph; ++m) {
           int o[4] = {a, b, c, d}; o[idx] = m;
           tmp[(((size_t)o[3] * nd[2] + o[2]) * nd[1] + o[1]) * nd[0] + o[0]] += U[i * nsph + m] * v;
@@ -443,6 +489,7 @@ void to_spherical(int la, int lb, int lc, int ld, const std::vector<double>& C, 
     S.swap(tmp);
     dims[idx] = nsph;
   }
+  add_flops(F_SPH, fl_sph);
 }
 
 // make_ERI (:433-457): basis-function block, a fastest
@@ -460,6 +507,9 @@ struct Ctx {
   std::vector<double> max_I;
   std::vector<ClassCount> counts;     // 5^4 classes (l <= 4)
   double schwarz_cutoff = 1e-12, pair_cutoff = 1e-6;
+  // wall times of the last jk call: the shell-quartet loop alone, and the whole call
+  // (density maxima, per-thread accumulators, their sum, fold and reflect included)
+  double t_loop = 0.0, t_total = 0.0;
 };
 
 int class_id(int la, int lb, int lc, int ld) { return ((la * 5 + lb) * 5 + lc) * 5 + ld; }
@@ -576,6 +626,8 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
   const Basis& B = C->B;
   const int n = B.n_bf;
   const double cutoff = C->schwarz_cutoff;
+  using clk = std::chrono::steady_clock;
+  const auto t_start = clk::now();
   std::vector<double> Pm;
   max_density(*C, Pscreen, Pm);
   double P_max = 0.0, I_max_all = 0.0;
@@ -592,6 +644,7 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
   std::vector<std::vector<double>> Jt(nt * nd, std::vector<double>((size_t)n * n, 0.0));
   std::vector<std::vector<double>> Kt(nt * nd, std::vector<double>((size_t)n * n, 0.0));
   std::vector<std::vector<ClassCount>> cnt(nt, std::vector<ClassCount>(625));
+  const auto t_loop0 = clk::now();
 #pragma omp parallel num_threads(nt)
   {
 #ifdef _OPENMP
@@ -635,6 +688,7 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
         if (aa == cc && bb == dd) factor *= 0.5;
         bool any_same = ab_same || cd_same || atom_a == atom_c || atom_a == atom_d || atom_b == atom_c ||
                         atom_b == atom_d;
+        for (int q = 0; q < F_NCAT; ++q) tl_flops[q] = 0.0;     // this quartet's tally
         set_side(B, pcd, !any_same, C->pair_cutoff, s_cd);
         const Side& s_ab = any_same ? s_ab_full : s_ab_skip;
         make_eri(B, s_ab, s_cd, W);
@@ -650,6 +704,14 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
         int fc = B.shell_first_bf[cc], fd = B.shell_first_bf[dd];
         int nc = B.nbf_of(pcd.la), ndd = B.nbf_of(pcd.lb);
         const double* I = W.out.data();
+        add_flops(F_DIGEST, 13.0 * nd * (double)na * nb * nc * ndd);   // factor I, six (+= I P) per density
+        {
+          int la = pab.la, lb = pab.lb, lc = pcd.la, ld = pcd.lb;
+          int p1a = std::max(la, lb), p1b = std::min(la, lb), p2a = std::max(lc, ld), p2b = std::min(lc, ld);
+          if (p1a * 5 + p1b < p2a * 5 + p2b) { std::swap(p1a, p2a); std::swap(p1b, p2b); }
+          ClassCount& cf = cnt[tid][class_id(p1a, p1b, p2a, p2b)];
+          for (int q = 0; q < F_NCAT; ++q) cf.flops[q] += tl_flops[q];
+        }
         for (int sp = 0; sp < nd; ++sp) {
           const double* P = Ps[sp];
           double* Jl = Jt[tid * nd + sp].data();
@@ -671,6 +733,7 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
       }
     }
   }
+  const auto t_loop1 = clk::now();
   for (int sp = 0; sp < nd; ++sp) {
     double* J = Js[sp];
     double* K = Ks[sp];
@@ -707,7 +770,10 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
     for (int q = 0; q < 625; ++q) {
       C->counts[q].quartets += cnt[t][q].quartets;
       C->counts[q].prim_quartets += cnt[t][q].prim_quartets;
+      for (int k = 0; k < F_NCAT; ++k) C->counts[q].flops[k] += cnt[t][q].flops[k];
     }
+  C->t_loop = std::chrono::duration<double>(t_loop1 - t_loop0).count();
+  C->t_total = std::chrono::duration<double>(clk::now() - t_start).count();
 }
 
 void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long max_ab_pairs, int n_threads,
@@ -738,6 +804,24 @@ void oracle_counts(OracleCtx* c, double* out, int reset) {
   Ctx* C = reinterpret_cast<Ctx*>(c);
   for (int q = 0; q < 625; ++q) { out[2 * q] = C->counts[q].quartets; out[2 * q + 1] = C->counts[q].prim_quartets; }
   if (reset) C->counts.assign(625, ClassCount());
+}
+
+// Counted FLOPs accumulated over oracle_jk calls: out[class * 8 + category] for the
+// 625 (la lb|lc ld) classes and the eight categories of FlopCat (set-up, pair terms,
+// roots, recurrences, (e0|f0) sums, transfers, spherical transform, digestion).
+void oracle_flops(OracleCtx* c, double* out, int reset) {
+  Ctx* C = reinterpret_cast<Ctx*>(c);
+  for (int q = 0; q < 625; ++q)
+    for (int k = 0; k < F_NCAT; ++k) out[q * F_NCAT + k] = C->counts[q].flops[k];
+  if (reset) C->counts.assign(625, ClassCount());
+}
+
+// Wall times (seconds) of the last J/K call: out[0] the shell-quartet loop, out[1]
+// the whole call.
+void oracle_last_times(OracleCtx* c, double* out) {
+  Ctx* C = reinterpret_cast<Ctx*>(c);
+  out[0] = C->t_loop;
+  out[1] = C->t_total;
 }
 
 // Cartesian-to-spherical matrix for l (ncart(l) x (2l+1), row-major)

@@ -70,4 +70,7 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TONTO_ROOT")
+    if not src:
+        sys.exit("usage: python make_fixtures.py <the root of a Tonto checkout> (or set TONTO_ROOT)")
+    main(src)

@@ -33,4 +33,7 @@ def main(libdir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis_sets")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TONTO_BASIS_DIR")
+    if not src:
+        sys.exit("usage: python extract_basis.py <the basis_sets directory of a Tonto checkout> (or set TONTO_BASIS_DIR)")
+    main(src)

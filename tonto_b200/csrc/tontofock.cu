@@ -30,6 +30,7 @@
 #include <numeric>
 #include <string>
 #include <vector>
+#include <atomic>
 #include <mutex>
 #include <map>
 
@@ -57,6 +58,18 @@ __constant__ double c_U[4][10 * 7];               // Cartesian -> spherical, l =
 
 thread_local std::string g_last_error;
 void set_error(const std::string& s) { g_last_error = s; }
+
+// Allocation-failure injection for the failure tests (tf_debug_fail_alloc): when
+// positive, the countdown-th later device allocation of any context fails as if the
+// device were out of memory.  0: off.
+static std::atomic<int> g_fail_alloc{0};
+static bool inject_alloc_failure() {
+  int v = g_fail_alloc.load();
+  while (v > 0) {
+    if (g_fail_alloc.compare_exchange_weak(v, v - 1)) return v == 1;
+  }
+  return false;
+}
 
 // ---------------------------------------------------------------------------
 // kernels: shell pairs
@@ -205,13 +218,17 @@ __global__ void k_density_to_cart(BatchArgs b, const double* __restrict__ P, con
 }
 
 // max |P(a,b)| over each shell pair block (Tonto basis) and, per molecule, the
-// maximum over all pairs (an upper bound: the high word is rounded up).
+// maximum over all pairs (an upper bound: the high word is rounded up).  A
+// non-finite density element is left out of the maxima and raises *bad; the list
+// passes then write no quartets and the host reports the density as invalid.
 __global__ void k_pmax(BatchArgs b, const double* __restrict__ P, const double* __restrict__ P2,
-                       double* __restrict__ pmax, unsigned long long* __restrict__ pglob) {
+                       double* __restrict__ pmax, unsigned long long* __restrict__ pglob,
+                       unsigned long long* __restrict__ bad) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long total = b.pmax_off[b.n_mol];
   double mx = 0.0;
   int m = 0;
+  bool nonfinite = false;
   if (t < total) {
     m = find_mol(b.pmax_off, b.n_mol, t);
     const MolInfo mi = b.mols[m];
@@ -223,10 +240,13 @@ __global__ void k_pmax(BatchArgs b, const double* __restrict__ P, const double* 
     for (int j = 0; j < nb; ++j)
       for (int i = 0; i < na; ++i) {
         const size_t at = (size_t)(fb + j) * mi.n_bf + fa + i;
-        mx = fmax(mx, fabs(Pm[at] + (Pm2 ? Pm2[at] : 0.0)));
+        const double v = fabs(Pm[at] + (Pm2 ? Pm2[at] : 0.0));
+        if (v <= 1.7976931348623157e308) mx = fmax(mx, v);
+        else nonfinite = true;                           // NaN or infinity
       }
     pmax[t] = mx;
   }
+  if (__any_sync(0xffffffffu, nonfinite) && (threadIdx.x & 31) == 0) atomicOr(bad, 1ull);
   // nonnegative doubles order like their bit patterns; reduce the high words
   // among the lanes of the same molecule, then one atomic per molecule and warp
   const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(mx) >> 32);
@@ -283,6 +303,8 @@ struct ListArgs {
   // captured builds: the list length (written by the scan); a list longer than
   // out_base + out_cap is not written at all (that build is redone), else null
   const long long* list_total;
+  // raised by k_pmax when the density has a non-finite element: no quartets listed
+  const unsigned long long* bad;
 };
 
 // Screening record of a sorted pair position, 16 bytes read in list order (coalesced):
@@ -347,7 +369,7 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
   const int g = a.unit_group[task.x];
   const int i = task.y;
   const int bra = a.sorted[cp.bra_off + i];
-  const int jend = (cp.p1 == cp.p2) ? i + 1 : cp.n_ket;
+  const int jend = (a.bad && *a.bad) ? 0 : ((cp.p1 == cp.p2) ? i + 1 : cp.n_ket);
   const long long coff = a.cand ? a.cand_off[t] : 0;
   const int len = MODE == 2 ? a.task_len[t] : jend;
   double Ib = 0.0, pg = 0.0;
@@ -1145,6 +1167,7 @@ struct DBuf {
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
+    if (inject_alloc_failure()) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
     if (e == cudaSuccess) n = std::max<size_t>(m, 1);
     return e;
@@ -1155,7 +1178,7 @@ struct DBuf {
 // read back after a build; pinned so that a captured graph can copy into them).
 struct PinnedStage {
   long long* goff = nullptr;                 // 3 per group, then the list length
-  unsigned long long* pc = nullptr;          // tf::NQCLS
+  unsigned long long* pc = nullptr;          // tf::NQCLS class counters, then the non-finite-density flag
   size_t n_goff = 0;
   ~PinnedStage() {
     if (goff) cudaFreeHost(goff);
@@ -1163,7 +1186,7 @@ struct PinnedStage {
   }
   cudaError_t reserve(size_t ng3) {
     if (!pc) {
-      cudaError_t e = cudaMallocHost(&pc, tf::NQCLS * sizeof(unsigned long long));
+      cudaError_t e = cudaMallocHost(&pc, (tf::NQCLS + 1) * sizeof(unsigned long long));
       if (e != cudaSuccess) return e;
     }
     if (ng3 <= n_goff && goff) return cudaSuccess;
@@ -1186,6 +1209,7 @@ struct tf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  cudaEvent_t order_ev = nullptr;                        // orders the context stream with a caller's stream
   // molecules (a single-molecule context is a batch of one)
   int n_mol = 0, spherical = 0;
   std::vector<tf::MolInfo> mols;
@@ -1693,13 +1717,17 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
     kernels++;
   }
   TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, c->n_mol * sizeof(unsigned long long), s));
-  k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, dPb, c->d_pmax.p, c->d_pglob.p);
+  // per-class primitive counters and, after them, the non-finite-density flag
+  TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, (NQCLS + 1) * sizeof(unsigned long long), s));
+  k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, dPb, c->d_pmax.p, c->d_pglob.p,
+                                                                             c->d_prim_count.p + NQCLS);
   kernels++;
   la = ListArgs{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
                 c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_srec.p, c->d_pairs.p,  c->d_mols.p,
                 c->d_pmax.p,
                 c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX,
                 c->use_cand ? c->d_cand.p : nullptr, c->d_task_cand_off.p, c->d_task_len.p};
+  la.bad = c->d_prim_count.p + NQCLS;
   const long long thr_list = LIST_THREADS;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   const long long nslots = c->n_tasks * NBUCKET;
@@ -1721,7 +1749,6 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
     TF_CUDA(cudaMemsetAsync(c->d_JcB.p, 0, nc * sizeof(double), s));
     TF_CUDA(cudaMemsetAsync(c->d_KcB.p, 0, nc * sizeof(double), s));
   }
-  TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, NQCLS * sizeof(unsigned long long), s));
   return TF_OK;
 }
 
@@ -1740,8 +1767,8 @@ static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, double* dJb, doub
   const int ng = (int)c->group_cls.size();
   TF_CUDA(cudaMemcpyAsync(c->pin->goff, c->d_group_offsets.p, (3 * ng + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
                           s));
-  TF_CUDA(cudaMemcpyAsync(c->pin->pc, c->d_prim_count.p, NQCLS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                          s));
+  TF_CUDA(cudaMemcpyAsync(c->pin->pc, c->d_prim_count.p, (NQCLS + 1) * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, s));
   return TF_OK;
 }
 
@@ -1807,6 +1834,10 @@ static int finish_stats(tf_ctx* c, int kernels, bool graph) {
   const int ng = (int)c->group_cls.size();
   const long long* goff = c->pin->goff;
   const unsigned long long* pc = c->pin->pc;
+  if (pc[NQCLS]) {                      // k_pmax saw NaN or infinity: nothing was listed
+    set_error("the density has non-finite elements (NaN or infinity)");
+    return TF_EINVAL;
+  }
   float ms_all = 0.f, ms_eri = 0.f;
   TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
   double npq = 0.0, flops = 0.0;
@@ -1879,7 +1910,14 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     size_t tmp_bytes = 0;
     const long long nslots = c->n_tasks * NBUCKET;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
-    TF_CUDA(c->d_scan_tmp.reserve(tmp_bytes));
+    if (tmp_bytes > c->d_scan_tmp.n || !c->d_scan_tmp.p) {
+      drop_graph(c);                     // a captured build holds the scan scratch it was given
+      if (c->d_scan_tmp.reserve(tmp_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("scan scratch does not fit in device memory");
+        return TF_ENOMEM;
+      }
+    }
   }
   // graph path: once a dynamic build has sized the list buffer and set up every
   // launch, later builds with the same arrays replay one captured graph
@@ -1951,6 +1989,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   const long long list_n = one_chunk ? std::max<long long>(chunk_max + chunk_max / 4, c->d_quartets.n) : chunk_max;
   if (c->d_quartets.reserve(list_n) != cudaSuccess) {
     cudaGetLastError();
+    drop_graph(c);                       // a captured build may hold the freed buffer
+    c->graph_cap = 0;
     if (c->d_quartets.reserve(chunk_max) != cudaSuccess) {
       cudaGetLastError();
       set_error("quartet list chunk does not fit in device memory");
@@ -2014,9 +2054,54 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   return finish_stats(c, kernels, false);
 }
 
+// Checks of one molecule's basis description, made before any device call: every
+// array present, shells on existing atoms with l in range and at least one
+// primitive, contiguous first basis functions, finite positions, exponents
+// positive and finite, coefficients finite.
+static int validate_basis(const tf_basis* B) {
+  if (B->n_atom <= 0 || B->n_shell <= 0 || !B->xyz || !B->shell_atom || !B->shell_l || !B->shell_nprim ||
+      !B->shell_first_bf || !B->exponents || !B->coefficients) {
+    set_error("incomplete basis description");
+    return TF_EINVAL;
+  }
+  for (int i = 0; i < 3 * B->n_atom; ++i)
+    if (!std::isfinite(B->xyz[i])) { set_error("non-finite atom position"); return TF_EINVAL; }
+  long long np = 0, nb = 0;
+  for (int s = 0; s < B->n_shell; ++s) {
+    const int l = B->shell_l[s];
+    if (l < 0) { set_error("negative angular momentum"); return TF_EINVAL; }
+    if (l > LMAX_SUPPORTED) { set_error("angular momentum beyond the built kernels"); return TF_EUNSUPPORTED; }
+    if (B->shell_atom[s] < 0 || B->shell_atom[s] >= B->n_atom || B->shell_nprim[s] <= 0) {
+      set_error("bad shell record"); return TF_EINVAL;
+    }
+    if (B->shell_first_bf[s] != nb) { set_error("shell_first_bf not contiguous"); return TF_EINVAL; }
+    for (int k = 0; k < B->shell_nprim[s]; ++k) {
+      const double e = B->exponents[np + k], cf = B->coefficients[np + k];
+      if (!(e > 0.0) || !std::isfinite(e) || !std::isfinite(cf)) {
+        set_error("exponents must be positive and finite, coefficients finite");
+        return TF_EINVAL;
+      }
+    }
+    np += B->shell_nprim[s];
+    nb += (B->is_spherical && l >= 2) ? 2 * l + 1 : ncart(l);
+  }
+  return TF_OK;
+}
+
 static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, tf_ctx** out) {
   if (!bases || !out || n_mol <= 0) { set_error("null argument"); return TF_EINVAL; }
   *out = nullptr;
+  for (int m = 0; m < n_mol; ++m) {
+    const int rc = validate_basis(bases + m);
+    if (rc) return rc;
+    if ((bases[m].is_spherical ? 1 : 0) != (bases[0].is_spherical ? 1 : 0)) {
+      set_error("all molecules of a batch must use the same basis kind"); return TF_EINVAL;
+    }
+  }
+  if (opt && (!(opt->eri_schwarz_cutoff > 0.0) || !(opt->eri_primitive_pair_cutoff >= 0.0) ||
+              !(opt->mixed_fp32_cut >= 0.0) || opt->device < 0)) {
+    set_error("bad options"); return TF_EINVAL;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { set_error("no CUDA device"); return TF_ENODEVICE; }
   tf_ctx* c = new tf_ctx();
@@ -2112,7 +2197,8 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
   };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev2) != cudaSuccess) {
+      cudaEventCreate(&c->ev2) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->order_ev, cudaEventDisableTiming) != cudaSuccess) {
     tf_ctx_destroy(c); set_error("stream/event creation"); return TF_ECUDA;
   }
   TF_TRY(up(c->d_mols, c->mols));
@@ -2136,7 +2222,8 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
   const size_t nb2 = (size_t)c->bmat_off[n_mol], nc2 = (size_t)c->cmat_off[n_mol];
   if (c->d_P.reserve(nb2) || c->d_J.reserve(nb2) || c->d_K.reserve(nb2) || c->d_H.reserve(nb2) ||
       c->d_Pc.reserve(nc2) || c->d_Jc.reserve(nc2) || c->d_Kc.reserve(nc2) ||
-      c->d_pmax.reserve((size_t)c->pmax_off[n_mol]) || c->d_pglob.reserve(n_mol) || c->d_prim_count.reserve(NQCLS)) {
+      c->d_pmax.reserve((size_t)c->pmax_off[n_mol]) || c->d_pglob.reserve(n_mol) ||
+      c->d_prim_count.reserve(NQCLS + 1)) {
     tf_ctx_destroy(c); set_error("device allocation"); return TF_ENOMEM;
   }
   TF_TRY(setup_pairs(c));
@@ -2346,14 +2433,13 @@ int tf_build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int 
   cudaStream_t user = static_cast<cudaStream_t>(stream);
   if (user != c->stream) {
     // order the context stream after the caller's work, and the caller's after ours
-    cudaEvent_t e;
-    TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    TF_CUDA(cudaEventRecord(e, user));
-    TF_CUDA(cudaStreamWaitEvent(c->stream, e, 0));
+    // (one event per context, recorded again each time: a wait takes the state of
+    // the event at the time of the wait call)
+    TF_CUDA(cudaEventRecord(c->order_ev, user));
+    TF_CUDA(cudaStreamWaitEvent(c->stream, c->order_ev, 0));
     rc = build_jk_device(c, dP, dJ, dK, flags);
-    TF_CUDA(cudaEventRecord(e, c->stream));
-    TF_CUDA(cudaStreamWaitEvent(user, e, 0));
-    TF_CUDA(cudaEventDestroy(e));
+    TF_CUDA(cudaEventRecord(c->order_ev, c->stream));
+    TF_CUDA(cudaStreamWaitEvent(user, c->order_ev, 0));
     return rc;
   }
   return build_jk_device(c, dP, dJ, dK, flags);
@@ -2384,14 +2470,11 @@ int tf_build_jk_uhf_device(tf_ctx* c, const double* dPa, const double* dPb, doub
   if (rc) return rc;
   cudaStream_t user = static_cast<cudaStream_t>(stream);   // NULL: the legacy default stream
   if (user != c->stream) {
-    cudaEvent_t e;
-    TF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    TF_CUDA(cudaEventRecord(e, user));
-    TF_CUDA(cudaStreamWaitEvent(c->stream, e, 0));
+    TF_CUDA(cudaEventRecord(c->order_ev, user));
+    TF_CUDA(cudaStreamWaitEvent(c->stream, c->order_ev, 0));
     rc = build_jk_device(c, dPa, dJa, dKa, flags, dPb, dJb, dKb);
-    TF_CUDA(cudaEventRecord(e, c->stream));
-    TF_CUDA(cudaStreamWaitEvent(user, e, 0));
-    TF_CUDA(cudaEventDestroy(e));
+    TF_CUDA(cudaEventRecord(c->order_ev, c->stream));
+    TF_CUDA(cudaStreamWaitEvent(user, c->order_ev, 0));
     return rc;
   }
   return build_jk_device(c, dPa, dJa, dKa, flags, dPb, dJb, dKb);
@@ -2468,6 +2551,28 @@ int tf_build_fock(tf_ctx* c, const double* P, const double* H, double* F) {
   return TF_OK;
 }
 
+void tf_build_jk_f(tf_ctx* c, const double* P, double* J, double* K, int flags, int* status) {
+  const int rc = tf_build_jk(c, P, J, K, flags);
+  if (status) *status = rc;
+}
+
+void tf_build_fock_f(tf_ctx* c, const double* P, const double* H, double* F, int* status) {
+  const int rc = tf_build_fock(c, P, H, F);
+  if (status) *status = rc;
+}
+
+void tf_build_jk_uhf_f(tf_ctx* c, const double* Pa, const double* Pb, double* Ja, double* Jb, double* Ka,
+                       double* Kb, int flags, int* status) {
+  const int rc = tf_build_jk_uhf(c, Pa, Pb, Ja, Jb, Ka, Kb, flags);
+  if (status) *status = rc;
+}
+
+int tf_debug_fail_alloc(int countdown) {
+  if (countdown < 0) { tf::set_error("negative countdown"); return TF_EINVAL; }
+  tf::g_fail_alloc.store(countdown);
+  return TF_OK;
+}
+
 int tf_build_jk_batch(tf_ctx** ctx, int n, const double* const* P, double* const* J, double* const* K, int flags) {
   if (!ctx || n < 0 || (n > 0 && (!P || !J || !K))) return TF_EINVAL;
   for (int i = 0; i < n; ++i) {
@@ -2529,10 +2634,9 @@ constexpr int NOALLOC_MAX_PRIM = 4096;
 constexpr int NOALLOC_MAX_CART = 512;      // also bounds n_bf
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
-struct NoAllocScratch {
-  double S[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
-  double T[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
-  double V[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+// The caller's inputs as the kernels read them: copied into this layout on the host
+// first (a static, pageable array), then sent in one copy into the scratch array.
+struct NoAllocInputs {
   double xyz[3 * NOALLOC_MAX_ATOM];
   double Z[NOALLOC_MAX_ATOM];
   double exps[NOALLOC_MAX_PRIM];
@@ -2540,6 +2644,13 @@ struct NoAllocScratch {
   int shell_atom[NOALLOC_MAX_SHELL];
   int shell_l[NOALLOC_MAX_SHELL];
   int shell_nprim[NOALLOC_MAX_SHELL];
+};
+
+struct NoAllocScratch {
+  double S[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+  double T[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+  double V[NOALLOC_MAX_CART * NOALLOC_MAX_CART];
+  NoAllocInputs in;
   int shell_poff[NOALLOC_MAX_SHELL];
   int shell_cart[NOALLOC_MAX_SHELL];
   int bf_shell[NOALLOC_MAX_CART];
@@ -2550,8 +2661,17 @@ struct NoAllocScratch {
 static __device__ __align__(256) unsigned char tf_noalloc_scratch[sizeof(NoAllocScratch)];
 
 // Device addresses of the array, one per device, looked up on the first call on
-// that device (host code cannot use the symbol's host-side name as an address).
+// that device (host code cannot use the symbol's host-side name as an address);
+// the look-up and the constant-table upload run under this lock.
 static NoAllocScratch* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_noalloc_setup_mutex;
+
+// Host staging of the inputs.  It is ordinary pageable memory, so a copy from it
+// has read it completely when cudaMemcpyAsync returns; the caller's arrays (pinned
+// or not) are therefore free again when the entry point returns.  One staging area
+// for all threads, held under its lock from the fill to the end of the copy call.
+static NoAllocInputs g_noalloc_stage;
+static std::mutex g_noalloc_stage_mutex;
 
 // Derived index tables (first primitive, first Cartesian function per shell,
 // basis function -> shell and position) from shell_l / shell_nprim.
@@ -2559,10 +2679,10 @@ __global__ void k_noalloc_index(int n_shell, int spherical, NoAllocScratch* sc) 
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   int np = 0, nc = 0, nb = 0;
   for (int s = 0; s < n_shell; ++s) {
-    const int l = sc->shell_l[s];
+    const int l = sc->in.shell_l[s];
     sc->shell_poff[s] = np;
     sc->shell_cart[s] = nc;
-    np += sc->shell_nprim[s];
+    np += sc->in.shell_nprim[s];
     nc += ncart(l);
     const int m = (spherical && l >= 2) ? 2 * l + 1 : ncart(l);
     for (int i = 0; i < m; ++i) { sc->bf_shell[nb + i] = s; sc->bf_local[nb + i] = i; }
@@ -2572,6 +2692,7 @@ __global__ void k_noalloc_index(int n_shell, int spherical, NoAllocScratch* sc) 
 
 static int noalloc_setup(int dev, NoAllocScratch** out) {
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) { set_error("device ordinal beyond the no-allocation table"); return TF_EINVAL; }
+  std::lock_guard<std::mutex> lock(g_noalloc_setup_mutex);
   if (!g_noalloc_ptr[dev]) {
     void* ptr = nullptr;
     TF_CUDA(cudaGetSymbolAddress(&ptr, tf_noalloc_scratch));
@@ -2582,6 +2703,13 @@ static int noalloc_setup(int dev, NoAllocScratch** out) {
   }
   *out = g_noalloc_ptr[dev];
   return TF_OK;
+}
+
+// An output array must be device (or managed) memory of the current device.
+static bool device_array_on(const void* p, int dev) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { cudaGetLastError(); return false; }
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == dev;
 }
 
 }  // namespace tf
@@ -2610,6 +2738,7 @@ int tf_one_electron_noalloc(const tf_basis* B, const double* Z, double* dS, doub
     np += B->shell_nprim[s];
     nc += ncart(l);
     nb += (B->is_spherical && l >= 2) ? 2 * l + 1 : ncart(l);
+    if (np > NOALLOC_MAX_PRIM || nc > NOALLOC_MAX_CART) break;
   }
   if (np > NOALLOC_MAX_PRIM || nc > NOALLOC_MAX_CART) {
     set_error("tf_one_electron_noalloc: at most 4096 primitives and 512 Cartesian functions");
@@ -2617,31 +2746,41 @@ int tf_one_electron_noalloc(const tf_basis* B, const double* Z, double* dS, doub
   }
   int dev = 0;
   TF_CUDA(cudaGetDevice(&dev));
+  if (!device_array_on(dS, dev) || !device_array_on(dT, dev) || !device_array_on(dV, dev)) {
+    set_error("tf_one_electron_noalloc: dS, dT, dV must be device memory of the current device");
+    return TF_EINVAL;
+  }
   NoAllocScratch* sc = nullptr;
   int rc = noalloc_setup(dev, &sc);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // stage the inputs in the scratch array (host arrays may be reused after return)
-  TF_CUDA(cudaMemcpyAsync(sc->xyz, B->xyz, 3 * B->n_atom * sizeof(double), cudaMemcpyHostToDevice, s));
-  TF_CUDA(cudaMemcpyAsync(sc->Z, Z, B->n_atom * sizeof(double), cudaMemcpyHostToDevice, s));
-  TF_CUDA(cudaMemcpyAsync(sc->exps, B->exponents, np * sizeof(double), cudaMemcpyHostToDevice, s));
-  TF_CUDA(cudaMemcpyAsync(sc->coefs, B->coefficients, np * sizeof(double), cudaMemcpyHostToDevice, s));
-  TF_CUDA(cudaMemcpyAsync(sc->shell_atom, B->shell_atom, B->n_shell * sizeof(int), cudaMemcpyHostToDevice, s));
-  TF_CUDA(cudaMemcpyAsync(sc->shell_l, B->shell_l, B->n_shell * sizeof(int), cudaMemcpyHostToDevice, s));
-  TF_CUDA(cudaMemcpyAsync(sc->shell_nprim, B->shell_nprim, B->n_shell * sizeof(int), cudaMemcpyHostToDevice, s));
+  {
+    // stage the inputs on the host, then one copy from pageable memory: the caller
+    // may overwrite or free its arrays as soon as this call returns
+    std::lock_guard<std::mutex> lock(g_noalloc_stage_mutex);
+    NoAllocInputs& h = g_noalloc_stage;
+    std::memcpy(h.xyz, B->xyz, 3 * B->n_atom * sizeof(double));
+    std::memcpy(h.Z, Z, B->n_atom * sizeof(double));
+    std::memcpy(h.exps, B->exponents, np * sizeof(double));
+    std::memcpy(h.coefs, B->coefficients, np * sizeof(double));
+    std::memcpy(h.shell_atom, B->shell_atom, B->n_shell * sizeof(int));
+    std::memcpy(h.shell_l, B->shell_l, B->n_shell * sizeof(int));
+    std::memcpy(h.shell_nprim, B->shell_nprim, B->n_shell * sizeof(int));
+    TF_CUDA(cudaMemcpyAsync(&sc->in, &h, sizeof(NoAllocInputs), cudaMemcpyHostToDevice, s));
+  }
   k_noalloc_index<<<1, 1, 0, s>>>(B->n_shell, B->is_spherical ? 1 : 0, sc);
   // every Cartesian element of S, T, V is written by the pair kernel (both
   // triangles of every shell-pair block), so nothing needs clearing first
   const long long npair = (long long)B->n_shell * (B->n_shell + 1) / 2;
   k_one_electron_single<<<(unsigned)((npair + 127) / 128), 128, 0, s>>>(
-      B->n_shell, B->n_atom, sc->xyz, sc->Z, sc->shell_atom, sc->shell_l, sc->shell_nprim, sc->shell_poff,
-      sc->shell_cart, sc->exps, sc->coefs, nc, sc->S, sc->T, sc->V);
+      B->n_shell, B->n_atom, sc->in.xyz, sc->in.Z, sc->in.shell_atom, sc->in.shell_l, sc->in.shell_nprim,
+      sc->shell_poff, sc->shell_cart, sc->in.exps, sc->in.coefs, nc, sc->S, sc->T, sc->V);
   const long long n2 = (long long)nb * nb;
   double* outs[3] = {dS, dT, dV};
   double* ins[3] = {sc->S, sc->T, sc->V};
   for (int k = 0; k < 3; ++k)
     k_cart_to_basis_single<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(nb, nc, ins[k], sc->bf_shell, sc->bf_local,
-                                                                 sc->shell_l, sc->shell_cart,
+                                                                 sc->in.shell_l, sc->shell_cart,
                                                                  B->is_spherical ? 1 : 0, outs[k]);
   TF_CUDA(cudaGetLastError());
   return TF_OK;
@@ -2679,6 +2818,7 @@ void tf_ctx_destroy(tf_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
+  if (c->order_ev) cudaEventDestroy(c->order_ev);
   for (cudaEvent_t e : c->cls_ev) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -112,6 +112,13 @@ def load_library(path: Optional[str] = None):
     L.tf_n_bf.argtypes = [vp]
     L.tf_schwarz.argtypes = [vp, P(d)]
     L.tf_ctx_destroy.argtypes = [vp]
+    L.tf_debug_fail_alloc.argtypes = [i]
+    L.tf_build_jk_f.argtypes = [vp, P(d), P(d), P(d), i, P(i)]
+    L.tf_build_jk_f.restype = None
+    L.tf_build_fock_f.argtypes = [vp, P(d), P(d), P(d), P(i)]
+    L.tf_build_fock_f.restype = None
+    L.tf_build_jk_uhf_f.argtypes = [vp, P(d), P(d), P(d), P(d), P(d), P(d), i, P(i)]
+    L.tf_build_jk_uhf_f.restype = None
     L.tf_error_string.argtypes = [i]
     L.tf_error_string.restype = ctypes.c_char_p
     L.tf_version.restype = ctypes.c_char_p
