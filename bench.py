@@ -478,6 +478,7 @@ def main():
 
     # dominant kernel by device time
     dom_cls, (dom_ms, dom_model, dom_n, _, _) = max(cls_acc.items(), key=lambda kv: kv[1][0])
+    dom_ms, dom_model = dom_ms / dom_n, dom_model / dom_n          # per launch (one build)
     tkern, traffic = traffic_from_profile()
     if tkern != dom_cls:
         traffic = None          # the committed capture is of another kernel

@@ -73,8 +73,8 @@ typedef struct tf_basis {
   const double* xyz;            /* [n_atom][3], bohr */
   int n_shell;
   const int* shell_atom;        /* [n_shell] atom of each shell */
-  const int* shell_l;           /* [n_shell] angular momentum (s, p, d: 0..2; higher l is refused
-                                   with TF_EUNSUPPORTED) */
+  const int* shell_l;           /* [n_shell] angular momentum (s, p, d, f: 0..3; higher l is
+                                   refused with TF_EUNSUPPORTED) */
   const int* shell_nprim;       /* [n_shell] primitives per shell */
   const int* shell_first_bf;    /* [n_shell] first basis function (Tonto order) */
   const double* exponents;      /* [sum nprim] primitive exponents, shell after shell */
@@ -211,12 +211,33 @@ int tf_autotune(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags
  * Results do not depend on it beyond summation order.  No reference counterpart. */
 int tf_set_kernel_variant(tf_ctx* ctx, int variant);
 
-/* Restrict this context's builds to shard `index` of `count`: every count-th bra
- * shell-pair task, as one MPI rank of Tonto's round-robin parallel do
- * (FooToFortran.java:2762-2783, molecule.fock.foo:1274).  The shards' J and K sum
- * to the full J and K (the caller reduces them, e.g. one NCCL all-reduce, as
- * PARALLEL_SYMMETRIC_SUM does at molecule.fock.foo:1355-1357). */
+/* Restrict this context's builds to shard `index` of `count`: the bra shell-pair
+ * tasks tf_plan_shards deals to that shard (by estimated cost; Tonto's MPI ranks
+ * share the bra pairs round-robin, FooToFortran.java:2762-2783,
+ * molecule.fock.foo:1274).  The shards' J and K sum to the full J and K (the caller
+ * reduces them, e.g. one NCCL all-reduce, as PARALLEL_SYMMETRIC_SUM does at
+ * molecule.fock.foo:1355-1357). */
 int tf_set_shard(tf_ctx* ctx, int index, int count);
+
+/* The shard plan of one molecule's build, on the host (no device calls, runs without
+ * a GPU): the bra tasks tf_set_shard deals out, and the shard of each.  A task is a
+ * bra shell pair with the kets of one pair class: every ket of that class when the
+ * bra's class is higher, else the kets at positions up to the bra's own in the class
+ * list (pairs of a class ordered by half-decade I_max band, largest first, then by
+ * pair index).  Together the tasks hold every unordered pair of shell pairs once, as
+ * Tonto's outer loop ab with cd <= ab does (molecule.fock.foo:1274-1286).  Tasks are
+ * dealt largest estimated cost first to the least-loaded shard (the estimate: the
+ * kets passing I_max(ab) I_max(cd) > cutoff at a unit density maximum, times primitive
+ * quartets and a per-class FLOP model); Tonto's parallel do deals them round-robin
+ * (FooToFortran.java:2762-2783), which leaves the shards' work uneven.
+ *   max_I: Schwarz bounds in Tonto pair order ab = a(a+1)/2 + b (tf_schwarz);
+ *   *n_tasks: the number of tasks; the arrays, if not NULL, receive per task the bra's
+ *   Tonto pair index, the ket pair class (l_hi(l_hi+1)/2 + l_lo) and the shard;
+ *   pair_position[n_pairs]: each pair's position in its class list;
+ *   shard_cost[n_shards]: the estimated FLOPs of every shard. */
+int tf_plan_shards(const tf_basis* basis, const double* max_I, double schwarz_cutoff, int n_shards,
+                   long long* n_tasks, int* task_bra, int* task_ket_class, int* task_shard, int* pair_position,
+                   double* shard_cost);
 
 /* J and K from the symmetric density P (host arrays, column-major n_bf x n_bf).
  * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*.  A density with a

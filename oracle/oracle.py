@@ -55,6 +55,7 @@ def lib():
         L.oracle_counts.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.oracle_flops.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.oracle_last_times.argtypes = [ctypes.c_void_p, dp]
+        L.oracle_jk_quartets.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_long, ip, ip, ctypes.c_int]
         L.oracle_jk_uhf.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, ctypes.c_int]
         L.oracle_spherical_matrix.argtypes = [ctypes.c_int, dp]
         L.oracle_spherical_matrix.restype = ctypes.c_int
@@ -153,6 +154,17 @@ class Oracle:
         J = np.zeros((self.n_bf, self.n_bf), order="F")
         K = np.zeros((self.n_bf, self.n_bf), order="F")
         lib().oracle_jk_sample(self.h, _dp(Pf), _dp(J), _dp(K), -1, int(n_threads), int(n_ranks), int(rank))
+        return np.ascontiguousarray(J), np.ascontiguousarray(K)
+
+    def jk_quartets(self, P: np.ndarray, bra: np.ndarray, ket: np.ndarray, n_threads: int = 0):
+        """J, K of the shell quartets (bra[i] | ket[i]) (Tonto pair indices, either order)
+        with make_r_JK_direct's screening, factors, digestion and fold."""
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        bra = np.ascontiguousarray(bra, dtype=np.int32)
+        ket = np.ascontiguousarray(ket, dtype=np.int32)
+        J = np.zeros((self.n_bf, self.n_bf), order="F")
+        K = np.zeros((self.n_bf, self.n_bf), order="F")
+        lib().oracle_jk_quartets(self.h, _dp(Pf), _dp(J), _dp(K), len(bra), _ip(bra), _ip(ket), int(n_threads))
         return np.ascontiguousarray(J), np.ascontiguousarray(K)
 
     def jk_uhf(self, Pa: np.ndarray, Pb: np.ndarray, n_threads: int = 0):

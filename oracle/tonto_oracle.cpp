@@ -616,6 +616,110 @@ void oracle_jk(OracleCtx* c, const double* P, double* J, double* K, long max_ab_
   oracle_jk_sample(c, P, J, K, max_ab_pairs, n_threads, 1, 0);
 }
 
+// One shell quartet (ab|cd) of make_r_JK_direct's loop (molecule.fock.foo:1286-1338):
+// Schwarz_inequality_test (:3454-3495), the coincidence factors, the integrals with
+// the primitive-pair cutoff where no two atoms coincide, and the digestion into the
+// accumulators Jl[sp], Kl[sp] of each density.  ab and cd are Tonto pair indices in
+// either order; sides[0] / sides[1] are the bra's positioned primitive pairs without
+// and with the cutoff.  The quartet's class counts and FLOPs go to cnt.
+static void jk_quartet(const Ctx* C, long ab, long cd, const std::vector<double>& Pm, const Side* const* sides,
+                       Side& s_cd, Work& W, int nd, const double* const* Ps, double* const* Jl, double* const* Kl,
+                       std::vector<ClassCount>& cnt) {
+  const Basis& B = C->B;
+  const int n = B.n_bf;
+  const double cutoff = C->schwarz_cutoff;
+  const PairData& pab = C->pairs[ab];
+  const int aa = pab.a, bb = pab.b;
+  const int atom_a = B.shell_atom[aa], atom_b = B.shell_atom[bb];
+  const bool ab_same = atom_a == atom_b;
+  const PairData& pcd = C->pairs[cd];
+  const int cc = pcd.a, dd = pcd.b;
+  const int atom_c = B.shell_atom[cc], atom_d = B.shell_atom[dd];
+  const bool cd_same = atom_c == atom_d;
+  {
+    const long ac = pair_index(std::max(aa, cc), std::min(aa, cc)), ad = pair_index(std::max(aa, dd), std::min(aa, dd));
+    const long bc = pair_index(std::max(bb, cc), std::min(bb, cc)), bd = pair_index(std::max(bb, dd), std::min(bb, dd));
+    const double pm = std::max({Pm[ab], Pm[cd], Pm[ac], Pm[ad], Pm[bc], Pm[bd]});
+    bool skip;
+    if (pm < SKIP_P) skip = true;
+    else skip = !(pm * C->max_I[ab] * C->max_I[cd] > cutoff);
+    if (skip) return;
+  }
+  double factor = 1.0;
+  if (aa == bb) factor = 0.5;
+  if (cc == dd) factor *= 0.5;
+  if (ab == cd) factor *= 0.5;
+  const bool any_same = ab_same || cd_same || atom_a == atom_c || atom_a == atom_d || atom_b == atom_c ||
+                        atom_b == atom_d;
+  for (int q = 0; q < F_NCAT; ++q) tl_flops[q] = 0.0;     // this quartet's tally
+  set_side(B, pcd, !any_same, C->pair_cutoff, s_cd);
+  const Side& s_ab = any_same ? *sides[0] : *sides[1];
+  make_eri(B, s_ab, s_cd, W);
+  const int fa = B.shell_first_bf[aa], fb = B.shell_first_bf[bb];
+  const int na = B.nbf_of(pab.la), nb = B.nbf_of(pab.lb);
+  const int fc = B.shell_first_bf[cc], fd = B.shell_first_bf[dd];
+  const int nc = B.nbf_of(pcd.la), ndd = B.nbf_of(pcd.lb);
+  const double* I = W.out.data();
+  add_flops(F_DIGEST, 13.0 * nd * (double)na * nb * nc * ndd);   // factor I, six (+= I P) per density
+  {
+    // canonical class id: larger pair class first, each pair larger l first
+    const int la = pab.la, lb = pab.lb, lc = pcd.la, ld = pcd.lb;
+    int p1a = std::max(la, lb), p1b = std::min(la, lb), p2a = std::max(lc, ld), p2b = std::min(lc, ld);
+    if (p1a * 5 + p1b < p2a * 5 + p2b) { std::swap(p1a, p2a); std::swap(p1b, p2b); }
+    ClassCount& cf = cnt[class_id(p1a, p1b, p2a, p2b)];
+    cf.quartets += 1;
+    cf.prim_quartets += (double)s_ab.n() * s_cd.n();
+    for (int q = 0; q < F_NCAT; ++q) cf.flops[q] += tl_flops[q];
+  }
+  for (int sp = 0; sp < nd; ++sp) {
+    const double* P = Ps[sp];
+    double* J = Jl[sp];
+    double* K = Kl[sp];
+    size_t abcd = 0;
+    for (int d = fd; d < fd + ndd; ++d)
+      for (int c2 = fc; c2 < fc + nc; ++c2)
+        for (int b = fb; b < fb + nb; ++b)
+          for (int a = fa; a < fa + na; ++a) {
+            double Iv = factor * I[abcd++];
+            J[(size_t)b * n + a] += Iv * P[(size_t)c2 * n + d];
+            J[(size_t)d * n + c2] += Iv * P[(size_t)a * n + b];
+            K[(size_t)c2 * n + a] += Iv * P[(size_t)b * n + d];
+            K[(size_t)d * n + a] += Iv * P[(size_t)b * n + c2];
+            K[(size_t)c2 * n + b] += Iv * P[(size_t)a * n + d];
+            K[(size_t)d * n + b] += Iv * P[(size_t)a * n + c2];
+          }
+  }
+}
+
+// weight_diagonal_blocks(J, 2), blockwise_symmetric_fold(K), J = 2J and the reflection
+// of the lower triangles (molecule.fock.foo:1351-1361, 4181-4263) on summed J, K.
+static void finish_jk(const Basis& B, double* J, double* K) {
+  const int n = B.n_bf;
+  // weight_diagonal_blocks(J,2); blockwise_symmetric_fold(K); J = 2J; reflect
+  for (int s = 0; s < B.n_shell; ++s) {
+    int f = B.shell_first_bf[s], m = B.nbf_of(B.shell_l[s]);
+    for (int j = f; j < f + m; ++j) for (int i = f; i < f + m; ++i) J[(size_t)j * n + i] *= 2.0;
+  }
+  for (int a = 0; a < B.n_shell; ++a) for (int b = 0; b <= a; ++b) {
+    int fa = B.shell_first_bf[a], na = B.nbf_of(B.shell_l[a]);
+    int fb = B.shell_first_bf[b], nb = B.nbf_of(B.shell_l[b]);
+    if (a == b) {
+      std::vector<double> blk((size_t)na * na);
+      for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i) blk[(size_t)j * na + i] = K[(size_t)(fa + j) * n + fa + i];
+      for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i)
+        K[(size_t)(fa + j) * n + fa + i] = blk[(size_t)j * na + i] + blk[(size_t)i * na + j];
+    } else {
+      for (int j = 0; j < nb; ++j) for (int i = 0; i < na; ++i)
+        K[(size_t)(fb + j) * n + fa + i] += K[(size_t)(fa + i) * n + fb + j];
+    }
+  }
+  for (size_t q = 0; q < (size_t)n * n; ++q) J[q] *= 2.0;
+  for (int i = 0; i < n; ++i) for (int j = 0; j < i; ++j) {
+    J[(size_t)i * n + j] = J[(size_t)j * n + i];
+    K[(size_t)i * n + j] = K[(size_t)j * n + i];
+  }
+}
+
 // J, K of nd densities Ps[0..nd) (nd = 1: make_r_JK_direct, molecule.fock.foo:1235-1363;
 // nd = 2: make_u_JK_direct, molecule.fock.foo:2360-2504, alpha and beta), screened
 // with the maxima of Pscreen.  The outer shell-pair loop is restricted to
@@ -654,9 +758,14 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
 #endif
     Work W;
     Side s_ab_skip, s_ab_full, s_cd;
-    // round-robin over ab, as Tonto's parallel do (FooToFortran.java:2762-2783)
+    // round-robin over ab, as Tonto's parallel do (FooToFortran.java:2762-2783); the
+    // threads take the bra pairs from the last (most kets, cd <= ab) down, so that the
+    // dynamic schedule ends on the cheapest pairs (the sums do not depend on the order
+    // beyond rounding)
+    const long n_mine = ab_offset < nab ? (nab - 1 - ab_offset) / ab_stride + 1 : 0;
 #pragma omp for schedule(dynamic, 1)
-    for (long ab = ab_offset; ab < nab; ab += ab_stride) {
+    for (long it = 0; it < n_mine; ++it) {
+      const long ab = ab_offset + (n_mine - 1 - it) * ab_stride;
       if (C->max_I[ab] * IP_max < cutoff) continue;
       const PairData& pab = C->pairs[ab];
       int aa = pab.a, bb = pab.b;
@@ -664,72 +773,12 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
       bool ab_same = atom_a == atom_b;
       if (!ab_same) set_side(B, pab, true, C->pair_cutoff, s_ab_skip);
       set_side(B, pab, false, C->pair_cutoff, s_ab_full);
-      int fa = B.shell_first_bf[aa], fb = B.shell_first_bf[bb];
-      int na = B.nbf_of(pab.la), nb = B.nbf_of(pab.lb);
       for (long cd = 0; cd <= ab; ++cd) {
         if (C->max_I[ab] * C->max_I[cd] * P_max < cutoff) continue;
-        const PairData& pcd = C->pairs[cd];
-        int cc = pcd.a, dd = pcd.b;
-        int atom_c = B.shell_atom[cc], atom_d = B.shell_atom[dd];
-        bool cd_same = atom_c == atom_d;
-        // Schwarz_inequality_test (:3454-3495)
-        {
-          int k = std::max(bb, cc), l = std::min(bb, cc), m = std::max(bb, dd), nn = std::min(bb, dd);
-          long ac = pair_index(aa, cc), ad = pair_index(aa, dd), bc = pair_index(k, l), bd = pair_index(m, nn);
-          double pm = std::max({Pm[ab], Pm[cd], Pm[ac], Pm[ad], Pm[bc], Pm[bd]});
-          bool skip;
-          if (pm < SKIP_P) skip = true;
-          else skip = !(pm * C->max_I[ab] * C->max_I[cd] > cutoff);
-          if (skip) continue;
-        }
-        double factor = 1.0;
-        if (aa == bb) factor = 0.5;
-        if (cc == dd) factor *= 0.5;
-        if (aa == cc && bb == dd) factor *= 0.5;
-        bool any_same = ab_same || cd_same || atom_a == atom_c || atom_a == atom_d || atom_b == atom_c ||
-                        atom_b == atom_d;
-        for (int q = 0; q < F_NCAT; ++q) tl_flops[q] = 0.0;     // this quartet's tally
-        set_side(B, pcd, !any_same, C->pair_cutoff, s_cd);
-        const Side& s_ab = any_same ? s_ab_full : s_ab_skip;
-        make_eri(B, s_ab, s_cd, W);
-        {
-          int la = pab.la, lb = pab.lb, lc = pcd.la, ld = pcd.lb;
-          // canonical class id: larger pair class first, each pair larger l first
-          int p1a = std::max(la, lb), p1b = std::min(la, lb), p2a = std::max(lc, ld), p2b = std::min(lc, ld);
-          if (p1a * 5 + p1b < p2a * 5 + p2b) { std::swap(p1a, p2a); std::swap(p1b, p2b); }
-          ClassCount& cnt1 = cnt[tid][class_id(p1a, p1b, p2a, p2b)];
-          cnt1.quartets += 1;
-          cnt1.prim_quartets += (double)s_ab.n() * s_cd.n();
-        }
-        int fc = B.shell_first_bf[cc], fd = B.shell_first_bf[dd];
-        int nc = B.nbf_of(pcd.la), ndd = B.nbf_of(pcd.lb);
-        const double* I = W.out.data();
-        add_flops(F_DIGEST, 13.0 * nd * (double)na * nb * nc * ndd);   // factor I, six (+= I P) per density
-        {
-          int la = pab.la, lb = pab.lb, lc = pcd.la, ld = pcd.lb;
-          int p1a = std::max(la, lb), p1b = std::min(la, lb), p2a = std::max(lc, ld), p2b = std::min(lc, ld);
-          if (p1a * 5 + p1b < p2a * 5 + p2b) { std::swap(p1a, p2a); std::swap(p1b, p2b); }
-          ClassCount& cf = cnt[tid][class_id(p1a, p1b, p2a, p2b)];
-          for (int q = 0; q < F_NCAT; ++q) cf.flops[q] += tl_flops[q];
-        }
-        for (int sp = 0; sp < nd; ++sp) {
-          const double* P = Ps[sp];
-          double* Jl = Jt[tid * nd + sp].data();
-          double* Kl = Kt[tid * nd + sp].data();
-          size_t abcd = 0;
-          for (int d = fd; d < fd + ndd; ++d)
-            for (int c2 = fc; c2 < fc + nc; ++c2)
-              for (int b = fb; b < fb + nb; ++b)
-                for (int a = fa; a < fa + na; ++a) {
-                  double Iv = factor * I[abcd++];
-                  Jl[(size_t)b * n + a] += Iv * P[(size_t)c2 * n + d];
-                  Jl[(size_t)d * n + c2] += Iv * P[(size_t)a * n + b];
-                  Kl[(size_t)c2 * n + a] += Iv * P[(size_t)b * n + d];
-                  Kl[(size_t)d * n + a] += Iv * P[(size_t)b * n + c2];
-                  Kl[(size_t)c2 * n + b] += Iv * P[(size_t)a * n + d];
-                  Kl[(size_t)d * n + b] += Iv * P[(size_t)a * n + c2];
-                }
-        }
+        const Side* sides[2] = {&s_ab_full, ab_same ? &s_ab_full : &s_ab_skip};
+        double* Jl[2] = {Jt[tid * nd].data(), nd > 1 ? Jt[tid * nd + 1].data() : nullptr};
+        double* Kl[2] = {Kt[tid * nd].data(), nd > 1 ? Kt[tid * nd + 1].data() : nullptr};
+        jk_quartet(C, ab, cd, Pm, sides, s_cd, W, nd, Ps, Jl, Kl, cnt[tid]);
       }
     }
   }
@@ -742,29 +791,7 @@ static void jk_impl(Ctx* C, const double* Pscreen, int nd, const double* const* 
       for (int t = 0; t < nt; ++t) { sj += Jt[t * nd + sp][q]; sk += Kt[t * nd + sp][q]; }
       J[q] = sj; K[q] = sk;
     }
-    // weight_diagonal_blocks(J,2); blockwise_symmetric_fold(K); J = 2J; reflect
-    for (int s = 0; s < B.n_shell; ++s) {
-      int f = B.shell_first_bf[s], m = B.nbf_of(B.shell_l[s]);
-      for (int j = f; j < f + m; ++j) for (int i = f; i < f + m; ++i) J[(size_t)j * n + i] *= 2.0;
-    }
-    for (int a = 0; a < B.n_shell; ++a) for (int b = 0; b <= a; ++b) {
-      int fa = B.shell_first_bf[a], na = B.nbf_of(B.shell_l[a]);
-      int fb = B.shell_first_bf[b], nb = B.nbf_of(B.shell_l[b]);
-      if (a == b) {
-        std::vector<double> blk((size_t)na * na);
-        for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i) blk[(size_t)j * na + i] = K[(size_t)(fa + j) * n + fa + i];
-        for (int j = 0; j < na; ++j) for (int i = 0; i < na; ++i)
-          K[(size_t)(fa + j) * n + fa + i] = blk[(size_t)j * na + i] + blk[(size_t)i * na + j];
-      } else {
-        for (int j = 0; j < nb; ++j) for (int i = 0; i < na; ++i)
-          K[(size_t)(fb + j) * n + fa + i] += K[(size_t)(fa + i) * n + fb + j];
-      }
-    }
-    for (size_t q = 0; q < (size_t)n * n; ++q) J[q] *= 2.0;
-    for (int i = 0; i < n; ++i) for (int j = 0; j < i; ++j) {
-      J[(size_t)i * n + j] = J[(size_t)j * n + i];
-      K[(size_t)i * n + j] = K[(size_t)j * n + i];
-    }
+    finish_jk(B, J, K);
   }
   for (int t = 0; t < nt; ++t)
     for (int q = 0; q < 625; ++q) {
@@ -782,6 +809,57 @@ void oracle_jk_sample(OracleCtx* c, const double* P, double* J, double* K, long 
   double* Js[1] = {J};
   double* Ks[1] = {K};
   jk_impl(reinterpret_cast<Ctx*>(c), P, 1, Ps, Js, Ks, max_ab_pairs, n_threads, ab_stride, ab_offset);
+}
+
+// J, K of an explicit set of shell quartets: quartet i is (bra[i] | ket[i]), Tonto
+// pair indices in either order, with make_r_JK_direct's screening, factors,
+// digestion and final fold (the same quartet body as jk_impl).  The J, K of
+// disjoint quartet sets sum to those of their union, so the shares of a shard plan
+// sum to the full build when the plan covers every quartet once.
+void oracle_jk_quartets(OracleCtx* c, const double* P, double* J, double* K, long n_quartets, const int* bra,
+                        const int* ket, int n_threads) {
+  Ctx* C = reinterpret_cast<Ctx*>(c);
+  const Basis& B = C->B;
+  const int n = B.n_bf;
+  std::vector<double> Pm;
+  max_density(*C, P, Pm);
+#ifdef _OPENMP
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#else
+  int nt = 1;
+#endif
+  std::vector<std::vector<double>> Jt(nt, std::vector<double>((size_t)n * n, 0.0));
+  std::vector<std::vector<double>> Kt(nt, std::vector<double>((size_t)n * n, 0.0));
+  std::vector<std::vector<ClassCount>> cnt(nt, std::vector<ClassCount>(625));
+  const double* Ps[1] = {P};
+#pragma omp parallel num_threads(nt)
+  {
+#ifdef _OPENMP
+    int tid = omp_get_thread_num();
+#else
+    int tid = 0;
+#endif
+    Work W;
+    Side s_ab_skip, s_ab_full, s_cd;
+#pragma omp for schedule(dynamic, 64)
+    for (long i = 0; i < n_quartets; ++i) {
+      const long ab = bra[i], cd = ket[i];
+      const PairData& pab = C->pairs[ab];
+      const bool ab_same = B.shell_atom[pab.a] == B.shell_atom[pab.b];
+      if (!ab_same) set_side(B, pab, true, C->pair_cutoff, s_ab_skip);
+      set_side(B, pab, false, C->pair_cutoff, s_ab_full);
+      const Side* sides[2] = {&s_ab_full, ab_same ? &s_ab_full : &s_ab_skip};
+      double* Jl[1] = {Jt[tid].data()};
+      double* Kl[1] = {Kt[tid].data()};
+      jk_quartet(C, ab, cd, Pm, sides, s_cd, W, 1, Ps, Jl, Kl, cnt[tid]);
+    }
+  }
+  for (size_t q = 0; q < (size_t)n * n; ++q) {
+    double sj = 0, sk = 0;
+    for (int t = 0; t < nt; ++t) { sj += Jt[t][q]; sk += Kt[t][q]; }
+    J[q] = sj; K[q] = sk;
+  }
+  finish_jk(B, J, K);
 }
 
 // make_u_JK_direct (molecule.fock.foo:2360-2504): screening on the maxima of

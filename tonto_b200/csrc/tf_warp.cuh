@@ -2,7 +2,9 @@
 // for the Schwarz diagonal (ab|ab) of the pair classes above the thread kernels
 // (the (e0|f0) block, up to 31 x 31 for (dd|dd), does not fit one thread's
 // registers; the J/K builds of those classes use the lane-group kernels of
-// tf_group.cuh).  One warp computes one contracted quartet:
+// tf_group.cuh), and for everything with an f shell: its Schwarz bounds and its
+// J/K quartets (k_jk_warp), in a per-warp scratch area of global memory (up to
+// 248 KB for (ff|ff)).  One warp computes one contracted quartet:
 //   * every lane evaluates the Rys nodes/weights of the primitive quartet
 //     (warp-uniform table reads);
 //   * lanes (direction, root) build the 2D recurrence tables in shared memory;
@@ -16,15 +18,39 @@
 
 namespace tf {
 
-constexpr int WL_MAX = 2;                       // highest l in the warp path
-constexpr int WD_MAX = 2 * WL_MAX + 1;          // 2D table edge
-constexpr int WNR_MAX = 2 * WL_MAX + 1;         // roots for (dd|dd)
-constexpr int WNE_MAX = 31;                     // comps of l in [2, 4]
-constexpr int W_NINT_MAX = 1296;                  // 6^4 Cartesian integrals
-// per-warp shared memory (doubles)
-constexpr int W_I2D = 3 * WNR_MAX * WD_MAX * WD_MAX;    // 375
-constexpr int W_BUF = W_NINT_MAX + WNE_MAX * 36;          // two HRR buffers
+constexpr int cmax_w(int a, int b) { return a > b ? a : b; }
+
+constexpr int WL_MAX = 3;                       // highest l in the warp path (f)
+constexpr int WNR_MAX = 2 * WL_MAX + 1;         // roots for (ff|ff)
+
+// Doubles one warp needs for a class of shells up to l = L: the 2D tables (3 axes x
+// roots x D1 x D2), and two buffers each holding the largest of the (e0|f0) block,
+// the ket transfer levels, the compacted [e][cd] block and the bra transfer levels.
+constexpr int w_i2d_need(int L) { return 3 * (2 * L + 1) * (2 * L + 1) * (2 * L + 1); }
+constexpr int w_buf_need(int L) {
+  int m = 0;
+  for (int la = 0; la <= L; ++la)
+    for (int lb = 0; lb <= la; ++lb)
+      for (int lc = 0; lc <= L; ++lc)
+        for (int ld = 0; ld <= lc; ++ld) {
+          const int fe = ncart_upto(la - 1), ne = ncart_upto(la + lb) - fe;
+          const int ff = ncart_upto(lc - 1), nf = ncart_upto(lc + ld) - ff;
+          const int ncd = ncart(lc) * ncart(ld);
+          m = cmax_w(m, ne * nf);
+          for (int k = 0; k < ld; ++k) m = cmax_w(m, ne * (ncart_upto(lc + ld - k - 1) - ff) * ncart(k + 1));
+          m = cmax_w(m, ne * ncd);
+          for (int k = 0; k < lb; ++k) m = cmax_w(m, (ncart_upto(la + lb - k - 1) - fe) * ncart(k + 1) * ncd);
+        }
+  return m;
+}
+// s, p, d (the Schwarz bounds of the d pair classes, in shared memory)
+constexpr int W_I2D = w_i2d_need(2);            // 375
+constexpr int W_BUF = w_buf_need(2);
 constexpr int W_SMEM = W_I2D + 2 * W_BUF;
+// up to f (quartets with an f shell, in global scratch)
+constexpr int WF_I2D = w_i2d_need(3);           // 1029
+constexpr int WF_BUF = w_buf_need(3);
+constexpr int WF_SCRATCH = WF_I2D + 2 * WF_BUF;
 
 struct WarpQuartet {
   int la, lb, lc, ld;
@@ -47,14 +73,15 @@ __constant__ unsigned char c_comp[3][NCOMP_ALL];
 __constant__ unsigned char c_cidx[LCOMP + 1][LCOMP + 1][LCOMP + 1];
 
 // Cartesian (ab|cd) of one quartet into out[((a*nb + b)*nc + c)*nd + d].
-// smem: W_SMEM doubles for this warp.  Returns the number of primitive quartets.
+// sm: this warp's scratch, i2d + 2 buf doubles (W_SMEM for s, p, d in shared memory,
+// WF_SCRATCH up to f).  Returns the number of primitive quartets.
 __device__ int warp_quartet(const WarpQuartet& q, const PrimPair* __restrict__ bp, int nbp,
                             const PrimPair* __restrict__ kp, int nkp, const double* Rab, const double* Rcd,
-                            double* __restrict__ sm, double*& out) {
+                            double* __restrict__ sm, double*& out, int i2d = W_I2D, int buf = W_BUF) {
   const int lane = threadIdx.x & 31;
   double* I2 = sm;                     // [3][nr][d1][d2]
-  double* es = sm + W_I2D;             // esfs [ne][nf]
-  double* tb = es + W_BUF;             // scratch
+  double* es = sm + i2d;               // esfs [ne][nf]
+  double* tb = es + buf;               // scratch
   const int nef = q.ne * q.nf;
   for (int k = lane; k < nef; k += 32) es[k] = 0.0;
   const int tsz = q.d1 * q.d2;
@@ -77,7 +104,9 @@ __device__ int warp_quartet(const WarpQuartet& q, const PrimPair* __restrict__ b
         case 2: { double uu[2], ww[2]; rys_eval<2>(xx, uu, ww); for (int i = 0; i < 2; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
         case 3: { double uu[3], ww[3]; rys_eval<3>(xx, uu, ww); for (int i = 0; i < 3; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
         case 4: { double uu[4], ww[4]; rys_eval<4>(xx, uu, ww); for (int i = 0; i < 4; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
-        default: { double uu[5], ww[5]; rys_eval<5>(xx, uu, ww); for (int i = 0; i < 5; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
+        case 5: { double uu[5], ww[5]; rys_eval<5>(xx, uu, ww); for (int i = 0; i < 5; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
+        case 6: { double uu[6], ww[6]; rys_eval<6>(xx, uu, ww); for (int i = 0; i < 6; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
+        default: { double uu[7], ww[7]; rys_eval<7>(xx, uu, ww); for (int i = 0; i < 7; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
       }
       const double scale = bcc * kcc * (rho * rsqrt_nr(rho));
       const double r_z = eta * inv, r_e = zeta * inv;

@@ -36,7 +36,7 @@
 
 namespace tf {
 
-constexpr int LMAX_SUPPORTED = 2;                 // s, p, d shells in the ERI kernels
+constexpr int LMAX_SUPPORTED = 3;                 // s, p, d, f shells (f: the warp path)
 constexpr int NPAIRCLS = (LMAX_SUPPORTED + 1) * (LMAX_SUPPORTED + 2) / 2;
 constexpr int NQCLS = 625;                        // (la lb lc ld) counter slots, l <= 4
 __host__ __device__ constexpr int pair_class(int lh, int ll) { return lh * (lh + 1) / 2 + ll; }
@@ -274,6 +274,13 @@ struct CPUnit {
   int n_ket, mol;
 };
 
+// Class lists of a context (built on the host, see make_class_lists).
+struct ClassLists {
+  std::vector<int> sorted;                 // pair ids by (molecule, class), then band order
+  std::vector<double> simax, sbmax;        // I_max of each position; largest I_max of its band
+  std::vector<int> cls_n, cls_off;         // [mol * NPAIRCLS + class]
+};
+
 struct ListArgs {
   const int2* tasks;            // (unit, bra position)
   long long t_base;             // tasks [t_base, n_tasks) are processed
@@ -448,6 +455,9 @@ struct JKArgs {
   double* J2;
   double* K2;
   int want;
+  // classes with an f shell (k_jk_warp): per-warp global scratch and its warp count
+  double* wscratch;
+  long long wscratch_warps;
 };
 
 
@@ -701,14 +711,18 @@ __global__ void __launch_bounds__(jk_threads<LA, LB, LC, LD, V>(), 1) k_jk(JKArg
 // ---------------------------------------------------------------------------
 constexpr int WARPS_PER_BLOCK = 2;
 
-// Schwarz bound of any pair class with the warp path (one warp per pair).
+// Schwarz bound of any pair class with the warp path (one warp per pair).  gscr:
+// per-warp scratch of WF_SCRATCH doubles in global memory (pair classes with an f
+// shell), else null (shared memory, W_SMEM doubles per warp).
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int* __restrict__ ids, int n,
                                                                       PairRec* __restrict__ pairs,
                                                                       const PrimPair* __restrict__ prim_full,
-                                                                      int spherical, int la, int lb) {
+                                                                      int spherical, int la, int lb,
+                                                                      double* __restrict__ gscr) {
   extern __shared__ double smem_all[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  double* sm = smem_all + wib * W_SMEM;
+  double* sm = gscr ? gscr + (size_t)(blockIdx.x * WARPS_PER_BLOCK + wib) * WF_SCRATCH : smem_all + wib * W_SMEM;
+  const int i2d = gscr ? WF_I2D : W_I2D, wbuf = gscr ? WF_BUF : W_BUF;
   const WarpQuartet q = wq_make(la, lb, la, lb);
   const int na = ncart(la), nb = ncart(lb);
   const bool sa = spherical && la >= 2, sb = spherical && lb >= 2;
@@ -719,7 +733,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int
     const PairRec pr = pairs[p];
     const double R[3] = {pr.Rx, pr.Ry, pr.Rz};
     double* I = nullptr;
-    warp_quartet(q, prim_full + pr.full_off, pr.n_full, prim_full + pr.full_off, pr.n_full, R, R, sm, I);
+    warp_quartet(q, prim_full + pr.full_off, pr.n_full, prim_full + pr.full_off, pr.n_full, R, R, sm, I, i2d, wbuf);
     double m = 0.0;
     for (int e = lane; e < MA * MB; e += 32) {
       const int ma = e / MB, mb = e % MB;
@@ -747,6 +761,106 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int
     if (lane == 0) pairs[p].imax = sqrt(m);
     __syncwarp();
   }
+}
+
+// ---------------------------------------------------------------------------
+// kernel: J/K of the classes with an f shell, one warp per quartet with runtime
+// angular momenta (the warp path above; shell1quartet.foo's generic make_esfs_XX,
+// transfer_cd/transfer_ab, and the digestion of molecule.fock.foo:1322-1338).
+// gscr: WF_SCRATCH doubles of global memory per warp of the grid.  Used for the
+// FP64 and the FP32 buckets alike (f classes are always evaluated in FP64).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int la, int lb, int lc, int ld,
+                                                                 double* __restrict__ gscr) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const long long gw = (long long)blockIdx.x * WARPS_PER_BLOCK + wib;
+  const long long nwarps = (long long)gridDim.x * WARPS_PER_BLOCK;
+  double* sm = gscr + (size_t)gw * WF_SCRATCH;
+  const WarpQuartet q = wq_make(la, lb, lc, ld);
+  const int2* quartets = a.quartets;
+  long long nq = a.n;
+  resolve_range(a.range, a.base, a.cap, quartets, nq);
+  const int NA = ncart(la), NB = ncart(lb), NC = ncart(lc), ND = ncart(ld), NCD = NC * ND;
+  unsigned long long nprim = 0;
+  for (long long t = gw; t < nq; t += nwarps) {
+    const int2 qd = quartets[t];
+    const PairJK b = load_pair_jk(a.jkrec, a.pairR, qd.x);
+    const PairJK k = load_pair_jk(a.jkrec, a.pairR, qd.y);
+    const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
+                          b.atom_hi == k.atom_lo || b.atom_lo == k.atom_hi || b.atom_lo == k.atom_lo;
+    const PrimPair* bp = any_same ? a.prim_full + b.full_off : a.prim_skip + b.skip_off;
+    const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
+    const int nbp = any_same ? b.n_full : b.n_skip;
+    const int nkp = any_same ? k.n_full : k.n_skip;
+    const double Rab[3] = {b.Rx, b.Ry, b.Rz};
+    const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
+    double* I = nullptr;
+    const int npq = warp_quartet(q, bp, nbp, kp, nkp, Rab, Rcd, sm, I, WF_I2D, WF_BUF);
+    nprim += (unsigned long long)npq;
+    double f = 1.0;
+    if (b.same) f *= 0.5;
+    if (k.same) f *= 0.5;
+    if (qd.x == qd.y) f *= 0.5;
+    const MolInfo mi = a.mols[b.mol];
+    const int n = mi.n_cart;
+    const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
+    auto digest = [&](const double* __restrict__ P, double* __restrict__ Jm, double* __restrict__ Km) {
+      if (a.want & 1) {
+        for (int e = lane; e < NA * NB; e += 32) {             // J(ab) = sum_cd I P(cd)
+          const int ia = e / NB, ib = e - ia * NB;
+          double s = 0.0;
+          for (int c = 0; c < NC; ++c)
+            for (int d = 0; d < ND; ++d) s += I[e * NCD + c * ND + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
+          atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, f * s);
+        }
+        for (int e = lane; e < NCD; e += 32) {                 // J(cd) = sum_ab I P(ab)
+          const int c = e / ND, d = e - c * ND;
+          double s = 0.0;
+          for (int ia = 0; ia < NA; ++ia)
+            for (int ib = 0; ib < NB; ++ib) s += I[(ia * NB + ib) * NCD + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ib);
+          atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+        }
+      }
+      if (a.want & 2) {
+        for (int e = lane; e < NA * NC; e += 32) {             // K(ac) = sum_bd I P(bd)
+          const int ia = e / NC, c = e - ia * NC;
+          double s = 0.0;
+          for (int ib = 0; ib < NB; ++ib)
+            for (int d = 0; d < ND; ++d)
+              s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
+          atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
+        }
+        for (int e = lane; e < NA * ND; e += 32) {             // K(ad) = sum_bc I P(bc)
+          const int ia = e / ND, d = e - ia * ND;
+          double s = 0.0;
+          for (int ib = 0; ib < NB; ++ib)
+            for (int c = 0; c < NC; ++c)
+              s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
+          atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
+        }
+        for (int e = lane; e < NB * NC; e += 32) {             // K(bc) = sum_ad I P(ad)
+          const int ib = e / NC, c = e - ib * NC;
+          double s = 0.0;
+          for (int ia = 0; ia < NA; ++ia)
+            for (int d = 0; d < ND; ++d)
+              s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
+          atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
+        }
+        for (int e = lane; e < NB * ND; e += 32) {             // K(bd) = sum_ac I P(ac)
+          const int ib = e / ND, d = e - ib * ND;
+          double s = 0.0;
+          for (int ia = 0; ia < NA; ++ia)
+            for (int c = 0; c < NC; ++c)
+              s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
+          atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
+        }
+      }
+    };
+    digest(a.P + mi.cmat, a.J + mi.cmat, a.K + mi.cmat);
+    if (a.P2) digest(a.P2 + mi.cmat, a.J2 + mi.cmat, a.K2 + mi.cmat);
+    __syncwarp();                        // the next quartet reuses the scratch
+  }
+  if (lane == 0 && nprim) atomicAdd(a.prim_count + qclass_id(la, lb, lc, ld), nprim);
 }
 
 // ---------------------------------------------------------------------------
@@ -832,9 +946,9 @@ __global__ void k_one_electron(long long n_pairs, const PairRec* __restrict__ pa
   const double* B = xyz + 3 * shell_atom[sb];
   const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
   const double r2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
-  double s_c[36], t_c[36], v_c[36];
+  double s_c[100], t_c[100], v_c[100];     // na x nb, l <= 3
   for (int i = 0; i < na * nb; ++i) { s_c[i] = 0.0; t_c[i] = 0.0; v_c[i] = 0.0; }
-  constexpr int LD = 6;                    // 1D table edge (l <= 2: i <= 3, j <= 4)
+  constexpr int LD = 6;                    // 1D table edge (l <= 3: i <= 4, j <= 5)
   const int nroot = (la + lb) / 2 + 1;
   for (int ia = 0; ia < shell_nprim[sa]; ++ia)
     for (int ib = 0; ib < shell_nprim[sb]; ++ib) {
@@ -883,16 +997,17 @@ __global__ void k_one_electron(long long n_pairs, const PairRec* __restrict__ pa
         const double* C = xyz + 3 * at;
         const double PC[3] = {P[0] - C[0], P[1] - C[1], P[2] - C[2]};
         const double x = z * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
-        double u[3], w[3];
+        double u[4], w[4];
         if (nroot == 1) rys_eval_n<1>(x, u, w);
         else if (nroot == 2) rys_eval_n<2>(x, u, w);
-        else rys_eval_n<3>(x, u, w);
+        else if (nroot == 3) rys_eval_n<3>(x, u, w);
+        else rys_eval_n<4>(x, u, w);
         const double pv = -Z[at] * 2.0 * M_PI / z * Kab;
         for (int r = 0; r < nroot; ++r) {
-          double tab[3][3][3];
+          double tab[3][4][4];
           for (int d = 0; d < 3; ++d) {
             const double c0 = PA[d] - u[r] * PC[d], bb = (1.0 - u[r]) * oo2z;
-            double g[5], h[5][3];
+            double g[7], h[7][4];
             g[0] = 1.0;
             const int L = la + lb;
             if (L >= 1) g[1] = c0;
@@ -973,9 +1088,9 @@ __global__ void k_one_electron_single(int n_shell, int n_atom, const double* __r
   const double* B = xyz + 3 * shell_atom[sb];
   const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
   const double r2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
-  double s_c[36], t_c[36], v_c[36];
+  double s_c[100], t_c[100], v_c[100];     // na x nb, l <= 3
   for (int i = 0; i < na * nb; ++i) { s_c[i] = 0.0; t_c[i] = 0.0; v_c[i] = 0.0; }
-  constexpr int LD = 6;                    // 1D table edge (l <= 2: i <= 3, j <= 4)
+  constexpr int LD = 6;                    // 1D table edge (l <= 3: i <= 4, j <= 5)
   const int nroot = (la + lb) / 2 + 1;
   for (int ia = 0; ia < shell_nprim[sa]; ++ia)
     for (int ib = 0; ib < shell_nprim[sb]; ++ib) {
@@ -1024,16 +1139,17 @@ __global__ void k_one_electron_single(int n_shell, int n_atom, const double* __r
         const double* C = xyz + 3 * at;
         const double PC[3] = {P[0] - C[0], P[1] - C[1], P[2] - C[2]};
         const double x = z * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
-        double u[3], w[3];
+        double u[4], w[4];
         if (nroot == 1) rys_eval_n<1>(x, u, w);
         else if (nroot == 2) rys_eval_n<2>(x, u, w);
-        else rys_eval_n<3>(x, u, w);
+        else if (nroot == 3) rys_eval_n<3>(x, u, w);
+        else rys_eval_n<4>(x, u, w);
         const double pv = -Z[at] * 2.0 * M_PI / z * Kab;
         for (int r = 0; r < nroot; ++r) {
-          double tab[3][3][3];
+          double tab[3][4][4];
           for (int d = 0; d < 3; ++d) {
             const double c0 = PA[d] - u[r] * PC[d], bb = (1.0 - u[r]) * oo2z;
-            double g[5], h[5][3];
+            double g[7], h[7][4];
             g[0] = 1.0;
             const int L = la + lb;
             if (L >= 1) g[1] = c0;
@@ -1224,6 +1340,8 @@ struct tf_ctx {
   std::vector<tf::PairRec> pairs_h;
   std::vector<int> pair_cls;
   std::vector<int> cls_n, cls_off;                       // [mol * NPAIRCLS + class]
+  tf::ClassLists lists;                                  // host copy of the sorted class lists
+  std::vector<double> shard_cost;                        // estimated FLOPs of every shard (tf_set_shard)
   std::vector<tf::CPUnit> units;
   std::vector<int> unit_group, group_task0;
   std::vector<int2> group_cls;                           // (bra class, ket class) of each group
@@ -1239,6 +1357,8 @@ struct tf_ctx {
   tf::DBuf<long long> d_cmat_off, d_bmat_off, d_pmax_off;
   tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax, d_sorted_bmax;
   tf::DBuf<double> d_PcB, d_JcB, d_KcB, d_Pb, d_Jb, d_Kb;  // unrestricted builds (allocated on first use)
+  tf::DBuf<double> d_wscratch;                             // f shells: per-warp scratch of the warp path
+  long long wscratch_warps = 0;
   tf::DBuf<int> d_shell_atom, d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
   tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_schwarz_ids;
   tf::DBuf<tf::PairRec> d_pairs;
@@ -1326,32 +1446,176 @@ __global__ void k_group_offsets(int n_groups, const int* __restrict__ group_task
 static std::mutex g_variant_mutex;
 static std::map<int, std::vector<int>> g_variant_cache;
 
-// Groups (class pairs p1 >= p2) of units (one per molecule having both classes);
-// tasks are (unit, bra position); with sharding this context keeps every
-// shard_count-th task (Tonto's round-robin parallel do).
-static int build_tasks(tf_ctx* c) {
-  drop_graph(c);                       // captured launches hold the old task arrays and grid sizes
-  c->units.clear();
-  c->unit_group.clear();
-  c->group_task0.clear();
-  c->group_cls.clear();
-  std::vector<int2> tasks;
-  long long g_counter = 0;
+// ---------------------------------------------------------------------------
+// host planning, no device calls: shell-pair records, the class lists in I_max
+// bands and the bra tasks with their shard assignment.  Shared by the contexts
+// and by tf_plan_shards.
+// ---------------------------------------------------------------------------
+double class_flops(int la, int lb, int lc, int ld, double nq, double npq);
+
+// Pair records of one molecule (Tonto pair order ab = a(a+1)/2 + b, a >= b), the
+// higher-l shell first; shell arrays global over the context, shells of molecule m
+// at [shell0, shell0 + n_shell).  Primitive-pair offsets continue from *full_tot.
+static void append_pair_records(int m, int shell0, int n_shell, const int* shell_l, const int* shell_atom,
+                                const int* shell_cart, const int* shell_nprim, long long* full_tot,
+                                std::vector<PairRec>& pairs, std::vector<int>& pair_cls) {
+  for (int la = 0; la < n_shell; ++la)
+    for (int lb = 0; lb <= la; ++lb) {
+      const int a = shell0 + la, b = shell0 + lb;
+      PairRec p{};
+      const bool a_hi = shell_l[a] >= shell_l[b];
+      p.sh_hi = a_hi ? a : b;
+      p.sh_lo = a_hi ? b : a;
+      p.atom_hi = shell_atom[p.sh_hi];
+      p.atom_lo = shell_atom[p.sh_lo];
+      p.cart_hi = shell_cart[p.sh_hi];
+      p.cart_lo = shell_cart[p.sh_lo];
+      p.n_full = shell_nprim[a] * shell_nprim[b];
+      p.full_off = (int)*full_tot;
+      p.skip_off = (int)*full_tot;
+      *full_tot += p.n_full;
+      p.mol = m;
+      p.tonto_ab = la * (la + 1) / 2 + lb;
+      pairs.push_back(p);
+      pair_cls.push_back(pair_class(shell_l[p.sh_hi], shell_l[p.sh_lo]));
+    }
+}
+
+// Each (molecule, class) list in I_max bands (half decades, largest first) and by
+// pair id inside a band.  The list kernels stop a bra's ket scan at the first band
+// whose largest I_max fails the screen, and the pair-id order inside a band puts
+// neighbouring shells on neighbouring lanes, so the ERI kernels' pair, primitive,
+// density and Fock accesses of a warp fall on few cache lines.
+
+static void make_class_lists(const std::vector<PairRec>& pairs, const std::vector<int>& pair_cls, int n_mol,
+                             ClassLists& L) {
+  const long long n_pairs = (long long)pairs.size();
+  L.sorted.clear(); L.simax.clear(); L.sbmax.clear();
+  L.cls_n.assign((size_t)n_mol * NPAIRCLS, 0);
+  L.cls_off.assign((size_t)n_mol * NPAIRCLS, 0);
+  std::vector<std::vector<int>> lists((size_t)n_mol * NPAIRCLS);
+  for (long long p = 0; p < n_pairs; ++p) lists[(size_t)pairs[p].mol * NPAIRCLS + pair_cls[p]].push_back((int)p);
+  std::vector<int> band_of(n_pairs);                  // half-decade band of each pair, computed once
+  for (long long p = 0; p < n_pairs; ++p) {
+    const double v = pairs[p].imax;
+    band_of[p] = v > 0.0 ? (int)std::floor(2.0 * std::log10(v)) : -1000000;
+  }
+  L.sorted.reserve(n_pairs);
+  L.simax.reserve(n_pairs);
+  L.sbmax.reserve(n_pairs);
+  for (size_t q = 0; q < lists.size(); ++q) {
+    auto& v = lists[q];
+    std::sort(v.begin(), v.end(), [&](int x, int y) {
+      const int bx = band_of[x], by = band_of[y];
+      return bx != by ? bx > by : x < y;
+    });
+    L.cls_off[q] = (int)L.sorted.size();
+    L.cls_n[q] = (int)v.size();
+    for (size_t i = 0; i < v.size();) {
+      size_t e = i;
+      double bm = 0.0;
+      while (e < v.size() && band_of[v[e]] == band_of[v[i]]) bm = std::max(bm, pairs[v[e++]].imax);
+      for (; i < e; ++i) { L.sorted.push_back(v[i]); L.simax.push_back(pairs[v[i]].imax); L.sbmax.push_back(bm); }
+    }
+  }
+}
+
+// Bra tasks: groups (class pairs p1 >= p2) of units (one per molecule having both
+// classes); a task is (unit, bra position) and covers the kets of class p2 (for
+// p1 == p2 those at positions up to the bra's own).  With n_shards > 1 every task
+// gets an estimated cost and the tasks are dealt to the shards largest first, each
+// to the least-loaded shard (longest-processing-time rule), so that the shards'
+// FLOPs, not their task counts, come out even.  The estimate: the kets of the
+// task's bands that pass the Schwarz bound I_max(bra) I_max(ket) > cutoff at a unit
+// density maximum, times the primitive quartets and the per-class FLOP model.
+struct TaskPlan {
+  std::vector<CPUnit> units;
+  std::vector<int> unit_group;
+  std::vector<int2> group_cls;             // (bra class, ket class) of each group
+  std::vector<int2> tasks;                 // every task, group by group
+  std::vector<int> task_group;
+  std::vector<double> cost;                // estimated FLOPs (n_shards > 1)
+  std::vector<int> shard;                  // shard of each task
+  std::vector<double> shard_cost;
+};
+
+static void make_task_plan(const ClassLists& L, const std::vector<PairRec>& pairs, int n_mol, double cutoff,
+                           int n_shards, TaskPlan& T) {
+  T = TaskPlan{};
   for (int p1 = 0; p1 < NPAIRCLS; ++p1)
     for (int p2 = 0; p2 <= p1; ++p2) {
-      const int g = (int)c->group_cls.size();
-      c->group_cls.push_back(make_int2(p1, p2));
-      c->group_task0.push_back((int)tasks.size());
-      for (int m = 0; m < c->n_mol; ++m) {
-        const int n1 = c->cls_n[m * NPAIRCLS + p1], n2 = c->cls_n[m * NPAIRCLS + p2];
+      const int g = (int)T.group_cls.size();
+      T.group_cls.push_back(make_int2(p1, p2));
+      for (int m = 0; m < n_mol; ++m) {
+        const int n1 = L.cls_n[m * NPAIRCLS + p1], n2 = L.cls_n[m * NPAIRCLS + p2];
         if (n1 == 0 || n2 == 0) continue;
-        const int u = (int)c->units.size();
-        c->units.push_back(CPUnit{p1, p2, c->cls_off[m * NPAIRCLS + p1], c->cls_off[m * NPAIRCLS + p2], n2, m});
-        c->unit_group.push_back(g);
-        for (int i = 0; i < n1; ++i, ++g_counter)
-          if (g_counter % c->shard_count == c->shard_index) tasks.push_back(make_int2(u, i));
+        const int u = (int)T.units.size();
+        T.units.push_back(CPUnit{p1, p2, L.cls_off[m * NPAIRCLS + p1], L.cls_off[m * NPAIRCLS + p2], n2, m});
+        T.unit_group.push_back(g);
+        for (int i = 0; i < n1; ++i) {
+          T.tasks.push_back(make_int2(u, i));
+          T.task_group.push_back(g);
+        }
       }
     }
+  const size_t nt = T.tasks.size();
+  T.shard.assign(nt, 0);
+  T.shard_cost.assign(std::max(1, n_shards), 0.0);
+  if (n_shards <= 1) return;
+  // prefix sums of primitive pairs over the sorted positions
+  std::vector<double> pref(L.sorted.size() + 1, 0.0);
+  for (size_t q = 0; q < L.sorted.size(); ++q) pref[q + 1] = pref[q] + pairs[L.sorted[q]].n_full;
+  T.cost.assign(nt, 0.0);
+  for (size_t t = 0; t < nt; ++t) {
+    const CPUnit& u = T.units[T.tasks[t].x];
+    const int i = T.tasks[t].y;
+    int lh1, ll1, lh2, ll2;
+    lh1 = 0; while ((lh1 + 1) * (lh1 + 2) / 2 <= u.p1) ++lh1; ll1 = u.p1 - lh1 * (lh1 + 1) / 2;
+    lh2 = 0; while ((lh2 + 1) * (lh2 + 2) / 2 <= u.p2) ++lh2; ll2 = u.p2 - lh2 * (lh2 + 1) / 2;
+    const double Ib = L.simax[u.bra_off + i];
+    const int jend = (u.p1 == u.p2) ? i + 1 : u.n_ket;
+    // band maxima are non-increasing along the list: the passing kets are a prefix
+    int lo = 0, hi = jend;
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (Ib * L.sbmax[u.ket_off + mid] > cutoff) lo = mid + 1; else hi = mid;
+    }
+    const double nprim_kets = pref[u.ket_off + lo] - pref[u.ket_off];
+    const double nb = pairs[L.sorted[u.bra_off + i]].n_full;
+    T.cost[t] = class_flops(lh1, ll1, lh2, ll2, (double)lo, nb * nprim_kets) + 1.0;
+  }
+  std::vector<size_t> order(nt);
+  for (size_t t = 0; t < nt; ++t) order[t] = t;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return T.cost[x] > T.cost[y]; });
+  for (size_t t : order) {
+    int best = 0;
+    for (int r = 1; r < n_shards; ++r)
+      if (T.shard_cost[r] < T.shard_cost[best]) best = r;
+    T.shard[t] = best;
+    T.shard_cost[best] += T.cost[t];
+  }
+}
+
+// Groups (class pairs p1 >= p2) of units (one per molecule having both classes);
+// tasks are (unit, bra position); with sharding this context keeps the tasks that
+// make_task_plan deals to its shard (Tonto's parallel do shares the bra pairs
+// round-robin, molecule.fock.foo:1274; here they are shared by estimated cost).
+static int build_tasks(tf_ctx* c) {
+  drop_graph(c);                       // captured launches hold the old task arrays and grid sizes
+  TaskPlan T;
+  make_task_plan(c->lists, c->pairs_h, c->n_mol, c->opt.eri_schwarz_cutoff, c->shard_count, T);
+  c->units = T.units;
+  c->unit_group = T.unit_group;
+  c->group_cls = T.group_cls;
+  c->group_task0.clear();
+  c->shard_cost = T.shard_cost;
+  std::vector<int2> tasks;
+  size_t t = 0;
+  for (int g = 0; g < (int)c->group_cls.size(); ++g) {
+    c->group_task0.push_back((int)tasks.size());
+    for (; t < T.tasks.size() && T.task_group[t] == g; ++t)
+      if (T.shard[t] == c->shard_index) tasks.push_back(T.tasks[t]);
+  }
   c->group_task0.push_back((int)tasks.size());
   c->n_tasks = (long long)tasks.size();
   c->cls_variant.assign(c->group_cls.size(), 0);
@@ -1417,26 +1681,8 @@ static int setup_pairs(tf_ctx* c) {
   for (int m = 0; m < c->n_mol; ++m) {
     const MolInfo& mi = c->mols[m];
     c->mol_pair0[m] = (long long)c->pairs_h.size();
-    for (int la = 0; la < mi.n_shell; ++la)
-      for (int lb = 0; lb <= la; ++lb) {
-        const int a = mi.shell0 + la, b = mi.shell0 + lb;
-        PairRec p{};
-        const bool a_hi = c->shell_l[a] >= c->shell_l[b];
-        p.sh_hi = a_hi ? a : b;
-        p.sh_lo = a_hi ? b : a;
-        p.atom_hi = c->shell_atom[p.sh_hi];
-        p.atom_lo = c->shell_atom[p.sh_lo];
-        p.cart_hi = c->shell_cart[p.sh_hi];
-        p.cart_lo = c->shell_cart[p.sh_lo];
-        p.n_full = c->shell_nprim[a] * c->shell_nprim[b];
-        p.full_off = (int)full_tot;
-        p.skip_off = (int)full_tot;
-        full_tot += p.n_full;
-        p.mol = m;
-        p.tonto_ab = la * (la + 1) / 2 + lb;
-        c->pairs_h.push_back(p);
-        c->pair_cls.push_back(pair_class(c->shell_l[p.sh_hi], c->shell_l[p.sh_lo]));
-      }
+    append_pair_records(m, mi.shell0, mi.n_shell, c->shell_l.data(), c->shell_atom.data(), c->shell_cart.data(),
+                        c->shell_nprim.data(), &full_tot, c->pairs_h, c->pair_cls);
   }
   c->mol_pair0[c->n_mol] = (long long)c->pairs_h.size();
   c->n_pairs = (long long)c->pairs_h.size();
@@ -1481,8 +1727,26 @@ static int setup_pairs(tf_ctx* c) {
       if (nk > 0)
         k_schwarz_warp<<<std::min(4096, (nk + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK), 32 * WARPS_PER_BLOCK,
                          WARPS_PER_BLOCK * W_SMEM * sizeof(double), c->stream>>>(
-            c->d_schwarz_ids.p + cls_start[k], nk, c->d_pairs.p, c->d_prim_full.p, c->spherical, lh, ll);
+            c->d_schwarz_ids.p + cls_start[k], nk, c->d_pairs.p, c->d_prim_full.p, c->spherical, lh, ll, nullptr);
     }
+  // pair classes with an f shell: the warp path in global scratch, which the f-class
+  // J/K kernels use too (two blocks of WARPS_PER_BLOCK warps per SM)
+  if (cls_start[NPAIRCLS] > cls_start[pair_class(3, 0)]) {
+    int dev = 0, nsm = 148;
+    TF_CUDA(cudaGetDevice(&dev));
+    TF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const long long warps = (long long)nsm * 2 * WARPS_PER_BLOCK;
+    TF_CUDA(c->d_wscratch.reserve((size_t)warps * WF_SCRATCH));
+    c->wscratch_warps = warps;
+    for (int ll = 0; ll <= 3; ++ll) {
+      const int k = pair_class(3, ll);
+      const int nk = cls_start[k + 1] - cls_start[k];
+      if (nk > 0)
+        k_schwarz_warp<<<(unsigned)std::min<long long>(warps / WARPS_PER_BLOCK, (nk + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK),
+                         32 * WARPS_PER_BLOCK, 0, c->stream>>>(c->d_schwarz_ids.p + cls_start[k], nk, c->d_pairs.p,
+                                                              c->d_prim_full.p, c->spherical, 3, ll, c->d_wscratch.p);
+    }
+  }
   TF_CUDA(cudaGetLastError());
   TF_CUDA(cudaMemcpyAsync(c->pairs_h.data(), c->d_pairs.p, c->n_pairs * sizeof(PairRec), cudaMemcpyDeviceToHost,
                           c->stream));
@@ -1492,42 +1756,12 @@ static int setup_pairs(tf_ctx* c) {
     const PairRec& pr = c->pairs_h[p];
     c->max_I_tonto[c->mol_pair0[pr.mol] + pr.tonto_ab] = pr.imax;
   }
-  // Order each (molecule, class) list by I_max band (half decades, largest first)
-  // and by pair id inside a band.  The list kernels stop a bra's ket scan at the
-  // first band whose largest I_max fails the screen, and the pair-id order inside a
-  // band puts neighbouring shells on neighbouring lanes, so the ERI kernels' pair,
-  // primitive, density and Fock accesses of a warp fall on few cache lines.
-  std::vector<int> sorted;
-  std::vector<double> simax, sbmax;
-  c->cls_n.assign((size_t)c->n_mol * NPAIRCLS, 0);
-  c->cls_off.assign((size_t)c->n_mol * NPAIRCLS, 0);
-  std::vector<std::vector<int>> lists((size_t)c->n_mol * NPAIRCLS);
-  for (long long p = 0; p < c->n_pairs; ++p)
-    lists[(size_t)c->pairs_h[p].mol * NPAIRCLS + c->pair_cls[p]].push_back((int)p);
-  std::vector<int> band_of(c->n_pairs);               // half-decade band of each pair, computed once
-  for (long long p = 0; p < c->n_pairs; ++p) {
-    const double v = c->pairs_h[p].imax;
-    band_of[p] = v > 0.0 ? (int)std::floor(2.0 * std::log10(v)) : -1000000;
-  }
-  auto band = [&](int p) { return band_of[p]; };
-  sorted.reserve(c->n_pairs);
-  simax.reserve(c->n_pairs);
-  sbmax.reserve(c->n_pairs);
-  for (size_t q = 0; q < lists.size(); ++q) {
-    auto& v = lists[q];
-    std::sort(v.begin(), v.end(), [&](int x, int y) {
-      const int bx = band_of[x], by = band_of[y];
-      return bx != by ? bx > by : x < y;
-    });
-    c->cls_off[q] = (int)sorted.size();
-    c->cls_n[q] = (int)v.size();
-    for (size_t i = 0; i < v.size();) {
-      size_t e = i;
-      double bm = 0.0;
-      while (e < v.size() && band(v[e]) == band(v[i])) bm = std::max(bm, c->pairs_h[v[e++]].imax);
-      for (; i < e; ++i) { sorted.push_back(v[i]); simax.push_back(c->pairs_h[v[i]].imax); sbmax.push_back(bm); }
-    }
-  }
+  make_class_lists(c->pairs_h, c->pair_cls, c->n_mol, c->lists);
+  c->cls_n = c->lists.cls_n;
+  c->cls_off = c->lists.cls_off;
+  const std::vector<int>& sorted = c->lists.sorted;
+  const std::vector<double>& simax = c->lists.simax;
+  const std::vector<double>& sbmax = c->lists.sbmax;
   // packed pair records of the ERI kernels (load_pair_jk)
   {
     std::vector<int4> jr(2 * c->n_pairs);
@@ -1659,9 +1893,21 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   return TF_OK;
 }
 
+// Classes with an f shell: one warp per quartet (k_jk_warp), a persistent grid of
+// as many warps as the scratch holds.
+static int launch_warp_jk(const JKArgs& a, cudaStream_t s, int la, int lb, int lc, int ld) {
+  if (a.n <= 0 && !a.range) return TF_OK;
+  if (!a.wscratch || a.wscratch_warps < WARPS_PER_BLOCK) { set_error("no scratch for the f-shell kernel"); return TF_ESTATE; }
+  const long long full = a.wscratch_warps / WARPS_PER_BLOCK;
+  const long long blocks = a.range ? full : std::min<long long>((a.n + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK, full);
+  k_jk_warp<<<(unsigned)blocks, 32 * WARPS_PER_BLOCK, 0, s>>>(a, la, lb, lc, ld, a.wscratch);
+  return TF_OK;
+}
+
 // fp32: evaluate the 2D recurrences and (e0|f0) sums in FP32 (thread-per-quartet
 // classes); roots, weights, transfers and the Fock accumulation stay FP64.
 static int dispatch_jk(int la, int lb, int lc, int ld, const JKArgs& a, cudaStream_t s, bool fp32, int variant = 0) {
+  if (la > 2 || lb > 2 || lc > 2 || ld > 2) return launch_warp_jk(a, s, la, lb, lc, ld);
   const int key = ((la * 3 + lb) * 3 + lc) * 3 + ld;
   switch (key) {
 #define TF_CASE(A, B, C, D) \
@@ -1802,6 +2048,7 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
     for (int i = 0; i + 1 < ns; ++i) TF_CUDA(cudaStreamWaitEvent(c->side[i], c->fork_ev, 0));
   }
   for (int g = 0; g < ng; ++g) {
+    if (c->group_task0[g + 1] == c->group_task0[g]) continue;   // no molecule has this class pair
     int l1h, l1l, l2h, l2l;
     class_l(c->group_cls[g].x, l1h, l1l);
     class_l(c->group_cls[g].y, l2h, l2l);
@@ -1810,6 +2057,8 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
     JKArgs a{c->d_quartets.p, 0, c->d_pairs.p, c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p,
              c->d_Kc.p, c->d_mols.p, c->d_prim_count.p, c->d_group_offsets.p + 3 * g, 0, c->graph_cap,
              c->d_jkrec.p, c->d_pairR.p, nullptr, nullptr, nullptr, want};
+    a.wscratch = c->d_wscratch.p;
+    a.wscratch_warps = c->wscratch_warps;
     JKArgs a32 = a;
     a32.range = c->d_group_offsets.p + 3 * g + 1;
     rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false, c->cls_variant[g]);
@@ -2030,6 +2279,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
                c->d_prim_full.p, c->d_prim_skip.p, c->d_Pc.p, c->d_Jc.p, c->d_Kc.p, c->d_mols.p,
                c->d_prim_count.p, nullptr, 0, LLONG_MAX, c->d_jkrec.p, c->d_pairR.p,
                dPb ? c->d_PcB.p : nullptr, dPb ? c->d_JcB.p : nullptr, dPb ? c->d_KcB.p : nullptr, want};
+      a.wscratch = c->d_wscratch.p;
+      a.wscratch_warps = c->wscratch_warps;
       JKArgs a32 = a;
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
       a32.n = goff[3 * g + 2] - goff[3 * g + 1];
@@ -2135,7 +2386,7 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
     int np = 0, nc = 0, nb = 0;
     for (int s = 0; s < B->n_shell; ++s) {
       const int l = B->shell_l[s];
-      if (l < 0 || l > LMAX_SUPPORTED) { delete c; set_error("angular momentum beyond d not built"); return TF_EUNSUPPORTED; }
+      if (l < 0 || l > LMAX_SUPPORTED) { delete c; set_error("angular momentum beyond the built kernels"); return TF_EUNSUPPORTED; }
       if (B->shell_atom[s] < 0 || B->shell_atom[s] >= B->n_atom || B->shell_nprim[s] <= 0) {
         delete c; set_error("bad shell record"); return TF_EINVAL;
       }
@@ -2421,6 +2672,42 @@ int tf_set_shard(tf_ctx* c, int index, int count) {
   c->shard_index = index;
   c->shard_count = count;
   return c->geometry_ready ? build_tasks(c) : TF_OK;
+}
+
+int tf_plan_shards(const tf_basis* basis, const double* max_I, double schwarz_cutoff, int n_shards,
+                   long long* n_tasks, int* task_bra, int* task_ket_class, int* task_shard, int* pair_position,
+                   double* shard_cost) {
+  using namespace tf;
+  if (!basis || !max_I || !n_tasks || n_shards < 1 || !(schwarz_cutoff > 0.0)) {
+    set_error("bad argument"); return TF_EINVAL;
+  }
+  int rc = validate_basis(basis);
+  if (rc) return rc;
+  std::vector<int> shell_cart(basis->n_shell);
+  for (int s = 0, nc = 0; s < basis->n_shell; ++s) { shell_cart[s] = nc; nc += ncart(basis->shell_l[s]); }
+  std::vector<PairRec> pairs;
+  std::vector<int> pcls;
+  long long full_tot = 0;
+  append_pair_records(0, 0, basis->n_shell, basis->shell_l, basis->shell_atom, shell_cart.data(), basis->shell_nprim,
+                      &full_tot, pairs, pcls);
+  for (PairRec& pr : pairs) pr.imax = max_I[pr.tonto_ab];
+  ClassLists L;
+  make_class_lists(pairs, pcls, 1, L);
+  TaskPlan T;
+  make_task_plan(L, pairs, 1, schwarz_cutoff, n_shards, T);
+  *n_tasks = (long long)T.tasks.size();
+  for (size_t t = 0; t < T.tasks.size(); ++t) {
+    const CPUnit& u = T.units[T.tasks[t].x];
+    if (task_bra) task_bra[t] = pairs[L.sorted[u.bra_off + T.tasks[t].y]].tonto_ab;
+    if (task_ket_class) task_ket_class[t] = u.p2;
+    if (task_shard) task_shard[t] = T.shard[t];
+  }
+  if (pair_position)
+    for (int q = 0; q < NPAIRCLS; ++q)
+      for (int i = 0; i < L.cls_n[q]; ++i) pair_position[pairs[L.sorted[L.cls_off[q] + i]].tonto_ab] = i;
+  if (shard_cost)
+    for (int r = 0; r < n_shards; ++r) shard_cost[r] = T.shard_cost[r];
+  return TF_OK;
 }
 
 int tf_build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, void* stream) {
