@@ -55,6 +55,8 @@ def lib():
         L.oracle_counts.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.oracle_flops.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.oracle_last_times.argtypes = [ctypes.c_void_p, dp]
+        L.oracle_fp32_bound.argtypes = [ctypes.c_void_p, dp, ctypes.c_double, dp, dp]
+        L.oracle_fp32_bound.restype = ctypes.c_long
         L.oracle_jk_quartets.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_long, ip, ip, ctypes.c_int]
         L.oracle_jk_uhf.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, ctypes.c_int]
         L.oracle_spherical_matrix.argtypes = [ctypes.c_int, dp]
@@ -166,6 +168,17 @@ class Oracle:
         K = np.zeros((self.n_bf, self.n_bf), order="F")
         lib().oracle_jk_quartets(self.h, _dp(Pf), _dp(J), _dp(K), len(bra), _ip(bra), _ip(ket), int(n_threads))
         return np.ascontiguousarray(J), np.ascontiguousarray(K)
+
+    def fp32_bound(self, P: np.ndarray, fp32_cut: float):
+        """(Jb, Kb, n): per element, the sum of the term bounds a mixed-precision build
+        evaluates in FP32 (quartets passing the screen with bound below fp32_cut), and
+        their number.  An FP32 evaluation with relative error delta is within delta Jb,
+        delta Kb of the FP64 build."""
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        Jb = np.zeros((self.n_bf, self.n_bf), order="F")
+        Kb = np.zeros((self.n_bf, self.n_bf), order="F")
+        n = lib().oracle_fp32_bound(self.h, _dp(Pf), float(fp32_cut), _dp(Jb), _dp(Kb))
+        return np.ascontiguousarray(Jb), np.ascontiguousarray(Kb), int(n)
 
     def jk_uhf(self, Pa: np.ndarray, Pb: np.ndarray, n_threads: int = 0):
         """Unrestricted (Ja, Jb, Ka, Kb) (Tonto's make_u_JK_direct): screened on Pa + Pb."""

@@ -862,6 +862,70 @@ void oracle_jk_quartets(OracleCtx* c, const double* P, double* J, double* K, lon
   finish_jk(B, J, K);
 }
 
+// The error budget of a mixed-precision build: over the quartets that pass
+// Tonto's screen and whose bound pm I_max(ab) I_max(cd) is below fp32_cut (the
+// quartets a mixed build evaluates in FP32), each J or K element's sum of the
+// bounds of the terms it receives: a digestion target element sums
+// (number of terms) x factor x bound over those quartets (J(ab): nc nd terms,
+// J(cd): na nb, K(ac): nb nd, K(ad): nb nc, K(bc): na nd, K(bd): na nc), then the
+// fold and reflection of the build.  Since |(ab|cd) P| <= bound for every term, an
+// FP32 evaluation with relative error delta changes an element by at most
+// delta x Jb (or Kb).  Returns the number of such quartets.
+long oracle_fp32_bound(OracleCtx* c, const double* P, double fp32_cut, double* Jb, double* Kb) {
+  Ctx* C = reinterpret_cast<Ctx*>(c);
+  const Basis& B = C->B;
+  const int n = B.n_bf;
+  const double cutoff = C->schwarz_cutoff;
+  std::vector<double> Pm;
+  max_density(*C, P, Pm);
+  std::vector<double> J((size_t)n * n, 0.0), K((size_t)n * n, 0.0);
+  long n_fp32 = 0;
+  const long npairs = (long)C->pairs.size();
+  for (long ab = 0; ab < npairs; ++ab) {
+    const PairData& pab = C->pairs[ab];
+    const int aa = pab.a, bb = pab.b;
+    const int fa = B.shell_first_bf[aa], fb = B.shell_first_bf[bb];
+    const int na = B.nbf_of(pab.la), nb = B.nbf_of(pab.lb);
+    for (long cd = 0; cd <= ab; ++cd) {
+      const PairData& pcd = C->pairs[cd];
+      const int cc = pcd.a, dd = pcd.b;
+      const long ac = pair_index(std::max(aa, cc), std::min(aa, cc)), ad = pair_index(std::max(aa, dd), std::min(aa, dd));
+      const long bc = pair_index(std::max(bb, cc), std::min(bb, cc)), bd = pair_index(std::max(bb, dd), std::min(bb, dd));
+      const double pm = std::max({Pm[ab], Pm[cd], Pm[ac], Pm[ad], Pm[bc], Pm[bd]});
+      if (pm < SKIP_P) continue;
+      const double bound = pm * C->max_I[ab] * C->max_I[cd];
+      if (!(bound > cutoff) || !(bound < fp32_cut)) continue;
+      ++n_fp32;
+      double factor = 1.0;
+      if (aa == bb) factor = 0.5;
+      if (cc == dd) factor *= 0.5;
+      if (ab == cd) factor *= 0.5;
+      const double fb_ = factor * bound;
+      const int fc = B.shell_first_bf[cc], fd = B.shell_first_bf[dd];
+      const int nc = B.nbf_of(pcd.la), ndd = B.nbf_of(pcd.lb);
+      auto add = [&](std::vector<double>& X, int r0, int nr, int c0, int ncl, double v) {
+        for (int j = c0; j < c0 + ncl; ++j)
+          for (int i = r0; i < r0 + nr; ++i) X[(size_t)j * n + i] += v;
+      };
+      add(J, fa, na, fb, nb, fb_ * nc * ndd);      // J(ab)
+      add(J, fc, nc, fd, ndd, fb_ * na * nb);      // J(cd)
+      add(K, fa, na, fc, nc, fb_ * nb * ndd);      // K(ac)
+      add(K, fa, na, fd, ndd, fb_ * nb * nc);      // K(ad)
+      add(K, fb, nb, fc, nc, fb_ * na * ndd);      // K(bc)
+      add(K, fb, nb, fd, ndd, fb_ * na * nc);      // K(bd)
+    }
+  }
+  // the fold moves contributions between triangles: bound both placements
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j) {
+      const double sj = J[(size_t)j * n + i] + J[(size_t)i * n + j], sk = K[(size_t)j * n + i] + K[(size_t)i * n + j];
+      J[(size_t)j * n + i] = J[(size_t)i * n + j] = sj;
+      K[(size_t)j * n + i] = K[(size_t)i * n + j] = sk;
+    }
+  for (size_t q = 0; q < (size_t)n * n; ++q) { Jb[q] = 4.0 * J[q]; Kb[q] = 2.0 * K[q]; }
+  return n_fp32;
+}
+
 // make_u_JK_direct (molecule.fock.foo:2360-2504): screening on the maxima of
 // Pa + Pb (:2397-2400), then alpha and beta J, K from each ERI.
 void oracle_jk_uhf(OracleCtx* c, const double* Pa, const double* Pb, double* Ja, double* Jb, double* Ka, double* Kb,

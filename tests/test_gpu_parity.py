@@ -98,19 +98,32 @@ def test_fock_matches_j_minus_half_k(cuda_ok, oracle_mod):
 
 
 @pytest.mark.gpu
-def test_mixed_precision_build_error_is_bounded(cuda_ok, oracle_mod):
-    """TF_JK_MIXED: quartets with Schwarz x density bound < 1e-6 in FP32 (FP64 roots,
-    weights, transfers and accumulation).  Each FP32 quartet contributes at most ~1e-6
-    with a relative error ~1e-6, so J and K stay within 1e-9 of the FP64 oracle."""
+@pytest.mark.parametrize("n_water", [4, 12])
+def test_mixed_precision_build_error_is_bounded(cuda_ok, oracle_mod, n_water):
+    """TF_JK_MIXED: quartets whose Schwarz x density bound is below the cut (1e-6) are
+    evaluated in FP32 after FP64 Rys nodes and weights, and accumulated in FP64.
+    The FP32 quartets are the oracle's quartets below the cut (their number pins the
+    cut), and every J, K element is within DELTA of its FP32 error budget of the FP64
+    oracle: the budget is the oracle's per-element sum of the bounds of the terms it
+    receives from those quartets (|(ab|cd) P| <= bound per term), DELTA a relative
+    error of FP32 evaluation, 2^-14, with room for the chain of about fifty FP32
+    operations and the spherical transform.  The observed error is far inside it, below
+    1e-9, which is checked too."""
     from tonto_b200.fock import FockBuilder, TF_JK_MIXED
-    mol = water_cluster(4, seed=0)
+    DELTA = 2.0 ** -14
+    mol = water_cluster(n_water, seed=0)
     orc = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
     P = core_density(orc, oracle_mod, mol)
     Jr, Kr = orc.jk(P)
+    Jb, Kb, n32 = orc.fp32_bound(P, 1e-6)
     fb = FockBuilder(mol, schwarz_cutoff=1e-12, mixed_fp32_cut=1e-6)
     J, K = fb.make_r_JK(P, TF_JK_MIXED)
     st = fb.stats()
     assert st["quartets_fp32"] > 0.3 * st["quartets"]
+    assert abs(st["quartets_fp32"] - n32) <= max(2, 1e-7 * n32), (st["quartets_fp32"], n32)
+    assert np.all(np.abs(J - Jr) <= DELTA * Jb + 1e-12)
+    assert np.all(np.abs(K - Kr) <= DELTA * Kb + 1e-12)
+    # and, as observed, far inside that budget
     assert np.max(np.abs(J - Jr)) < 1e-9 and np.max(np.abs(K - Kr)) < 1e-9
 
 

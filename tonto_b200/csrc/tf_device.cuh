@@ -435,6 +435,7 @@ __device__ __forceinline__ double4 ld4(const PrimPair* p, int half) {
 #ifndef TF_PRIM_UNROLL
 #define TF_PRIM_UNROLL 1
 #endif
+
 constexpr int kPrimUnroll = TF_PRIM_UNROLL;
 constexpr int PPS = sizeof(PrimPair) / sizeof(double2);         // 5 16-byte loads per record
 
@@ -459,12 +460,93 @@ __device__ __forceinline__ PrimRegs load_prim(const double2* __restrict__ q, int
   return r;
 }
 
+// 1/x and 1/sqrt(x) in FP32 (the PTX approximate instructions, about 23 correct
+// bits: the rounding level of the FP32 arithmetic they feed).
+__device__ __forceinline__ float rcp_f32(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_f32(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// One primitive quartet in the mixed-precision path: the Boys-function argument
+// and everything after the Rys nodes and weights in FP32 (exponent sums, rho, the
+// prefactor, the recurrence coefficients, the 2D recurrences and the (e0|f0)
+// products); P - Q in FP64 (a difference of positions), then the nodes and weights
+// themselves in FP64 from the FP64 tables, as for the FP64 path.
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void prim_quartet_f32(const PrimRegs& B, const PrimRegs& K, double wmask,
+                                                 float (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
+                                                 const double* __restrict__ rys_smem) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
+  const float zeta = (float)B.Z.y, eta = (float)K.Z.y;
+  const float half_zinv = (float)B.C.y, half_einv = (float)K.C.y;
+  const float inv = rcp_f32(zeta + eta);
+  const float rho = zeta * eta * inv;
+  const float QP[3] = {(float)(K.P.x - B.P.x), (float)(K.P.y - B.P.y), (float)(K.Z.x - B.Z.x)};
+  const float xx = rho * (QP[0] * QP[0] + QP[1] * QP[1] + QP[2] * QP[2]);
+  double u[NR], w[NR];
+  if (rys_smem) RysSmem<NR>::eval(rys_smem, (double)xx, u, w);
+  else rys_eval<NR>((double)xx, u, w);
+  const float scale = (float)(B.C.x * K.C.x * (TWOPI5ON2 * wmask)) * (rho * rsqrt_f32(rho));
+  const float r_z = eta * inv;     // rho / zeta
+  const float r_e = zeta * inv;    // rho / eta
+  const float PA[3] = {(float)B.A0.x, (float)B.A0.y, (float)B.A1.x};
+  const float QC[3] = {(float)K.A0.x, (float)K.A0.y, (float)K.A1.x};
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const float t2 = (float)u[r];
+    const float t2_rz = t2 * r_z, t2_re = t2 * r_e;
+    const float B10 = (1.0f - t2_rz) * half_zinv;
+    const float B01 = (1.0f - t2_re) * half_einv;
+    const float B00 = 0.5f * t2 * inv;
+    const float wt = (float)w[r] * scale;
+    float I[3][D1][D2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float c00 = fmaf(t2_rz, QP[d], PA[d]);
+      const float d00 = fmaf(-t2_re, QP[d], QC[d]);
+      I[d][0][0] = (d == 2) ? wt : 1.0f;
+      if (D1 > 1) I[d][1][0] = c00 * I[d][0][0];
+#pragma unroll
+      for (int e = 1; e + 1 < D1; ++e) I[d][e + 1][0] = c00 * I[d][e][0] + float(e) * B10 * I[d][e - 1][0];
+#pragma unroll
+      for (int f = 0; f + 1 < D2; ++f) {
+#pragma unroll
+        for (int e = 0; e < D1; ++e) {
+          float v = d00 * I[d][e][f];
+          if (f > 0) v += float(f) * B01 * I[d][e][f - 1];
+          if (e > 0) v += float(e) * B00 * I[d][e - 1][f];
+          I[d][e][f + 1] = v;
+        }
+      }
+    }
+    static_for<Q::NE>([&](auto e) {
+      constexpr int ge = Q::FE + decltype(e)::value;
+      static_for<Q::NF>([&](auto f) {
+        constexpr int gf = Q::FF + decltype(f)::value;
+        esfs[decltype(e)::value][decltype(f)::value] +=
+            I[0][gx(ge)][gx(gf)] * I[1][gy(ge)][gy(gf)] * I[2][gz(ge)][gz(gf)];
+      });
+    });
+  }
+}
+
 // One primitive quartet: Rys nodes and weights, the 2D recurrences and the
 // (e0|f0) products, added to esfs with weight `wmask`.
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void prim_quartet(const PrimRegs& B, const PrimRegs& K, double wmask,
                                              T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
                                              const double* __restrict__ rys_smem) {
+  if constexpr (std::is_same<T, float>::value) {
+    prim_quartet_f32<LA, LB, LC, LD>(B, K, wmask, esfs, rys_smem);
+    return;
+  }
   using Q = Quartet<LA, LB, LC, LD>;
   constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
   const double bcc = B.C.x * TWOPI5ON2, kcc = K.C.x;

@@ -1820,8 +1820,8 @@ static void class_l(int k, int& lh, int& ll) {
 // kernel and before any graph capture: a zero-sized, range-less JKArgs only sets up.
 template <int LA, int LB, int LC, int LD, typename T, int V>
 static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
-  constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
   constexpr int thr = jk_threads<LA, LB, LC, LD, V>();
+  constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {
     cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
