@@ -220,24 +220,26 @@ int tf_set_kernel_variant(tf_ctx* ctx, int variant);
 int tf_set_shard(tf_ctx* ctx, int index, int count);
 
 /* The shard plan of one molecule's build, on the host (no device calls, runs without
- * a GPU): the bra tasks tf_set_shard deals out, and the shard of each.  A task is a
- * bra shell pair with the kets of one pair class: every ket of that class when the
- * bra's class is higher, else the kets at positions up to the bra's own in the class
- * list (pairs of a class ordered by half-decade I_max band, largest first, then by
- * pair index).  Together the tasks hold every unordered pair of shell pairs once, as
- * Tonto's outer loop ab with cd <= ab does (molecule.fock.foo:1274-1286).  Tasks are
- * dealt largest estimated cost first to the least-loaded shard (the estimate: the
- * kets passing I_max(ab) I_max(cd) > cutoff at a unit density maximum, times primitive
- * quartets and a per-class FLOP model); Tonto's parallel do deals them round-robin
+ * a GPU): the bra tasks tf_set_shard deals out, and the shard of each, written as
+ * rows of (bra shell pair, ket pair class, ket limit, shard).  A row covers the ket
+ * pairs of its class at class-list positions up to its limit; the class list orders a
+ * class's pairs by half-decade I_max band (largest first; a shell-pair family, see
+ * tf_ctx_create, placed by its largest I_max with its members together), then by
+ * pair index.  A task whose bra is a family gives one row per member.  Together the
+ * rows hold every unordered pair of shell pairs once, as Tonto's outer loop ab with
+ * cd <= ab does (molecule.fock.foo:1274-1286).  Tasks are dealt largest estimated
+ * cost first to the least-loaded shard (the estimate: the kets passing
+ * I_max(ab) I_max(cd) > cutoff at a unit density maximum, times primitive quartets
+ * and a per-class FLOP model); Tonto's parallel do deals them round-robin
  * (FooToFortran.java:2762-2783), which leaves the shards' work uneven.
  *   max_I: Schwarz bounds in Tonto pair order ab = a(a+1)/2 + b (tf_schwarz);
- *   *n_tasks: the number of tasks; the arrays, if not NULL, receive per task the bra's
- *   Tonto pair index, the ket pair class (l_hi(l_hi+1)/2 + l_lo) and the shard;
- *   pair_position[n_pairs]: each pair's position in its class list;
+ *   *n_rows: the number of rows; the arrays, if not NULL, receive per row the bra's
+ *   Tonto pair index, the ket pair class (l_hi(l_hi+1)/2 + l_lo), the ket limit and
+ *   the shard; pair_position[n_pairs]: each pair's position in its class list;
  *   shard_cost[n_shards]: the estimated FLOPs of every shard. */
 int tf_plan_shards(const tf_basis* basis, const double* max_I, double schwarz_cutoff, int n_shards,
-                   long long* n_tasks, int* task_bra, int* task_ket_class, int* task_shard, int* pair_position,
-                   double* shard_cost);
+                   long long* n_rows, int* row_bra, int* row_ket_class, int* row_ket_limit, int* row_shard,
+                   int* pair_position, double* shard_cost);
 
 /* J and K from the symmetric density P (host arrays, column-major n_bf x n_bf).
  * Replaces make_r_JK_direct / make_r_JK_engine.  flags: TF_JK_*.  A density with a

@@ -102,8 +102,9 @@ def test_fock_matches_j_minus_half_k(cuda_ok, oracle_mod):
 def test_mixed_precision_build_error_is_bounded(cuda_ok, oracle_mod, n_water):
     """TF_JK_MIXED: quartets whose Schwarz x density bound is below the cut (1e-6) are
     evaluated in FP32 after FP64 Rys nodes and weights, and accumulated in FP64.
-    The FP32 quartets are the oracle's quartets below the cut (their number pins the
-    cut), and every J, K element is within DELTA of its FP32 error budget of the FP64
+    The FP32 quartets are the oracle's quartets below the cut, less at most 3 % that
+    share a bra-family entry with an above-cut quartet (the count pins the cut), and
+    every J, K element is within DELTA of its FP32 error budget of the FP64
     oracle: the budget is the oracle's per-element sum of the bounds of the terms it
     receives from those quartets (|(ab|cd) P| <= bound per term), DELTA a relative
     error of FP32 evaluation, 2^-14, with room for the chain of about fifty FP32
@@ -120,7 +121,10 @@ def test_mixed_precision_build_error_is_bounded(cuda_ok, oracle_mod, n_water):
     J, K = fb.make_r_JK(P, TF_JK_MIXED)
     st = fb.stats()
     assert st["quartets_fp32"] > 0.3 * st["quartets"]
-    assert abs(st["quartets_fp32"] - n32) <= max(2, 1e-7 * n32), (st["quartets_fp32"], n32)
+    # a bra-family entry runs in FP32 only when every member quartet it holds is below
+    # the cut, so the FP32 member quartets are the oracle's below-cut quartets less the
+    # few that share an entry with an above-cut one
+    assert 0.97 * n32 <= st["quartets_fp32"] <= n32, (st["quartets_fp32"], n32)
     assert np.all(np.abs(J - Jr) <= DELTA * Jb + 1e-12)
     assert np.all(np.abs(K - Kr) <= DELTA * Kb + 1e-12)
     # and, as observed, far inside that budget

@@ -36,16 +36,17 @@ def _plan(mol, max_I, cutoff, world):
     dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
     ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))     # noqa: E731
     nt = ctypes.c_longlong()
-    rc = L.tf_plan_shards(ctypes.byref(basis), dp(mi), cutoff, world, ctypes.byref(nt), None, None, None, None, None)
+    rc = L.tf_plan_shards(ctypes.byref(basis), dp(mi), cutoff, world, ctypes.byref(nt), None, None, None, None, None,
+                          None)
     assert rc == 0
     n = nt.value
-    bra, kcls, shard = (np.zeros(n, dtype=np.int32) for _ in range(3))
+    bra, kcls, klim, shard = (np.zeros(n, dtype=np.int32) for _ in range(4))
     pos = np.zeros(len(mi), dtype=np.int32)
     cost = np.zeros(world)
-    rc = L.tf_plan_shards(ctypes.byref(basis), dp(mi), cutoff, world, ctypes.byref(nt), ip(bra), ip(kcls), ip(shard),
-                          ip(pos), dp(cost))
+    rc = L.tf_plan_shards(ctypes.byref(basis), dp(mi), cutoff, world, ctypes.byref(nt), ip(bra), ip(kcls), ip(klim),
+                          ip(shard), ip(pos), dp(cost))
     assert rc == 0
-    return bra, kcls, shard, pos, cost
+    return bra, kcls, klim, shard, pos, cost
 
 
 def _pair_classes(mol):
@@ -58,15 +59,14 @@ def _pair_classes(mol):
     return np.array(cls)
 
 
-def _expand(bra, kcls, pos, pcls):
-    """Shell quartets of a set of tasks: the kets of the task's class, all of them for a
-    higher bra class, else those at list positions up to the bra's own."""
+def _expand(bra, kcls, klim, pos, pcls):
+    """Shell quartets of a set of plan rows: the kets of the row's class at class-list
+    positions up to the row's limit."""
     by_cls = {c: np.flatnonzero(pcls == c) for c in np.unique(pcls)}
     qb, qk = [], []
-    for b, kc in zip(bra, kcls):
+    for b, kc, lim in zip(bra, kcls, klim):
         kets = by_cls.get(int(kc), np.zeros(0, dtype=np.int64))
-        if pcls[b] == kc:
-            kets = kets[pos[kets] <= pos[b]]
+        kets = kets[pos[kets] <= lim]
         qb.append(np.full(len(kets), b))
         qk.append(kets)
     return np.concatenate(qb), np.concatenate(qk)
@@ -89,9 +89,9 @@ def _plan_worker(rank, world, port, q):
     orc = oracle.Oracle(mol, schwarz_cutoff=cutoff)
     S, T, V = orc.one_electron()
     P, _, _ = oracle.density_from_fock(T + V, oracle.orthogonaliser(S), mol.n_electrons // 2)
-    bra, kcls, shard, pos, cost = _plan(mol, orc.max_I(), cutoff, world)
+    bra, kcls, klim, shard, pos, cost = _plan(mol, orc.max_I(), cutoff, world)
     mine = shard == rank
-    qb, qk = _expand(bra[mine], kcls[mine], pos, _pair_classes(mol))
+    qb, qk = _expand(bra[mine], kcls[mine], klim[mine], pos, _pair_classes(mol))
     J, K = orc.jk_quartets(P, qb, qk, n_threads=1)
     Jt = torch.from_numpy(J.copy())
     Kt = torch.from_numpy(K.copy())
@@ -104,7 +104,7 @@ def _plan_worker(rank, world, port, q):
     if rank == 0:
         Jr, Kr = orc.jk(P, n_threads=1)
         # every unordered pair of shell pairs exactly once over the shards
-        qa, qc = _expand(bra, kcls, pos, _pair_classes(mol))
+        qa, qc = _expand(bra, kcls, klim, pos, _pair_classes(mol))
         key = np.maximum(qa, qc).astype(np.int64) * 10**6 + np.minimum(qa, qc)
         n_pairs = len(pos)
         q.put({"dJ": float(np.max(np.abs(Jt.numpy() - Jr))), "dK": float(np.max(np.abs(Kt.numpy() - Kr))),
@@ -142,7 +142,7 @@ def test_shard_plan_balances_estimated_cost():
     from tonto_b200.molecules import water_cluster
     mol = water_cluster(8, seed=2)
     orc = oracle.Oracle(mol, schwarz_cutoff=1e-12)
-    bra, kcls, shard, pos, cost = _plan(mol, orc.max_I(), 1e-12, 4)
+    bra, kcls, klim, shard, pos, cost = _plan(mol, orc.max_I(), 1e-12, 4)
     assert cost.max() / cost.mean() - 1.0 < 0.01
     assert sorted(np.unique(shard)) == [0, 1, 2, 3]
 

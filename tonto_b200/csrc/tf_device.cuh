@@ -742,6 +742,82 @@ __device__ __forceinline__ void hrr_bra(const T (&G)[CT.first[LA + LB + 1] - CT.
   }
 }
 
+// (e0|f0) of a bra family: the primitive loop runs once over the positioned
+// primitive pairs the members share (bp, the first member's), each primitive
+// quartet evaluated with a unit bra coefficient and added into every member's block
+// with that member's coefficient product (bm[m][ib].cc; bm[m] null: no member m).
+template <int LA, int LB, int LC, int LD, typename T, int MB>
+__device__ __forceinline__ void accumulate_esfs_fam(const PrimPair* __restrict__ bp, int nbp,
+                                                    const PrimPair* __restrict__ kp, int nkp,
+                                                    const PrimPair* const (&bm)[MB],
+                                                    T (&esfs)[MB][Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
+                                                    const double* __restrict__ rys_smem) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  constexpr bool BPA = Q::LAB > 0, KPA = Q::LCD > 0;
+#pragma unroll
+  for (int m = 0; m < MB; ++m)
+#pragma unroll
+    for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+      for (int f = 0; f < Q::NF; ++f) esfs[m][e][f] = T(0);
+  const int npq = nbp * nkp;
+  if (npq <= 0) return;
+  const double2* bq = reinterpret_cast<const double2*>(bp);
+  const double2* kq = reinterpret_cast<const double2*>(kp);
+  int ib = 0, ik = 0;
+  PrimRegs kc = load_prim<KPA>(kq, 0);
+  for (int p = 0; p < npq; ++p) {
+    PrimRegs b = load_prim<BPA>(bq, ib);
+    double cb[MB];
+#pragma unroll
+    for (int m = 0; m < MB; ++m) cb[m] = bm[m] ? __ldg(&bm[m][ib].cc) : 0.0;
+    b.C.x = 1.0;
+    const PrimRegs k = kc;
+    if (++ib == nbp) {
+      ib = 0;
+      ++ik;
+      if (ik < nkp) kc = load_prim<KPA>(kq, ik);
+    }
+    T one[Q::NE][Q::NF];
+#pragma unroll
+    for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+      for (int f = 0; f < Q::NF; ++f) one[e][f] = T(0);
+    prim_quartet<LA, LB, LC, LD, T>(b, k, 1.0, one, rys_smem);
+#pragma unroll
+    for (int m = 0; m < MB; ++m) {
+      const T w = T(cb[m]);
+#pragma unroll
+      for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+        for (int f = 0; f < Q::NF; ++f) esfs[m][e][f] += w * one[e][f];
+    }
+  }
+}
+
+// Horizontal transfers of one (e0|f0) block to the Cartesian (ab|cd), as double.
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void hrr_quartet(const T (&esfs)[Quartet<LA, LB, LC, LD>::NE][Quartet<LA, LB, LC, LD>::NF],
+                                            const double* Rab, const double* Rcd,
+                                            double (&abcd)[ncart(LA)][ncart(LB)][ncart(LC) * ncart(LD)]) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  double ed[Q::NE][Q::NF];
+#pragma unroll
+  for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+    for (int f = 0; f < Q::NF; ++f) ed[e][f] = (double)esfs[e][f];
+  double ket[Q::NE][Q::NC][Q::ND];
+  hrr_ket<LC, LD, Q::NE, double>(ed, Rcd, ket);
+  double flat[Q::NE][Q::NC * Q::ND];
+#pragma unroll
+  for (int e = 0; e < Q::NE; ++e)
+#pragma unroll
+    for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) flat[e][c * Q::ND + d] = ket[e][c][d];
+  hrr_bra<LA, LB, Q::NC * Q::ND, double>(flat, Rab, abcd);
+}
+
 // Contracted Cartesian integrals (ab|cd) of one quartet, as double.
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void quartet_integrals(const PrimPair* bp, int nbp, const PrimPair* kp, int nkp,

@@ -233,6 +233,7 @@ struct GroupArgs {
   double* J2;
   double* K2;
   int want;                     // bit 0 J, bit 1 K
+  unsigned long long* qcount;   // quartets counted per class (the launch's FP64 or FP32 half), or null
 };
 
 // Rys nodes and weights of a lane group's primitive quartet: the 2 N polynomial
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
   const int gf = Q::FF + (in_group ? gl : 0);
   const int fx = sc.x[gf], fy = sc.y[gf], fz = sc.z[gf];
   const long long nwarps = (long long)gridDim.x * wpb;
-  unsigned long long nprim = 0;
+  unsigned long long nprim = 0, nquart = 0;
   const int2* quartets = a.quartets;
   long long nq = a.n;
   resolve_range(a.range, a.base, a.cap, quartets, nq);
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
     const int nbp = any_same ? b.n_full : b.n_skip;
     const int nkp = any_same ? k.n_full : k.n_skip;
     const int npq = act ? nbp * nkp : 0;
-    if (act && gl == 0) nprim += (unsigned long long)npq;
+    if (act && gl == 0) { nprim += (unsigned long long)npq; nquart += 1; }
     const int maxnpq = __reduce_max_sync(0xffffffffu, npq);
     double es[Q::NE];
 #pragma unroll
@@ -493,8 +494,12 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
     __syncwarp();
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) nprim += __shfl_xor_sync(0xffffffffu, nprim, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    nprim += __shfl_xor_sync(0xffffffffu, nprim, o);
+    nquart += __shfl_xor_sync(0xffffffffu, nquart, o);
+  }
   if (lane == 0 && nprim) atomicAdd(a.prim_count + (((LA * 5 + LB) * 5 + LC) * 5 + LD), nprim);
+  if (lane == 0 && nquart && a.qcount) atomicAdd(a.qcount + (((LA * 5 + LB) * 5 + LC) * 5 + LD), nquart);
 }
 
 template <int LA, int LB, int LC, int LD>

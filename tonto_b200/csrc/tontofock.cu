@@ -39,8 +39,22 @@ namespace tf {
 constexpr int LMAX_SUPPORTED = 3;                 // s, p, d, f shells (f: the warp path)
 constexpr int NPAIRCLS = (LMAX_SUPPORTED + 1) * (LMAX_SUPPORTED + 2) / 2;
 constexpr int NQCLS = 625;                        // (la lb lc ld) counter slots, l <= 4
+// Counters of a build, zeroed with it and read back after it: primitive quartets per
+// class [0, NQCLS), the non-finite-density flag [NQCLS], contracted quartets per class
+// of the FP64 buckets [NQCLS + 1, 2 NQCLS + 1) and of the FP32 buckets after them.
+constexpr int BUILD_COUNTERS = 3 * NQCLS + 1;
 __host__ __device__ constexpr int pair_class(int lh, int ll) { return lh * (lh + 1) / 2 + ll; }
 __host__ __device__ constexpr int qclass_id(int la, int lb, int lc, int ld) { return ((la * 5 + lb) * 5 + lc) * 5 + ld; }
+// Bra-family members the thread kernel of a class holds at once (accumulator
+// capacity), for the classes where evaluating a bra family's primitive quartets once
+// measured faster on (H2O)32 cc-pVDZ: (ss|ss) 9.36 -> 8.36 ms, (ds|ss) 3.87 -> 3.63 ms.
+// (ps|ss), (ps|ps) and (ds|ps) measured slower with it (13.33 -> 13.45, 8.55 -> 8.90
+// and 4.29 -> 5.63 ms: the extra accumulators cost registers and the coefficient
+// loads and products every primitive quartet, and few of their bras are families),
+// so they, like every other class, take one member per list entry (capacity 1).
+__host__ __device__ constexpr int fam_cap_l(int la, int lb, int lc, int ld) {
+  return (la == 0 && lb == 0 && lc == 0 && ld == 0) ? 4 : (la == 2 && lb == 0 && lc == 0 && ld == 0) ? 2 : 1;
+}
 
 __constant__ double c_U[4][10 * 7];               // Cartesian -> spherical, l = 0..3, [cart][m]
 
@@ -270,15 +284,32 @@ static_assert(NBUCKET < 0xff, "bucket ids are recorded as bytes, 0xff = screened
 // pair are consecutive and form a group; the quartets of a group are one launch.
 struct CPUnit {
   int p1, p2;                   // bra and ket pair classes
-  int bra_off, ket_off;         // offsets of the molecule's class lists in `sorted`
+  int bra_off, ket_off;         // offsets of the molecule's class lists: the bra list in `csorted`
+                                // (family units) or `sorted`, the ket list in `sorted`
   int n_ket, mol;
+  int fam;                      // 1: the bra tasks are shell-pair families (see make_pair_families)
+  int bra_xoff;                 // offset of the bra class's list in `sorted` (family units)
+};
+
+// Shell-pair families of a context (built on the host, see make_pair_families).
+struct PairFamilies {
+  std::vector<int> rep;                    // first member of each pair's family (pair ids)
+  std::vector<int> index;                  // position of each pair in its family
+  std::vector<int4> members;               // the family's member pair ids, -1 padded
+  std::vector<int> n;                      // members of the pair's family
 };
 
 // Class lists of a context (built on the host, see make_class_lists).
 struct ClassLists {
-  std::vector<int> sorted;                 // pair ids by (molecule, class), then band order
-  std::vector<double> simax, sbmax;        // I_max of each position; largest I_max of its band
+  std::vector<int> sorted;                 // pair ids by (molecule, class), band order, families contiguous
+  std::vector<double> simax, sbmax;        // I_max of each position; largest family I_max of its band
   std::vector<int> cls_n, cls_off;         // [mol * NPAIRCLS + class]
+  // the same lists with each shell-pair family collapsed to its first member
+  std::vector<int> csorted;                // first member's pair id
+  std::vector<double> cimax;               // the family's largest I_max
+  std::vector<int> cxstart, cn;            // position of the first member in the class's `sorted` list; members
+  std::vector<int> cls_cn, cls_coff;       // [mol * NPAIRCLS + class]
+  std::vector<int> cls_maxm;               // largest family of the (molecule, class) list
 };
 
 struct ListArgs {
@@ -312,6 +343,13 @@ struct ListArgs {
   const long long* list_total;
   // raised by k_pmax when the density has a non-finite element: no quartets listed
   const unsigned long long* bad;
+  // family units (CPUnit::fam): the collapsed bra lists, and per list entry the mask of
+  // the bra family's members whose quartet with the ket passes the screen
+  const int* csorted;
+  const double* cimax;
+  const int* cxstart;
+  const int* cn;
+  unsigned char* qmask;
 };
 
 // Screening record of a sorted pair position, 16 bytes read in list order (coalesced):
@@ -375,28 +413,53 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
   const CPUnit cp = a.units[task.x];
   const int g = a.unit_group[task.x];
   const int i = task.y;
-  const int bra = a.sorted[cp.bra_off + i];
-  const int jend = (a.bad && *a.bad) ? 0 : ((cp.p1 == cp.p2) ? i + 1 : cp.n_ket);
+  // a family task: the family's first member stands for the bra; its members sit at
+  // xs .. xs + nm - 1 of the bra class's list
+  const int bra = cp.fam ? a.csorted[cp.bra_off + i] : a.sorted[cp.bra_off + i];
+  const int xs = cp.fam ? a.cxstart[cp.bra_off + i] : 0;
+  const int nm = cp.fam ? a.cn[cp.bra_off + i] : 1;
+  const int jend = (a.bad && *a.bad) ? 0 : ((cp.p1 == cp.p2) ? (cp.fam ? xs + nm : i + 1) : cp.n_ket);
   const long long coff = a.cand ? a.cand_off[t] : 0;
   const int len = MODE == 2 ? a.task_len[t] : jend;
   double Ib = 0.0, pg = 0.0;
   int4 b = make_int4(0, 0, 0, 0);
   MolInfo mi{};
-  if (MODE != 2) {
-    Ib = a.sorted_imax[cp.bra_off + i];
-    b = a.srec[cp.bra_off + i];
+  if (MODE != 2 || cp.fam) {
+    Ib = cp.fam ? a.cimax[cp.bra_off + i] : a.sorted_imax[cp.bra_off + i];
+    b = cp.fam ? a.srec[cp.bra_xoff + xs] : a.srec[cp.bra_off + i];
     mi = a.mols[cp.mol];
     pg = __longlong_as_double((long long)a.pglob[cp.mol]);
   }
+  // members of the bra family whose quartet with ket position j passes the screen
+  // (inside the family's own block, p1 == p2, only members at or after the ket)
+  auto family_mask = [&](int j, const int4 k, double Ik, double& maxb) {
+    unsigned m_ok = 0;
+    maxb = 0.0;
+    for (int m = 0; m < nm; ++m) {
+      if (cp.p1 == cp.p2 && j - xs > m) continue;
+      const int4 bm = a.srec[cp.bra_xoff + xs + m];
+      const double bound = quartet_bound(a, mi, bm, k, a.sorted_imax[cp.bra_xoff + xs + m], Ik);
+      if (bound > a.cutoff) { m_ok |= 1u << m; maxb = fmax(maxb, bound); }
+    }
+    return m_ok;
+  };
   int scanned = 0;
   for (int j0 = 0; j0 < len; j0 += 32) {
     const int j = j0 + lane;
     bool beyond = false;
     int ket = 0, bucket = -1;
+    unsigned fmask = 1;
     if (MODE == 2) {
       if (j < len) {
         const unsigned char cb = a.cand[coff + j];
-        if (cb != 0xff) { bucket = cb; ket = a.sorted[cp.ket_off + j]; }
+        if (cb != 0xff) {
+          bucket = cb;
+          ket = a.sorted[cp.ket_off + j];
+          if (cp.fam) {
+            double maxb;
+            fmask = family_mask(j, a.srec[cp.ket_off + j], a.sorted_imax[cp.ket_off + j], maxb);
+          }
+        }
       }
     } else if (j < jend) {
       const double Ik = a.sorted_imax[cp.ket_off + j];
@@ -405,8 +468,14 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
       } else if (Ib * Ik * pg > a.cutoff) {
         const int4 k = a.srec[cp.ket_off + j];
         ket = k.w;
-        const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
-        if (bound > a.cutoff) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
+        if (cp.fam) {
+          double maxb;
+          fmask = family_mask(j, k, Ik, maxb);
+          if (fmask) bucket = cost_bucket(b, k) + (maxb < a.fp32_cut ? NCOST : 0);
+        } else {
+          const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
+          if (bound > a.cutoff) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
+        }
       }
       if (MODE == 0 && a.cand) a.cand[coff + j] = bucket >= 0 ? (unsigned char)bucket : (unsigned char)0xff;
     }
@@ -418,7 +487,10 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
     __syncwarp();
     if (MODE != 0 && bucket >= 0) {
       const long long pos = offsets[slot(a, t, g, bucket)] - a.out_base + base + rank;
-      if (pos < a.out_cap) out[pos] = make_int2(bra, ket);
+      if (pos < a.out_cap) {
+        out[pos] = make_int2(bra, ket);
+        if (cp.fam) a.qmask[pos] = (unsigned char)fmask;
+      }
     }
     scanned = j0 + 32;
     if (MODE != 2 && __any_sync(0xffffffffu, beyond)) break;
@@ -458,6 +530,13 @@ struct JKArgs {
   // classes with an f shell (k_jk_warp): per-warp global scratch and its warp count
   double* wscratch;
   long long wscratch_warps;
+  // bra families (family groups): per list entry the members' mask, per pair its
+  // family members; member quartets counted per class, FP64 buckets then FP32
+  const unsigned char* qmask;
+  const int4* fam_mem;
+  unsigned long long* qcount;
+  int fam;                      // bra-family capacity of the launch's kernel (1: none)
+  int bucket32;                 // 1: the launch covers the FP32 buckets
 };
 
 
@@ -489,25 +568,231 @@ constexpr int jk_threads() {
   return jk_min_blocks<LA, LB, LC, LD, V>() == 1 ? 256 : 128 * jk_min_blocks<LA, LB, LC, LD, V>();
 }
 
-template <int LA, int LB, int LC, int LD, typename T, int V>
+// Digestion of one quartet's Cartesian integrals I into J and K with the coincidence
+// factor f (f = 0: the lane adds nothing but still takes part in the warp sums):
+// bid is the bra pair (lanes of one bra are summed together), ob/oa the bra's and
+// oc/od the ket's first Cartesian functions.
+//   J(ab) += f sum_cd I P(cd);  J(cd) += f sum_ab I P(ab)  (per spin when unrestricted)
+//   K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
+//   K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
+// The lists are bra-major, so the lanes of a warp usually share the bra pair: then
+// J(ab) is summed over the warp and added once, and P(ab) is a broadcast.  Otherwise
+// the lanes of one bra are neighbours (a bra's kets of one cost bucket are
+// consecutive) and J(ab) is summed over each run of equal bras by a segmented warp
+// scan, then added by the run's last lane.  Variant bit 2: the K rows a and b are the
+// same for all lanes of one bra, and lanes whose kets share the c (or d) shell add to
+// the same K elements; such lanes are neighbours (pair-id order), so each run of
+// equal (bra, shell) keys is summed with a segmented warp scan and added once, by its
+// last lane.  K(bc), K(bd) are summed over a's components in registers first.
+template <int LA, int LB, int LC, int LD, int V>
+__device__ __forceinline__ void digest_jk(const JKArgs& a, const MolInfo& mi,
+                                          const double (&I)[ncart(LA)][ncart(LB)][ncart(LC) * ncart(LD)], double f,
+                                          int bid, int oa, int ob, int oc, int od) {
+  using Q = Quartet<LA, LB, LC, LD>;
+  const int lane = threadIdx.x & 31;
+  const bool live = f != 0.0;
+  const int n = mi.n_cart;
+  const bool uni = __all_sync(0xffffffffu, bid == __shfl_sync(0xffffffffu, bid, 0));
+  const unsigned lt_mask = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+  // (every lane executes the shuffle: none may be skipped by a short-circuit)
+  const int upx = __shfl_up_sync(0xffffffffu, bid, 1);
+  const bool headx = lane == 0 || bid != upx;
+  const unsigned heada = __ballot_sync(0xffffffffu, headx);
+  const int sega = 31 - __clz(heada & lt_mask);
+  const bool taila = lane == 31 || ((heada >> (lane + 1)) & 1u);
+  auto digest_j = [&](const double* __restrict__ P, double* __restrict__ Jm) {
+    double Pcd[Q::NC][Q::ND];
+#pragma unroll
+    for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Pcd[c][d] = __ldg(P + (size_t)(oc + c) * n + od + d);
+#pragma unroll
+    for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) {
+        double s = 0.0;
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
+        s *= f;
+        if (uni) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+          if (lane == 0 && s != 0.0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+        } else {                       // idle lanes join the last run with s = 0
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const double t = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane - o >= sega) s += t;
+          }
+          if (taila && s != 0.0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+        }
+      }
+    if (live) {
+      double Pab[Q::NA][Q::NB];
+#pragma unroll
+      for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < Q::NB; ++ib) Pab[ia][ib] = __ldg(P + (size_t)(oa + ia) * n + ob + ib);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d) {
+          double s = 0.0;
+#pragma unroll
+          for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
+          atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+        }
+    }
+  };
+  if (a.want & 1) {                    // uniform over the warp (the J(ab) sums shuffle)
+    digest_j(a.P + mi.cmat, a.J + mi.cmat);
+    if (a.P2) digest_j(a.P2 + mi.cmat, a.J2 + mi.cmat);
+  }
+  constexpr bool SEG = (V & 2) != 0;
+  int segc = lane, segd = lane;
+  bool tailc = true, taild = true;
+  if constexpr (SEG) {
+    // (every lane executes both shuffles: none may be skipped by a short-circuit)
+    const int upc = __shfl_up_sync(0xffffffffu, oc, 1), upd = __shfl_up_sync(0xffffffffu, od, 1);
+    const unsigned headc = __ballot_sync(0xffffffffu, headx || oc != upc);
+    const unsigned headd = __ballot_sync(0xffffffffu, headx || od != upd);
+    segc = 31 - __clz(headc & lt_mask);
+    segd = 31 - __clz(headd & lt_mask);
+    tailc = lane == 31 || ((headc >> (lane + 1)) & 1u);
+    taild = lane == 31 || ((headd >> (lane + 1)) & 1u);
+  }
+  auto kadd = [&](double* addr, double v, int seg, bool tail) {
+    if constexpr (SEG) {
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane - o >= seg) v += t;
+      }
+      if (tail && v != 0.0) atomicAdd(addr, v);
+    } else {
+      atomicAdd(addr, v);
+    }
+  };
+#define TF_KADD_C(addr, v) kadd((addr), (v), segc, tailc)
+#define TF_KADD_D(addr, v) kadd((addr), (v), segd, taild)
+  auto digest_k = [&](const double* __restrict__ P, double* __restrict__ Km) {
+    double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
+    double Kbc[Q::NB][Q::NC], Kbd[Q::NB][Q::ND];
+#pragma unroll
+    for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) Kbc[ib][c] = 0.0;
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Kbd[ib][d] = 0.0;
+    }
+#pragma unroll
+    for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Pbd[ib][d] = __ldg(P + (size_t)(ob + ib) * n + od + d);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) Pbc[ib][c] = __ldg(P + (size_t)(ob + ib) * n + oc + c);
+    }
+#pragma unroll
+    for (int ia = 0; ia < Q::NA; ++ia) {
+      double Pad[Q::ND], Pac[Q::NC];
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) Pad[d] = __ldg(P + (size_t)(oa + ia) * n + od + d);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) Pac[c] = __ldg(P + (size_t)(oa + ia) * n + oc + c);
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int ib = 0; ib < Q::NB; ++ib)
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pbd[ib][d];
+        TF_KADD_C(Km + (size_t)(oa + ia) * n + oc + c, f * s);
+      }
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) {
+        double s = 0.0;
+#pragma unroll
+        for (int ib = 0; ib < Q::NB; ++ib)
+#pragma unroll
+          for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pbc[ib][c];
+        TF_KADD_D(Km + (size_t)(oa + ia) * n + od + d, f * s);
+      }
+#pragma unroll
+      for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+        for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+          for (int d = 0; d < Q::ND; ++d) Kbc[ib][c] += I[ia][ib][c * Q::ND + d] * Pad[d];
+#pragma unroll
+        for (int d = 0; d < Q::ND; ++d)
+#pragma unroll
+          for (int c = 0; c < Q::NC; ++c) Kbd[ib][d] += I[ia][ib][c * Q::ND + d] * Pac[c];
+      }
+    }
+    // K(bc), K(bd): summed over the a components first, one atomic per element
+#pragma unroll
+    for (int ib = 0; ib < Q::NB; ++ib) {
+#pragma unroll
+      for (int c = 0; c < Q::NC; ++c) TF_KADD_C(Km + (size_t)(ob + ib) * n + oc + c, f * Kbc[ib][c]);
+#pragma unroll
+      for (int d = 0; d < Q::ND; ++d) TF_KADD_D(Km + (size_t)(ob + ib) * n + od + d, f * Kbd[ib][d]);
+    }
+  };
+  // with segmented sums every lane takes part (idle lanes add f = 0)
+  if ((SEG || live) && (a.want & 2)) {
+    digest_k(a.P + mi.cmat, a.K + mi.cmat);
+    if (a.P2) digest_k(a.P2 + mi.cmat, a.K2 + mi.cmat);
+  }
+#undef TF_KADD_C
+#undef TF_KADD_D
+}
+
+// Per-class counters of a launch, summed over the warp: primitive quartets, and
+// contracted (member) quartets of the FP64 or the FP32 buckets.
+__device__ __forceinline__ void count_quartets(const JKArgs& a, int cls, unsigned long long nprim,
+                                               unsigned long long nq) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nprim += __shfl_xor_sync(0xffffffffu, nprim, o);
+    nq += __shfl_xor_sync(0xffffffffu, nq, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (nprim) atomicAdd(a.prim_count + cls, nprim);
+    if (nq) atomicAdd(a.qcount + (a.bucket32 ? NQCLS : 0) + cls, nq);
+  }
+}
+
+// One thread per contracted quartet.  MB = 1: a list entry is one quartet.  MB > 1
+// (family groups): a list entry is a bra family (its first member's pair id) with a
+// ket, and the mask of the members whose quartet passed the screen; the primitive
+// loop runs once for all members (accumulate_esfs_fam), then each member quartet of
+// the mask is transferred and digested with its own Cartesian offsets and
+// coincidence factors (molecule.fock.foo:1296-1300).
+template <int LA, int LB, int LC, int LD, typename T, int V, int MB>
 __global__ void __launch_bounds__(jk_threads<LA, LB, LC, LD, V>(), 1) k_jk(JKArgs a) {
   using Q = Quartet<LA, LB, LC, LD>;
   using RS = RysSmem<Q::NROOT>;
   extern __shared__ double rys_tab[];
   RS::load(rys_tab);
   __syncthreads();
-  unsigned long long nprim = 0;
+  unsigned long long nprim = 0, nquart = 0;
   const int2* quartets = a.quartets;
   long long nq = a.n;
+  long long qoff = 0;
   resolve_range(a.range, a.base, a.cap, quartets, nq);
+  qoff = quartets - a.quartets;                      // offset of this launch's entries in the mask array
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long n_pad = (nq + 31) / 32 * 32;      // whole warps stay in the loop together
-  const int lane = threadIdx.x & 31;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n_pad; t += stride) {
     // lanes past the end repeat the last quartet with weight 0, so that whole warps
     // take part in the warp reductions below
     const bool active = t < nq;
-    const int2 qd = quartets[active ? t : nq - 1];
+    const long long te = active ? t : nq - 1;
+    const int2 qd = quartets[te];
     const PairJK b = load_pair_jk(a.jkrec, a.pairR, qd.x);
     const PairJK k = load_pair_jk(a.jkrec, a.pairR, qd.y);
     const bool any_same = b.atom_hi == b.atom_lo || k.atom_hi == k.atom_lo || b.atom_hi == k.atom_hi ||
@@ -516,194 +801,48 @@ __global__ void __launch_bounds__(jk_threads<LA, LB, LC, LD, V>(), 1) k_jk(JKArg
     const PrimPair* kp = any_same ? a.prim_full + k.full_off : a.prim_skip + k.skip_off;
     const int nbp = any_same ? b.n_full : b.n_skip;
     const int nkp = any_same ? k.n_full : k.n_skip;
-    if (active) nprim += (unsigned long long)nbp * nkp;
-    double f = active ? 1.0 : 0.0;
-    if (b.same) f *= 0.5;
-    if (k.same) f *= 0.5;
-    if (qd.x == qd.y) f *= 0.5;
     const double Rab[3] = {b.Rx, b.Ry, b.Rz};
     const double Rcd[3] = {k.Rx, k.Ry, k.Rz};
-    double I[Q::NA][Q::NB][Q::NC * Q::ND];
-    quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I, rys_tab);
-
-    // The lists are bra-major, so the lanes of a warp usually share the bra pair:
-    // then J(ab) is summed over the warp and added once, and P(ab) is a broadcast.
-    // Otherwise the lanes of one bra are neighbours (a bra's kets of one cost bucket
-    // are consecutive) and J(ab) is summed over each run of equal bras by a segmented
-    // warp scan, then added by the run's last lane.
-    const bool uni = __all_sync(0xffffffffu, qd.x == __shfl_sync(0xffffffffu, qd.x, 0));
-    const unsigned lt_mask = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-    // (every lane executes the shuffle: none may be skipped by a short-circuit)
-    const int upx = __shfl_up_sync(0xffffffffu, qd.x, 1);
-    const bool headx = lane == 0 || qd.x != upx;
-    const unsigned heada = __ballot_sync(0xffffffffu, headx);
-    const int sega = 31 - __clz(heada & lt_mask);
-    const bool taila = lane == 31 || ((heada >> (lane + 1)) & 1u);
     const MolInfo mi = a.mols[b.mol];
-    const int n = mi.n_cart;
-    const int oa = b.cart_hi, ob = b.cart_lo, oc = k.cart_hi, od = k.cart_lo;
-    // J(ab) += f sum_cd I P(cd);  J(cd) += f sum_ab I P(ab)  (per spin when unrestricted)
-    auto digest_j = [&](const double* __restrict__ P, double* __restrict__ Jm) {
-      double Pcd[Q::NC][Q::ND];
+    double fk = 1.0;
+    if (k.same) fk *= 0.5;
+    if constexpr (MB == 1) {
+      if (active) { nprim += (unsigned long long)nbp * nkp; nquart += 1; }
+      double f = active ? fk : 0.0;
+      if (b.same) f *= 0.5;
+      if (qd.x == qd.y) f *= 0.5;
+      double I[Q::NA][Q::NB][Q::NC * Q::ND];
+      quartet_integrals<LA, LB, LC, LD, T>(bp, nbp, kp, nkp, Rab, Rcd, I, rys_tab);
+      digest_jk<LA, LB, LC, LD, V>(a, mi, I, f, qd.x, b.cart_hi, b.cart_lo, k.cart_hi, k.cart_lo);
+    } else {
+      const unsigned mask = active ? a.qmask[qoff + te] : 0u;
+      nprim += (unsigned long long)nbp * nkp * __popc(mask);
+      nquart += __popc(mask);
+      const int4 mv = a.fam_mem[qd.x];
+      const int mid[4] = {mv.x, mv.y, mv.z, mv.w};
+      PairJK bm[MB];
+      const PrimPair* bmp[MB];
 #pragma unroll
-      for (int c = 0; c < Q::NC; ++c)
-#pragma unroll
-        for (int d = 0; d < Q::ND; ++d) Pcd[c][d] = __ldg(P + (size_t)(oc + c) * n + od + d);
-#pragma unroll
-      for (int ia = 0; ia < Q::NA; ++ia)
-#pragma unroll
-        for (int ib = 0; ib < Q::NB; ++ib) {
-          double s = 0.0;
-#pragma unroll
-          for (int c = 0; c < Q::NC; ++c)
-#pragma unroll
-            for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pcd[c][d];
-          s *= f;
-          if (uni) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
-          } else {                       // idle lanes join the last run with s = 0
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-              const double t = __shfl_up_sync(0xffffffffu, s, o);
-              if (lane - o >= sega) s += t;
-            }
-            if (taila && s != 0.0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
-          }
-        }
-      if (active) {
-        double Pab[Q::NA][Q::NB];
-#pragma unroll
-        for (int ia = 0; ia < Q::NA; ++ia)
-#pragma unroll
-          for (int ib = 0; ib < Q::NB; ++ib) Pab[ia][ib] = __ldg(P + (size_t)(oa + ia) * n + ob + ib);
-#pragma unroll
-        for (int c = 0; c < Q::NC; ++c)
-#pragma unroll
-          for (int d = 0; d < Q::ND; ++d) {
-            double s = 0.0;
-#pragma unroll
-            for (int ia = 0; ia < Q::NA; ++ia)
-#pragma unroll
-              for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
-            atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
-          }
+      for (int m = 0; m < MB; ++m) {
+        bm[m] = load_pair_jk(a.jkrec, a.pairR, mid[m] >= 0 ? mid[m] : qd.x);
+        bmp[m] = mid[m] < 0 ? nullptr : (any_same ? a.prim_full + bm[m].full_off : a.prim_skip + bm[m].skip_off);
       }
-    };
-    if (a.want & 1) {                    // uniform over the warp (the J(ab) sums shuffle)
-      digest_j(a.P + mi.cmat, a.J + mi.cmat);
-      if (a.P2) digest_j(a.P2 + mi.cmat, a.J2 + mi.cmat);
+      T esfs[MB][Q::NE][Q::NF];
+      accumulate_esfs_fam<LA, LB, LC, LD, T, MB>(bp, nbp, kp, nkp, bmp, esfs, rys_tab);
+#pragma unroll
+      for (int m = 0; m < MB; ++m) {
+        if (!__any_sync(0xffffffffu, (mask >> m) & 1u)) continue;      // uniform over the warp
+        double f = ((mask >> m) & 1u) ? fk : 0.0;
+        if (bm[m].same) f *= 0.5;
+        if (mid[m] == qd.y) f *= 0.5;
+        double I[Q::NA][Q::NB][Q::NC * Q::ND];
+        hrr_quartet<LA, LB, LC, LD, T>(esfs[m], Rab, Rcd, I);
+        digest_jk<LA, LB, LC, LD, V>(a, mi, I, f, mid[m] >= 0 ? mid[m] : qd.x, bm[m].cart_hi, bm[m].cart_lo,
+                                     k.cart_hi, k.cart_lo);
+      }
     }
-    // K(ac) += f sum_bd I P(bd);  K(ad) += f sum_bc I P(bc)
-    // K(bc) += f sum_ad I P(ad);  K(bd) += f sum_ac I P(ac)
-    // (twice for an unrestricted build: alpha and beta densities)
-    // Variant bit 2: the K rows a and b are the same for all lanes of one bra, and
-    // lanes whose kets share the c (or d) shell add to the same K elements.  Such
-    // lanes are neighbours (pair-id order), so each run of equal (bra, shell) keys
-    // is summed with a segmented warp scan and added once, by its last lane.
-    constexpr bool SEG = (V & 2) != 0;
-    int segc = lane, segd = lane;
-    bool tailc = true, taild = true;
-    if constexpr (SEG) {
-      // (every lane executes both shuffles: none may be skipped by a short-circuit)
-      const int upc = __shfl_up_sync(0xffffffffu, oc, 1), upd = __shfl_up_sync(0xffffffffu, od, 1);
-      const unsigned headc = __ballot_sync(0xffffffffu, headx || oc != upc);
-      const unsigned headd = __ballot_sync(0xffffffffu, headx || od != upd);
-      segc = 31 - __clz(headc & lt_mask);
-      segd = 31 - __clz(headd & lt_mask);
-      tailc = lane == 31 || ((headc >> (lane + 1)) & 1u);
-      taild = lane == 31 || ((headd >> (lane + 1)) & 1u);
-    }
-    auto kadd = [&](double* addr, double v, int seg, bool tail) {
-      if constexpr (SEG) {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const double t = __shfl_up_sync(0xffffffffu, v, o);
-          if (lane - o >= seg) v += t;
-        }
-        if (tail && v != 0.0) atomicAdd(addr, v);
-      } else {
-        atomicAdd(addr, v);
-      }
-    };
-#define TF_KADD_C(addr, v) kadd((addr), (v), segc, tailc)
-#define TF_KADD_D(addr, v) kadd((addr), (v), segd, taild)
-    auto digest_k = [&](const double* __restrict__ P, double* __restrict__ Km) {
-      double Pbd[Q::NB][Q::ND], Pbc[Q::NB][Q::NC];
-      double Kbc[Q::NB][Q::NC], Kbd[Q::NB][Q::ND];
-#pragma unroll
-      for (int ib = 0; ib < Q::NB; ++ib) {
-#pragma unroll
-        for (int c = 0; c < Q::NC; ++c) Kbc[ib][c] = 0.0;
-#pragma unroll
-        for (int d = 0; d < Q::ND; ++d) Kbd[ib][d] = 0.0;
-      }
-#pragma unroll
-      for (int ib = 0; ib < Q::NB; ++ib) {
-#pragma unroll
-        for (int d = 0; d < Q::ND; ++d) Pbd[ib][d] = __ldg(P + (size_t)(ob + ib) * n + od + d);
-#pragma unroll
-        for (int c = 0; c < Q::NC; ++c) Pbc[ib][c] = __ldg(P + (size_t)(ob + ib) * n + oc + c);
-      }
-#pragma unroll
-      for (int ia = 0; ia < Q::NA; ++ia) {
-        double Pad[Q::ND], Pac[Q::NC];
-#pragma unroll
-        for (int d = 0; d < Q::ND; ++d) Pad[d] = __ldg(P + (size_t)(oa + ia) * n + od + d);
-#pragma unroll
-        for (int c = 0; c < Q::NC; ++c) Pac[c] = __ldg(P + (size_t)(oa + ia) * n + oc + c);
-#pragma unroll
-        for (int c = 0; c < Q::NC; ++c) {
-          double s = 0.0;
-#pragma unroll
-          for (int ib = 0; ib < Q::NB; ++ib)
-#pragma unroll
-            for (int d = 0; d < Q::ND; ++d) s += I[ia][ib][c * Q::ND + d] * Pbd[ib][d];
-          TF_KADD_C(Km + (size_t)(oa + ia) * n + oc + c, f * s);
-        }
-#pragma unroll
-        for (int d = 0; d < Q::ND; ++d) {
-          double s = 0.0;
-#pragma unroll
-          for (int ib = 0; ib < Q::NB; ++ib)
-#pragma unroll
-            for (int c = 0; c < Q::NC; ++c) s += I[ia][ib][c * Q::ND + d] * Pbc[ib][c];
-          TF_KADD_D(Km + (size_t)(oa + ia) * n + od + d, f * s);
-        }
-#pragma unroll
-        for (int ib = 0; ib < Q::NB; ++ib) {
-#pragma unroll
-          for (int c = 0; c < Q::NC; ++c)
-#pragma unroll
-            for (int d = 0; d < Q::ND; ++d) Kbc[ib][c] += I[ia][ib][c * Q::ND + d] * Pad[d];
-#pragma unroll
-          for (int d = 0; d < Q::ND; ++d)
-#pragma unroll
-            for (int c = 0; c < Q::NC; ++c) Kbd[ib][d] += I[ia][ib][c * Q::ND + d] * Pac[c];
-        }
-      }
-      // K(bc), K(bd): summed over the a components first, one atomic per element
-#pragma unroll
-      for (int ib = 0; ib < Q::NB; ++ib) {
-#pragma unroll
-        for (int c = 0; c < Q::NC; ++c) TF_KADD_C(Km + (size_t)(ob + ib) * n + oc + c, f * Kbc[ib][c]);
-#pragma unroll
-        for (int d = 0; d < Q::ND; ++d) TF_KADD_D(Km + (size_t)(ob + ib) * n + od + d, f * Kbd[ib][d]);
-      }
-    };
-    // with segmented sums every lane takes part (idle lanes add f = 0)
-    if ((SEG || active) && (a.want & 2)) {
-      digest_k(a.P + mi.cmat, a.K + mi.cmat);
-      if (a.P2) digest_k(a.P2 + mi.cmat, a.K2 + mi.cmat);
-    }
-#undef TF_KADD_C
-#undef TF_KADD_D
   }
-  // primitive-quartet counter (per class, one atomic per warp)
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) nprim += __shfl_xor_sync(0xffffffffu, nprim, o);
-  if ((threadIdx.x & 31) == 0 && nprim) atomicAdd(a.prim_count + qclass_id(LA, LB, LC, LD), nprim);
+  count_quartets(a, qclass_id(LA, LB, LC, LD), nprim, nquart);
 }
 
 // ---------------------------------------------------------------------------
@@ -781,7 +920,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
   long long nq = a.n;
   resolve_range(a.range, a.base, a.cap, quartets, nq);
   const int NA = ncart(la), NB = ncart(lb), NC = ncart(lc), ND = ncart(ld), NCD = NC * ND;
-  unsigned long long nprim = 0;
+  unsigned long long nprim = 0, nquart = 0;
   for (long long t = gw; t < nq; t += nwarps) {
     const int2 qd = quartets[t];
     const PairJK b = load_pair_jk(a.jkrec, a.pairR, qd.x);
@@ -858,9 +997,13 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
     };
     digest(a.P + mi.cmat, a.J + mi.cmat, a.K + mi.cmat);
     if (a.P2) digest(a.P2 + mi.cmat, a.J2 + mi.cmat, a.K2 + mi.cmat);
+    nquart += 1;
     __syncwarp();                        // the next quartet reuses the scratch
   }
-  if (lane == 0 && nprim) atomicAdd(a.prim_count + qclass_id(la, lb, lc, ld), nprim);
+  if (lane == 0) {
+    if (nprim) atomicAdd(a.prim_count + qclass_id(la, lb, lc, ld), nprim);
+    if (nquart) atomicAdd(a.qcount + (a.bucket32 ? NQCLS : 0) + qclass_id(la, lb, lc, ld), nquart);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1294,7 +1437,7 @@ struct DBuf {
 // read back after a build; pinned so that a captured graph can copy into them).
 struct PinnedStage {
   long long* goff = nullptr;                 // 3 per group, then the list length
-  unsigned long long* pc = nullptr;          // tf::NQCLS class counters, then the non-finite-density flag
+  unsigned long long* pc = nullptr;          // tf::BUILD_COUNTERS (see there)
   size_t n_goff = 0;
   ~PinnedStage() {
     if (goff) cudaFreeHost(goff);
@@ -1302,7 +1445,7 @@ struct PinnedStage {
   }
   cudaError_t reserve(size_t ng3) {
     if (!pc) {
-      cudaError_t e = cudaMallocHost(&pc, (tf::NQCLS + 1) * sizeof(unsigned long long));
+      cudaError_t e = cudaMallocHost(&pc, tf::BUILD_COUNTERS * sizeof(unsigned long long));
       if (e != cudaSuccess) return e;
     }
     if (ng3 <= n_goff && goff) return cudaSuccess;
@@ -1345,6 +1488,8 @@ struct tf_ctx {
   std::vector<tf::CPUnit> units;
   std::vector<int> unit_group, group_task0;
   std::vector<int2> group_cls;                           // (bra class, ket class) of each group
+  std::vector<int> group_fam;                            // bra-family capacity of each group's kernel (1: none)
+  tf::PairFamilies fams;                                 // shell-pair families (host)
   long long n_tasks = 0;
   long long list_budget = 1LL << 30;                     // quartets per list chunk (8 B each)
   // screening record: one byte per candidate (bra task, ket) pair, when it fits
@@ -1358,6 +1503,11 @@ struct tf_ctx {
   tf::DBuf<double> d_xyz, d_exps, d_coefs, d_P, d_Pc, d_Jc, d_Kc, d_J, d_K, d_H, d_pmax, d_sorted_imax, d_sorted_bmax;
   tf::DBuf<double> d_PcB, d_JcB, d_KcB, d_Pb, d_Jb, d_Kb;  // unrestricted builds (allocated on first use)
   tf::DBuf<double> d_wscratch;                             // f shells: per-warp scratch of the warp path
+  tf::DBuf<int> d_csorted, d_cxstart, d_cn;                // collapsed (family) class lists
+  tf::DBuf<double> d_cimax;
+  tf::DBuf<int4> d_fam_mem;                                // family members of every pair
+  tf::DBuf<unsigned char> d_qmask;                         // per list entry: the bra members it holds
+  tf::DBuf<unsigned long long> d_qcount;                   // member quartets per class, FP64 then FP32
   long long wscratch_warps = 0;
   tf::DBuf<int> d_shell_atom, d_shell_nprim, d_shell_poff, d_shell_l, d_shell_first_bf, d_shell_nbf, d_shell_cart;
   tf::DBuf<int> d_cart_shell, d_cart_local, d_bf_shell, d_bf_local, d_sorted, d_schwarz_ids;
@@ -1481,23 +1631,106 @@ static void append_pair_records(int m, int shell0, int n_shell, const int* shell
     }
 }
 
-// Each (molecule, class) list in I_max bands (half decades, largest first) and by
-// pair id inside a band.  The list kernels stop a bra's ket scan at the first band
-// whose largest I_max fails the screen, and the pair-id order inside a band puts
-// neighbouring shells on neighbouring lanes, so the ERI kernels' pair, primitive,
-// density and Fock accesses of a warp fall on few cache lines.
+// Shell-pair families.  Two shells of one atom with the same l and the same
+// primitive exponents (cc-pVDZ's oxygen 1s and 2s: eight exponents, two
+// contractions; Tonto stores them as two segmented shells) form a shell family.
+// The pairs (a', b') with a' in the family of a and b' in that of b then have the
+// same positioned primitive pairs, up to the contraction coefficients, so a kernel
+// can evaluate each primitive quartet once for all of them and weight it with
+// each member's coefficients.  Families have at most two shells (consecutive
+// members of a larger group pair up), a pair family at most four members.
 
+// shell_* arrays global over the context; prim_off[s]: first primitive of shell s in exps.
+static void make_pair_families(const std::vector<PairRec>& pairs, int n_mol, const std::vector<long long>& mol_pair0,
+                               const int* mol_shell0, const int* mol_nshell, const int* shell_l, const int* shell_atom,
+                               const int* shell_nprim, const int* prim_off, const double* exps, PairFamilies& F) {
+  const size_t np = pairs.size();
+  F.rep.resize(np);
+  F.index.assign(np, 0);
+  F.members.assign(np, make_int4(-1, -1, -1, -1));
+  F.n.assign(np, 1);
+  for (size_t p = 0; p < np; ++p) { F.rep[p] = (int)p; F.members[p].x = (int)p; }
+  auto same_exps = [&](int s, int t) {
+    if (shell_l[s] != shell_l[t] || shell_atom[s] != shell_atom[t] || shell_nprim[s] != shell_nprim[t]) return false;
+    for (int k = 0; k < shell_nprim[s]; ++k)
+      if (exps[prim_off[s] + k] != exps[prim_off[t] + k]) return false;
+    return true;
+  };
+  for (int m = 0; m < n_mol; ++m) {
+    const int s0 = mol_shell0[m], ns = mol_nshell[m];
+    std::vector<int> partner(ns, -1), done(ns, 0);
+    for (int u = 0; u < ns; ++u) {
+      if (done[u]) continue;
+      std::vector<int> grp{u};
+      for (int v = u + 1; v < ns; ++v)
+        if (!done[v] && same_exps(s0 + u, s0 + v)) grp.push_back(v);
+      for (int v : grp) done[v] = 1;
+      for (size_t k = 0; k + 1 < grp.size(); k += 2) { partner[grp[k]] = grp[k + 1]; partner[grp[k + 1]] = grp[k]; }
+    }
+    const long long base = mol_pair0[m];
+    auto pid = [&](int x, int y) { const int hi = std::max(x, y), lo = std::min(x, y); return base + (long long)hi * (hi + 1) / 2 + lo; };
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b <= a; ++b) {
+        const long long p = pid(a, b);
+        if (partner[a] < 0 && partner[b] < 0) continue;
+        std::vector<long long> mem;
+        for (int x : {a, partner[a]})
+          for (int y : {b, partner[b]})
+            if (x >= 0 && y >= 0) mem.push_back(pid(x, y));
+        std::sort(mem.begin(), mem.end());
+        mem.erase(std::unique(mem.begin(), mem.end()), mem.end());
+        if (mem.size() < 2 || mem.size() > 4) continue;
+        // members must share the positioned primitive pairs: the same atoms, angular
+        // momenta and exponents of the higher-l shell and of the other shell
+        const PairRec& r0 = pairs[mem[0]];
+        bool ok = true;
+        for (long long q : mem) {
+          const PairRec& rq = pairs[q];
+          if (rq.atom_hi != r0.atom_hi || rq.atom_lo != r0.atom_lo || !same_exps(rq.sh_hi, r0.sh_hi) ||
+              !same_exps(rq.sh_lo, r0.sh_lo) || rq.n_full != r0.n_full)
+            ok = false;
+        }
+        if (!ok) continue;
+        int4 mv = make_int4(-1, -1, -1, -1);
+        int* mp = &mv.x;
+        for (size_t k = 0; k < mem.size(); ++k) mp[k] = (int)mem[k];
+        for (size_t k = 0; k < mem.size(); ++k) {
+          F.rep[mem[k]] = (int)mem[0];
+          F.index[mem[k]] = (int)k;
+          F.members[mem[k]] = mv;
+          F.n[mem[k]] = (int)mem.size();
+        }
+      }
+  }
+}
+
+// Each (molecule, class) list in I_max bands (half decades, largest first) and by
+// pair id inside a band, the members of a family next to each other (the family
+// placed by its largest I_max).  The list kernels stop a bra's ket scan at the first
+// band whose largest I_max fails the screen, and the pair-id order inside a band
+// puts neighbouring shells on neighbouring lanes, so the ERI kernels' pair,
+// primitive, density and Fock accesses of a warp fall on few cache lines.  The
+// collapsed lists hold one entry per family.
 static void make_class_lists(const std::vector<PairRec>& pairs, const std::vector<int>& pair_cls, int n_mol,
-                             ClassLists& L) {
+                             const PairFamilies& F, ClassLists& L) {
   const long long n_pairs = (long long)pairs.size();
-  L.sorted.clear(); L.simax.clear(); L.sbmax.clear();
+  L = ClassLists{};
   L.cls_n.assign((size_t)n_mol * NPAIRCLS, 0);
   L.cls_off.assign((size_t)n_mol * NPAIRCLS, 0);
+  L.cls_cn.assign((size_t)n_mol * NPAIRCLS, 0);
+  L.cls_coff.assign((size_t)n_mol * NPAIRCLS, 0);
+  L.cls_maxm.assign((size_t)n_mol * NPAIRCLS, 1);
   std::vector<std::vector<int>> lists((size_t)n_mol * NPAIRCLS);
-  for (long long p = 0; p < n_pairs; ++p) lists[(size_t)pairs[p].mol * NPAIRCLS + pair_cls[p]].push_back((int)p);
-  std::vector<int> band_of(n_pairs);                  // half-decade band of each pair, computed once
+  for (long long p = 0; p < n_pairs; ++p)
+    if (F.rep[p] == p) lists[(size_t)pairs[p].mol * NPAIRCLS + pair_cls[p]].push_back((int)p);
+  std::vector<double> fmax(n_pairs, 0.0);             // largest I_max of each family (at its first member)
+  std::vector<int> band_of(n_pairs);                  // half-decade band of each family
   for (long long p = 0; p < n_pairs; ++p) {
-    const double v = pairs[p].imax;
+    const int r = F.rep[p];
+    fmax[r] = std::max(fmax[r], pairs[p].imax);
+  }
+  for (long long p = 0; p < n_pairs; ++p) {
+    const double v = fmax[p];
     band_of[p] = v > 0.0 ? (int)std::floor(2.0 * std::log10(v)) : -1000000;
   }
   L.sorted.reserve(n_pairs);
@@ -1510,28 +1743,60 @@ static void make_class_lists(const std::vector<PairRec>& pairs, const std::vecto
       return bx != by ? bx > by : x < y;
     });
     L.cls_off[q] = (int)L.sorted.size();
-    L.cls_n[q] = (int)v.size();
+    L.cls_coff[q] = (int)L.csorted.size();
+    L.cls_cn[q] = (int)v.size();
     for (size_t i = 0; i < v.size();) {
       size_t e = i;
       double bm = 0.0;
-      while (e < v.size() && band_of[v[e]] == band_of[v[i]]) bm = std::max(bm, pairs[v[e++]].imax);
-      for (; i < e; ++i) { L.sorted.push_back(v[i]); L.simax.push_back(pairs[v[i]].imax); L.sbmax.push_back(bm); }
+      while (e < v.size() && band_of[v[e]] == band_of[v[i]]) bm = std::max(bm, fmax[v[e++]]);
+      for (; i < e; ++i) {
+        const int r = v[i];
+        L.csorted.push_back(r);
+        L.cimax.push_back(fmax[r]);
+        L.cxstart.push_back((int)L.sorted.size() - L.cls_off[q]);
+        L.cn.push_back(F.n[r]);
+        L.cls_maxm[q] = std::max(L.cls_maxm[q], F.n[r]);
+        const int* mp = &F.members[r].x;
+        for (int k = 0; k < F.n[r]; ++k) {
+          L.sorted.push_back(mp[k]);
+          L.simax.push_back(pairs[mp[k]].imax);
+          L.sbmax.push_back(bm);
+        }
+      }
     }
+    L.cls_n[q] = (int)L.sorted.size() - L.cls_off[q];
   }
+}
+
+// Members a kernel of the class pair (bra class p1, ket class p2) can evaluate at once
+// from one bra family (its accumulator capacity): the thread-kernel classes whose
+// bra has an s shell; 1 elsewhere (family quartets are then listed member by member).
+static int family_capacity(int p1, int p2) {
+  int lh1 = 0; while ((lh1 + 1) * (lh1 + 2) / 2 <= p1) ++lh1;
+  const int ll1 = p1 - lh1 * (lh1 + 1) / 2;
+  int lh2 = 0; while ((lh2 + 1) * (lh2 + 2) / 2 <= p2) ++lh2;
+  const int ll2 = p2 - lh2 * (lh2 + 1) / 2;
+  return fam_cap_l(lh1, ll1, lh2, ll2);
 }
 
 // Bra tasks: groups (class pairs p1 >= p2) of units (one per molecule having both
 // classes); a task is (unit, bra position) and covers the kets of class p2 (for
-// p1 == p2 those at positions up to the bra's own).  With n_shards > 1 every task
-// gets an estimated cost and the tasks are dealt to the shards largest first, each
-// to the least-loaded shard (longest-processing-time rule), so that the shards'
-// FLOPs, not their task counts, come out even.  The estimate: the kets of the
-// task's bands that pass the Schwarz bound I_max(bra) I_max(ket) > cutoff at a unit
-// density maximum, times the primitive quartets and the per-class FLOP model.
+// p1 == p2 those at positions up to the bra's own).  In a family group (the class
+// pair's kernel takes bra families, family_capacity, and some bra family has several
+// members) the bra positions are those of the collapsed list: one task per bra
+// family, whose kets are those of its members (for p1 == p2 up to the end of the
+// family's own block, the ket members of that block paired with the bra members at or
+// after them).  With n_shards > 1 every task gets an estimated cost and the tasks
+// are dealt to the shards largest first, each to the least-loaded shard
+// (longest-processing-time rule), so that the shards' FLOPs, not their task counts,
+// come out even.  The estimate: the kets of the task's bands that pass the Schwarz
+// bound I_max(bra) I_max(ket) > cutoff at a unit density maximum, times the
+// primitive quartets and the per-class FLOP model.
 struct TaskPlan {
   std::vector<CPUnit> units;
   std::vector<int> unit_group;
   std::vector<int2> group_cls;             // (bra class, ket class) of each group
+  std::vector<int> group_fam;              // bra-family capacity of each group's kernel (1: none)
   std::vector<int2> tasks;                 // every task, group by group
   std::vector<int> task_group;
   std::vector<double> cost;                // estimated FLOPs (n_shards > 1)
@@ -1546,11 +1811,21 @@ static void make_task_plan(const ClassLists& L, const std::vector<PairRec>& pair
     for (int p2 = 0; p2 <= p1; ++p2) {
       const int g = (int)T.group_cls.size();
       T.group_cls.push_back(make_int2(p1, p2));
+      // a family group when the kernel takes bra families and some bra family has
+      // several members, none more than the kernel holds
+      const int cap = family_capacity(p1, p2);
+      int maxm = 1;
+      for (int m = 0; m < n_mol; ++m)
+        if (L.cls_n[m * NPAIRCLS + p2] > 0) maxm = std::max(maxm, L.cls_maxm[m * NPAIRCLS + p1]);
+      const bool fam = cap >= 2 && maxm >= 2 && maxm <= cap;
+      T.group_fam.push_back(fam ? cap : 1);
       for (int m = 0; m < n_mol; ++m) {
-        const int n1 = L.cls_n[m * NPAIRCLS + p1], n2 = L.cls_n[m * NPAIRCLS + p2];
+        const int q1 = m * NPAIRCLS + p1, q2 = m * NPAIRCLS + p2;
+        const int n1 = fam ? L.cls_cn[q1] : L.cls_n[q1], n2 = L.cls_n[q2];
         if (n1 == 0 || n2 == 0) continue;
         const int u = (int)T.units.size();
-        T.units.push_back(CPUnit{p1, p2, L.cls_off[m * NPAIRCLS + p1], L.cls_off[m * NPAIRCLS + p2], n2, m});
+        T.units.push_back(CPUnit{p1, p2, fam ? L.cls_coff[q1] : L.cls_off[q1], L.cls_off[q2], n2, m, fam ? 1 : 0,
+                                 L.cls_off[q1]});
         T.unit_group.push_back(g);
         for (int i = 0; i < n1; ++i) {
           T.tasks.push_back(make_int2(u, i));
@@ -1572,8 +1847,9 @@ static void make_task_plan(const ClassLists& L, const std::vector<PairRec>& pair
     int lh1, ll1, lh2, ll2;
     lh1 = 0; while ((lh1 + 1) * (lh1 + 2) / 2 <= u.p1) ++lh1; ll1 = u.p1 - lh1 * (lh1 + 1) / 2;
     lh2 = 0; while ((lh2 + 1) * (lh2 + 2) / 2 <= u.p2) ++lh2; ll2 = u.p2 - lh2 * (lh2 + 1) / 2;
-    const double Ib = L.simax[u.bra_off + i];
-    const int jend = (u.p1 == u.p2) ? i + 1 : u.n_ket;
+    const double Ib = u.fam ? L.cimax[u.bra_off + i] : L.simax[u.bra_off + i];
+    const int bra = u.fam ? L.csorted[u.bra_off + i] : L.sorted[u.bra_off + i];
+    const int jend = (u.p1 == u.p2) ? (u.fam ? L.cxstart[u.bra_off + i] + L.cn[u.bra_off + i] : i + 1) : u.n_ket;
     // band maxima are non-increasing along the list: the passing kets are a prefix
     int lo = 0, hi = jend;
     while (lo < hi) {
@@ -1581,7 +1857,7 @@ static void make_task_plan(const ClassLists& L, const std::vector<PairRec>& pair
       if (Ib * L.sbmax[u.ket_off + mid] > cutoff) lo = mid + 1; else hi = mid;
     }
     const double nprim_kets = pref[u.ket_off + lo] - pref[u.ket_off];
-    const double nb = pairs[L.sorted[u.bra_off + i]].n_full;
+    const double nb = pairs[bra].n_full;
     T.cost[t] = class_flops(lh1, ll1, lh2, ll2, (double)lo, nb * nprim_kets) + 1.0;
   }
   std::vector<size_t> order(nt);
@@ -1607,6 +1883,7 @@ static int build_tasks(tf_ctx* c) {
   c->units = T.units;
   c->unit_group = T.unit_group;
   c->group_cls = T.group_cls;
+  c->group_fam = T.group_fam;
   c->group_task0.clear();
   c->shard_cost = T.shard_cost;
   std::vector<int2> tasks;
@@ -1628,7 +1905,10 @@ static int build_tasks(tf_ctx* c) {
   std::vector<long long> cand_off(tasks.size() + 1, 0);
   for (size_t t = 0; t < tasks.size(); ++t) {
     const CPUnit& u = c->units[tasks[t].x];
-    cand_off[t + 1] = cand_off[t] + (u.p1 == u.p2 ? tasks[t].y + 1 : u.n_ket);
+    const int i = tasks[t].y;
+    const long long nk = u.p1 != u.p2 ? u.n_ket
+                         : u.fam ? c->lists.cxstart[u.bra_off + i] + c->lists.cn[u.bra_off + i] : i + 1;
+    cand_off[t + 1] = cand_off[t] + nk;
   }
   c->use_cand = false;
   if (cand_off.back() <= c->cand_budget && c->d_cand.reserve(std::max<long long>(cand_off.back(), 1)) == cudaSuccess &&
@@ -1756,7 +2036,13 @@ static int setup_pairs(tf_ctx* c) {
     const PairRec& pr = c->pairs_h[p];
     c->max_I_tonto[c->mol_pair0[pr.mol] + pr.tonto_ab] = pr.imax;
   }
-  make_class_lists(c->pairs_h, c->pair_cls, c->n_mol, c->lists);
+  {
+    std::vector<int> shell0(c->n_mol), nshell(c->n_mol);
+    for (int m = 0; m < c->n_mol; ++m) { shell0[m] = c->mols[m].shell0; nshell[m] = c->mols[m].n_shell; }
+    make_pair_families(c->pairs_h, c->n_mol, c->mol_pair0, shell0.data(), nshell.data(), c->shell_l.data(),
+                       c->shell_atom.data(), c->shell_nprim.data(), c->shell_poff.data(), c->exps.data(), c->fams);
+  }
+  make_class_lists(c->pairs_h, c->pair_cls, c->n_mol, c->fams, c->lists);
   c->cls_n = c->lists.cls_n;
   c->cls_off = c->lists.cls_off;
   const std::vector<int>& sorted = c->lists.sorted;
@@ -1792,6 +2078,23 @@ static int setup_pairs(tf_ctx* c) {
     }
     srec[q] = make_int4(sh | (sl << 16), ah | (al << 16), pr.n_full | (pr.n_skip << 16), sorted[q]);
   }
+  {                                    // collapsed (family) lists and family members
+    const ClassLists& L = c->lists;
+    TF_CUDA(c->d_csorted.reserve(std::max<size_t>(L.csorted.size(), 1)));
+    TF_CUDA(c->d_cimax.reserve(std::max<size_t>(L.cimax.size(), 1)));
+    TF_CUDA(c->d_cxstart.reserve(std::max<size_t>(L.cxstart.size(), 1)));
+    TF_CUDA(c->d_cn.reserve(std::max<size_t>(L.cn.size(), 1)));
+    TF_CUDA(c->d_fam_mem.reserve(std::max<size_t>(c->fams.members.size(), 1)));
+    if (!L.csorted.empty()) {
+      TF_CUDA(cudaMemcpy(c->d_csorted.p, L.csorted.data(), L.csorted.size() * sizeof(int), cudaMemcpyHostToDevice));
+      TF_CUDA(cudaMemcpy(c->d_cimax.p, L.cimax.data(), L.cimax.size() * sizeof(double), cudaMemcpyHostToDevice));
+      TF_CUDA(cudaMemcpy(c->d_cxstart.p, L.cxstart.data(), L.cxstart.size() * sizeof(int), cudaMemcpyHostToDevice));
+      TF_CUDA(cudaMemcpy(c->d_cn.p, L.cn.data(), L.cn.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (!c->fams.members.empty())
+      TF_CUDA(cudaMemcpy(c->d_fam_mem.p, c->fams.members.data(), c->fams.members.size() * sizeof(int4),
+                         cudaMemcpyHostToDevice));
+  }
   TF_CUDA(c->d_srec.reserve(std::max<size_t>(srec.size(), 1)));
   TF_CUDA(cudaMemcpyAsync(c->d_srec.p, srec.data(), srec.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
   TF_CUDA(c->d_sorted.reserve(std::max<size_t>(sorted.size(), 1)));
@@ -1818,21 +2121,21 @@ static void class_l(int k, int& lh, int& ll) {
 
 // Launch set-up (shared-memory attribute, resident blocks per SM), done once per
 // kernel and before any graph capture: a zero-sized, range-less JKArgs only sets up.
-template <int LA, int LB, int LC, int LD, typename T, int V>
+template <int LA, int LB, int LC, int LD, typename T, int V, int MB>
 static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   constexpr int thr = jk_threads<LA, LB, LC, LD, V>();
   constexpr size_t smem = RysSmem<Quartet<LA, LB, LC, LD>::NROOT>::SIZE * sizeof(double);
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {
-    cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     {                                  // shared storage for one block, the rest to L1
       int dev = 0, per_sm = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
       const int pct = per_sm > 0 ? std::min(100, (int)((smem + 2048) * 100 / per_sm) + 1) : 100;
-      cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+      cudaFuncSetAttribute(k_jk<LA, LB, LC, LD, T, V, MB>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T, V>, thr, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jk<LA, LB, LC, LD, T, V, MB>, thr, smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   if (a.n <= 0 && !a.range) return;
@@ -1841,23 +2144,36 @@ static void launch_jk_t(const JKArgs& a, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const long long full = (long long)nsm * blocks_per_sm;
   const long long blocks = a.range ? full : std::min<long long>((a.n + thr - 1) / thr, full);
-  k_jk<LA, LB, LC, LD, T, V><<<(unsigned)blocks, thr, smem, s>>>(a);
+  k_jk<LA, LB, LC, LD, T, V, MB><<<(unsigned)blocks, thr, smem, s>>>(a);
 }
 
-template <int LA, int LB, int LC, int LD, int V>
+template <int LA, int LB, int LC, int LD, int V, int MB>
 static void launch_jk_v(const JKArgs& a, cudaStream_t s, bool fp32) {
-  if (fp32) launch_jk_t<LA, LB, LC, LD, float, V>(a, s);
-  else launch_jk_t<LA, LB, LC, LD, double, V>(a, s);
+  if (fp32) launch_jk_t<LA, LB, LC, LD, float, V, MB>(a, s);
+  else launch_jk_t<LA, LB, LC, LD, double, V, MB>(a, s);
 }
 
+template <int LA, int LB, int LC, int LD, int MB>
+static void launch_jk_m(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
+  switch (variant & 3) {
+    case 1: launch_jk_v<LA, LB, LC, LD, 1, MB>(a, s, fp32); break;
+    case 2: launch_jk_v<LA, LB, LC, LD, 2, MB>(a, s, fp32); break;
+    case 3: launch_jk_v<LA, LB, LC, LD, 3, MB>(a, s, fp32); break;
+    default: launch_jk_v<LA, LB, LC, LD, 0, MB>(a, s, fp32); break;
+  }
+}
+
+// The bra-family kernel of the class (family_capacity) when the launch is a family group.
 template <int LA, int LB, int LC, int LD>
 static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
-  switch (variant & 3) {
-    case 1: launch_jk_v<LA, LB, LC, LD, 1>(a, s, fp32); break;
-    case 2: launch_jk_v<LA, LB, LC, LD, 2>(a, s, fp32); break;
-    case 3: launch_jk_v<LA, LB, LC, LD, 3>(a, s, fp32); break;
-    default: launch_jk_v<LA, LB, LC, LD, 0>(a, s, fp32); break;
+  constexpr int CAP = fam_cap_l(LA, LB, LC, LD);
+  if constexpr (CAP > 1) {
+    if (a.fam > 1) {
+      launch_jk_m<LA, LB, LC, LD, CAP>(a, s, fp32, variant);
+      return;
+    }
   }
+  launch_jk_m<LA, LB, LC, LD, 1>(a, s, fp32, variant);
 }
 
 constexpr int GROUP_WPB = 4;
@@ -1888,7 +2204,8 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   const long long full = (long long)nsm * group_blocks_per_sm;
   const long long blocks = a.range ? full : std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
   GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count,
-              a.range, a.base, a.cap, a.jkrec, a.pairR, a.P2, a.J2, a.K2, a.want};
+              a.range, a.base, a.cap, a.jkrec, a.pairR, a.P2, a.J2, a.K2, a.want,
+              a.qcount ? a.qcount + (a.bucket32 ? NQCLS : 0) : nullptr};
   k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
   return TF_OK;
 }
@@ -1964,7 +2281,7 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   }
   TF_CUDA(cudaMemsetAsync(c->d_pglob.p, 0, c->n_mol * sizeof(unsigned long long), s));
   // per-class primitive counters and, after them, the non-finite-density flag
-  TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, (NQCLS + 1) * sizeof(unsigned long long), s));
+  TF_CUDA(cudaMemsetAsync(c->d_prim_count.p, 0, BUILD_COUNTERS * sizeof(unsigned long long), s));
   k_pmax<<<(unsigned)std::max<long long>(1, (ns2 + 255) / 256), 256, 0, s>>>(bt, dP, dPb, c->d_pmax.p, c->d_pglob.p,
                                                                              c->d_prim_count.p + NQCLS);
   kernels++;
@@ -1974,6 +2291,11 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
                 c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX,
                 c->use_cand ? c->d_cand.p : nullptr, c->d_task_cand_off.p, c->d_task_len.p};
   la.bad = c->d_prim_count.p + NQCLS;
+  la.csorted = c->d_csorted.p;
+  la.cimax = c->d_cimax.p;
+  la.cxstart = c->d_cxstart.p;
+  la.cn = c->d_cn.p;
+  la.qmask = c->d_qmask.p;
   const long long thr_list = LIST_THREADS;
   const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
   const long long nslots = c->n_tasks * NBUCKET;
@@ -2013,7 +2335,7 @@ static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, double* dJb, doub
   const int ng = (int)c->group_cls.size();
   TF_CUDA(cudaMemcpyAsync(c->pin->goff, c->d_group_offsets.p, (3 * ng + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
                           s));
-  TF_CUDA(cudaMemcpyAsync(c->pin->pc, c->d_prim_count.p, (NQCLS + 1) * sizeof(unsigned long long),
+  TF_CUDA(cudaMemcpyAsync(c->pin->pc, c->d_prim_count.p, BUILD_COUNTERS * sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, s));
   return TF_OK;
 }
@@ -2059,8 +2381,14 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
              c->d_jkrec.p, c->d_pairR.p, nullptr, nullptr, nullptr, want};
     a.wscratch = c->d_wscratch.p;
     a.wscratch_warps = c->wscratch_warps;
+    a.qmask = c->d_qmask.p;
+    a.fam_mem = c->d_fam_mem.p;
+    a.qcount = c->d_prim_count.p + NQCLS + 1;
+    a.fam = c->group_fam[g];
+    a.bucket32 = 0;
     JKArgs a32 = a;
     a32.range = c->d_group_offsets.p + 3 * g + 1;
+    a32.bucket32 = 1;
     rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false, c->cls_variant[g]);
     if (rc != TF_OK) return rc;
     kernels++;
@@ -2089,17 +2417,20 @@ static int finish_stats(tf_ctx* c, int kernels, bool graph) {
   }
   float ms_all = 0.f, ms_eri = 0.f;
   TF_CUDA(cudaEventElapsedTime(&ms_all, c->ev0, c->ev2));
-  double npq = 0.0, flops = 0.0;
-  long long n_fp32 = 0;
+  double npq = 0.0, flops = 0.0, n_all = 0.0, n_fp32 = 0.0;
   c->cls_stats.clear();
+  const unsigned long long* q64 = pc + NQCLS + 1;        // contracted (member) quartets per class
+  const unsigned long long* q32 = q64 + NQCLS;
   for (int g = 0; g < ng; ++g) {
-    const long long nq = goff[3 * g + 2] - goff[3 * g];
-    n_fp32 += goff[3 * g + 2] - goff[3 * g + 1];
-    if (nq == 0) continue;
+    if (goff[3 * g + 2] == goff[3 * g]) continue;       // no list entries
     int l1h, l1l, l2h, l2l;
     class_l(c->group_cls[g].x, l1h, l1l);
     class_l(c->group_cls[g].y, l2h, l2l);
-    const double p = (double)pc[qclass_id(l1h, l1l, l2h, l2l)];
+    const int cid = qclass_id(l1h, l1l, l2h, l2l);
+    const double nq = (double)q64[cid] + (double)q32[cid];
+    n_all += nq;
+    n_fp32 += (double)q32[cid];
+    const double p = (double)pc[cid];
     npq += p;
     const double fl = class_flops(l1h, l1l, l2h, l2l, (double)nq, p);
     flops += fl;
@@ -2118,8 +2449,8 @@ static int finish_stats(tf_ctx* c, int kernels, bool graph) {
   }
   c->stats.build_ms = ms_all;
   c->stats.eri_ms = graph ? ms_all : ms_eri;
-  c->stats.quartets = ng > 0 ? (double)goff[3 * (ng - 1) + 2] : 0.0;
-  c->stats.quartets_fp32 = (double)n_fp32;
+  c->stats.quartets = n_all;
+  c->stats.quartets_fp32 = n_fp32;
   c->stats.prim_quartets = npq;
   c->stats.flops = flops;
   c->stats.kernels = kernels;
@@ -2180,7 +2511,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
         int l1h, l1l, l2h, l2l;
         class_l(c->group_cls[g].x, l1h, l1l);
         class_l(c->group_cls[g].y, l2h, l2l);
-        const JKArgs none{};
+        JKArgs none{};
+        none.fam = c->group_fam[g];
         for (int fp32 = 0; fp32 < 2; ++fp32) {
           const int rc = dispatch_jk(l1h, l1l, l2h, l2l, none, s, fp32 != 0, c->cls_variant[g]);
           if (rc != TF_OK) return rc;
@@ -2246,6 +2578,17 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       return TF_ENOMEM;
     }
   }
+  // family groups: one member mask per list entry
+  if (std::any_of(c->group_fam.begin(), c->group_fam.end(), [](int v) { return v > 1; }) &&
+      c->d_qmask.n < c->d_quartets.n) {
+    drop_graph(c);                       // a captured build holds the old mask buffer
+    if (c->d_qmask.reserve(c->d_quartets.n) != cudaSuccess) {
+      cudaGetLastError();
+      c->graph_cap = 0;
+      set_error("quartet list masks do not fit in device memory");
+      return TF_ENOMEM;
+    }
+  }
   if (one_chunk && c->graph_cap != (long long)c->d_quartets.n) {
     drop_graph(c);
     c->graph_cap = (long long)c->d_quartets.n;
@@ -2262,6 +2605,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       lw.t_base = c->group_task0[g0];
       lw.n_tasks = c->group_task0[g1];
       lw.out_base = base;
+      lw.qmask = c->d_qmask.p;
       const unsigned grid_w =
           (unsigned)std::max<long long>(1, ((lw.n_tasks - lw.t_base) * 32 + thr_list - 1) / thr_list);
       if (c->use_cand)
@@ -2281,9 +2625,16 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
                dPb ? c->d_PcB.p : nullptr, dPb ? c->d_JcB.p : nullptr, dPb ? c->d_KcB.p : nullptr, want};
       a.wscratch = c->d_wscratch.p;
       a.wscratch_warps = c->wscratch_warps;
+      a.qmask = c->d_qmask.p + (goff[3 * g] - base);
+      a.fam_mem = c->d_fam_mem.p;
+      a.qcount = c->d_prim_count.p + NQCLS + 1;
+      a.fam = c->group_fam[g];
+      a.bucket32 = 0;
       JKArgs a32 = a;
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
+      a32.qmask = c->d_qmask.p + (goff[3 * g + 1] - base);
       a32.n = goff[3 * g + 2] - goff[3 * g + 1];
+      a32.bucket32 = 1;
       if (a.n > 0) {
         rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false, c->cls_variant[g]);
         if (rc != TF_OK) return rc;
@@ -2474,7 +2825,7 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
   if (c->d_P.reserve(nb2) || c->d_J.reserve(nb2) || c->d_K.reserve(nb2) || c->d_H.reserve(nb2) ||
       c->d_Pc.reserve(nc2) || c->d_Jc.reserve(nc2) || c->d_Kc.reserve(nc2) ||
       c->d_pmax.reserve((size_t)c->pmax_off[n_mol]) || c->d_pglob.reserve(n_mol) ||
-      c->d_prim_count.reserve(NQCLS + 1)) {
+      c->d_prim_count.reserve(BUILD_COUNTERS)) {
     tf_ctx_destroy(c); set_error("device allocation"); return TF_ENOMEM;
   }
   TF_TRY(setup_pairs(c));
@@ -2675,38 +3026,55 @@ int tf_set_shard(tf_ctx* c, int index, int count) {
 }
 
 int tf_plan_shards(const tf_basis* basis, const double* max_I, double schwarz_cutoff, int n_shards,
-                   long long* n_tasks, int* task_bra, int* task_ket_class, int* task_shard, int* pair_position,
-                   double* shard_cost) {
+                   long long* n_rows, int* row_bra, int* row_ket_class, int* row_ket_limit, int* row_shard,
+                   int* pair_position, double* shard_cost) {
   using namespace tf;
-  if (!basis || !max_I || !n_tasks || n_shards < 1 || !(schwarz_cutoff > 0.0)) {
+  if (!basis || !max_I || !n_rows || n_shards < 1 || !(schwarz_cutoff > 0.0)) {
     set_error("bad argument"); return TF_EINVAL;
   }
   int rc = validate_basis(basis);
   if (rc) return rc;
-  std::vector<int> shell_cart(basis->n_shell);
-  for (int s = 0, nc = 0; s < basis->n_shell; ++s) { shell_cart[s] = nc; nc += ncart(basis->shell_l[s]); }
+  const int ns = basis->n_shell;
+  std::vector<int> shell_cart(ns), prim_off(ns);
+  for (int s = 0, nc = 0, np = 0; s < ns; ++s) {
+    shell_cart[s] = nc; nc += ncart(basis->shell_l[s]);
+    prim_off[s] = np; np += basis->shell_nprim[s];
+  }
   std::vector<PairRec> pairs;
   std::vector<int> pcls;
   long long full_tot = 0;
-  append_pair_records(0, 0, basis->n_shell, basis->shell_l, basis->shell_atom, shell_cart.data(), basis->shell_nprim,
+  append_pair_records(0, 0, ns, basis->shell_l, basis->shell_atom, shell_cart.data(), basis->shell_nprim,
                       &full_tot, pairs, pcls);
   for (PairRec& pr : pairs) pr.imax = max_I[pr.tonto_ab];
+  PairFamilies F;
+  const std::vector<long long> mol_pair0{0, (long long)pairs.size()};
+  const int shell0 = 0;
+  make_pair_families(pairs, 1, mol_pair0, &shell0, &ns, basis->shell_l, basis->shell_atom, basis->shell_nprim,
+                     prim_off.data(), basis->exponents, F);
   ClassLists L;
-  make_class_lists(pairs, pcls, 1, L);
+  make_class_lists(pairs, pcls, 1, F, L);
   TaskPlan T;
   make_task_plan(L, pairs, 1, schwarz_cutoff, n_shards, T);
-  *n_tasks = (long long)T.tasks.size();
+  long long r = 0;
   for (size_t t = 0; t < T.tasks.size(); ++t) {
     const CPUnit& u = T.units[T.tasks[t].x];
-    if (task_bra) task_bra[t] = pairs[L.sorted[u.bra_off + T.tasks[t].y]].tonto_ab;
-    if (task_ket_class) task_ket_class[t] = u.p2;
-    if (task_shard) task_shard[t] = T.shard[t];
+    const int i = T.tasks[t].y;
+    const int nmem = u.fam ? L.cn[u.bra_off + i] : 1;
+    for (int k = 0; k < nmem; ++k, ++r) {
+      const int bra = u.fam ? L.sorted[u.bra_xoff + L.cxstart[u.bra_off + i] + k] : L.sorted[u.bra_off + i];
+      const int lim = u.p1 == u.p2 ? (u.fam ? L.cxstart[u.bra_off + i] + k : i) : u.n_ket - 1;
+      if (row_bra) row_bra[r] = pairs[bra].tonto_ab;
+      if (row_ket_class) row_ket_class[r] = u.p2;
+      if (row_ket_limit) row_ket_limit[r] = lim;
+      if (row_shard) row_shard[r] = T.shard[t];
+    }
   }
+  *n_rows = r;
   if (pair_position)
     for (int q = 0; q < NPAIRCLS; ++q)
       for (int i = 0; i < L.cls_n[q]; ++i) pair_position[pairs[L.sorted[L.cls_off[q] + i]].tonto_ab] = i;
   if (shard_cost)
-    for (int r = 0; r < n_shards; ++r) shard_cost[r] = T.shard_cost[r];
+    for (int k = 0; k < n_shards; ++k) shard_cost[k] = T.shard_cost[k];
   return TF_OK;
 }
 

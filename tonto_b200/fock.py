@@ -113,7 +113,7 @@ def load_library(path: Optional[str] = None):
     L.tf_schwarz.argtypes = [vp, P(d)]
     L.tf_ctx_destroy.argtypes = [vp]
     L.tf_debug_fail_alloc.argtypes = [i]
-    L.tf_plan_shards.argtypes = [P(_Basis), P(d), d, i, P(ctypes.c_longlong), P(i), P(i), P(i), P(i), P(d)]
+    L.tf_plan_shards.argtypes = [P(_Basis), P(d), d, i, P(ctypes.c_longlong), P(i), P(i), P(i), P(i), P(i), P(d)]
     L.tf_build_jk_f.argtypes = [vp, P(d), P(d), P(d), i, P(i)]
     L.tf_build_jk_f.restype = None
     L.tf_build_fock_f.argtypes = [vp, P(d), P(d), P(d), P(i)]
