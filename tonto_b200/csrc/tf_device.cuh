@@ -135,9 +135,12 @@ __host__ __device__ constexpr int gidx(int x, int y, int z) { return CT.first[x 
 // ---------------------------------------------------------------------------
 // data layouts shared with the host code
 // ---------------------------------------------------------------------------
-// One primitive pair (Gaussian product), positioned.  cc already holds
-// c_a c_b zeta^(-3/2) exp(-a b |AB|^2 / zeta) and, for bra-side use, nothing else:
-// the 2 pi^(5/2) factor is applied per primitive quartet.
+// One primitive pair (Gaussian product), positioned.  cc holds
+// c_a c_b zeta^(-1) exp(-a b |AB|^2 / zeta): the prefactor c_a c_b zeta^(-3/2) exp(...)
+// times sqrt(zeta), so that a primitive quartet's
+// 2 pi^(5/2) cc_ab zeta^(-3/2) cc_cd eta^(-3/2) sqrt(rho), rho = zeta eta / (zeta + eta),
+// becomes 2 pi^(5/2) cc_ab cc_cd / sqrt(zeta + eta): one reciprocal square root of
+// zeta + eta gives both it and 1/(zeta + eta) (its square).
 struct __align__(16) PrimPair {
   double Px, Py, Pz, zeta;
   double cc, half_zinv;              // prefactor, 1/(2 zeta)
@@ -486,14 +489,15 @@ __device__ __forceinline__ void prim_quartet_f32(const PrimRegs& B, const PrimRe
   constexpr int D1 = Q::LAB + 1, D2 = Q::LCD + 1, NR = Q::NROOT;
   const float zeta = (float)B.Z.y, eta = (float)K.Z.y;
   const float half_zinv = (float)B.C.y, half_einv = (float)K.C.y;
-  const float inv = rcp_f32(zeta + eta);
+  const float sq = rsqrt_f32(zeta + eta);
+  const float inv = sq * sq;
   const float rho = zeta * eta * inv;
   const float QP[3] = {(float)(K.P.x - B.P.x), (float)(K.P.y - B.P.y), (float)(K.Z.x - B.Z.x)};
   const float xx = rho * (QP[0] * QP[0] + QP[1] * QP[1] + QP[2] * QP[2]);
   double u[NR], w[NR];
   if (rys_smem) RysSmem<NR>::eval(rys_smem, (double)xx, u, w);
   else rys_eval<NR>((double)xx, u, w);
-  const float scale = (float)(B.C.x * K.C.x * (TWOPI5ON2 * wmask)) * (rho * rsqrt_f32(rho));
+  const float scale = (float)(B.C.x * K.C.x * (TWOPI5ON2 * wmask)) * sq;
   const float r_z = eta * inv;     // rho / zeta
   const float r_e = zeta * inv;    // rho / eta
   const float PA[3] = {(float)B.A0.x, (float)B.A0.y, (float)B.A1.x};
@@ -552,14 +556,15 @@ __device__ __forceinline__ void prim_quartet(const PrimRegs& B, const PrimRegs& 
   const double bcc = B.C.x * TWOPI5ON2, kcc = K.C.x;
   const double zeta = B.Z.y, half_zinv = B.C.y;
   const double eta = K.Z.y, half_einv = K.C.y;
-  const double inv = rcp_nr(zeta + eta);
+  const double sq = rsqrt_nr(zeta + eta);     // 1/sqrt(zeta + eta)
+  const double inv = sq * sq;
   const double rho = zeta * eta * inv;
   const double QPx = K.P.x - B.P.x, QPy = K.P.y - B.P.y, QPz = K.Z.x - B.Z.x;
   const double xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
   double u[NR], w[NR];
   if (rys_smem) RysSmem<NR>::eval(rys_smem, xx, u, w);
   else rys_eval<NR>(xx, u, w);
-  const double scale = bcc * kcc * (rho * rsqrt_nr(rho)) * wmask;
+  const double scale = bcc * kcc * sq * wmask;
   const double r_z = eta * inv;     // rho / zeta
   const double r_e = zeta * inv;    // rho / eta
 #pragma unroll

@@ -336,11 +336,12 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
         b0 = ld4(bp + ib, 0); b1 = ld4(bp + ib, 1);
         k0 = ld4(kp + ik, 0); k1 = ld4(kp + ik, 1);
         const double bcc = __ldg(&bp[ib].cc) * TWOPI5ON2, kcc = __ldg(&kp[ik].cc);
-        inv = rcp_nr(b0.w + k0.w);
+        const double sq = rsqrt_nr(b0.w + k0.w);
+        inv = sq * sq;
         const double rho = b0.w * k0.w * inv;
         const double QPx = k0.x - b0.x, QPy = k0.y - b0.y, QPz = k0.z - b0.z;
         xx = rho * (QPx * QPx + QPy * QPy + QPz * QPz);
-        scale = bcc * kcc * (rho * rsqrt_nr(rho));
+        scale = bcc * kcc * sq;                  // (cc holds the pair's sqrt(zeta))
         r_z = k0.w * inv;
         r_e = b0.w * inv;
       }

@@ -94,7 +94,8 @@ __device__ int warp_quartet(const WarpQuartet& q, const PrimPair* __restrict__ b
       const double4 k1 = ld4(kp + ik, 1);
       const double kcc = __ldg(&kp[ik].cc);
       const double zeta = b0.w, eta = k0.w;
-      const double inv = rcp_nr(zeta + eta);
+      const double sq = rsqrt_nr(zeta + eta);
+      const double inv = sq * sq;
       const double rho = zeta * eta * inv;
       const double QP[3] = {k0.x - b0.x, k0.y - b0.y, k0.z - b0.z};
       const double xx = rho * (QP[0] * QP[0] + QP[1] * QP[1] + QP[2] * QP[2]);
@@ -108,7 +109,7 @@ __device__ int warp_quartet(const WarpQuartet& q, const PrimPair* __restrict__ b
         case 6: { double uu[6], ww[6]; rys_eval<6>(xx, uu, ww); for (int i = 0; i < 6; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
         default: { double uu[7], ww[7]; rys_eval<7>(xx, uu, ww); for (int i = 0; i < 7; ++i) { u[i] = uu[i]; w[i] = ww[i]; } } break;
       }
-      const double scale = bcc * kcc * (rho * rsqrt_nr(rho));
+      const double scale = bcc * kcc * sq;      // (cc holds the pair's sqrt(zeta))
       const double r_z = eta * inv, r_e = zeta * inv;
       __syncwarp();
       // 2D tables: lane -> (direction, root)

@@ -118,7 +118,7 @@ __global__ void k_pair_prep(int n_pairs, PairRec* __restrict__ pairs, const doub
       q.zeta = zeta;
       q.PAx = q.Px - A[0]; q.PAy = q.Py - A[1]; q.PAz = q.Pz - A[2];
       q.half_zinv = 0.5 * inv;
-      q.cc = ch * cl * inv * sqrt(inv) * prefac;
+      q.cc = ch * cl * inv * prefac;      // c_a c_b / zeta x prefactor: see PrimPair
       q.pad = 0.0;
       static_assert(sizeof(PrimPair) == 80, "primitive-pair record layout");
       prim_full[pr.full_off + i] = q;
