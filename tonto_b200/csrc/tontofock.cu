@@ -350,6 +350,11 @@ struct ListArgs {
   const int* cxstart;
   const int* cn;
   unsigned char* qmask;
+  // the family tasks (ascending task indices) and, with the screening record, where
+  // each one's member masks start in cmask (one byte per candidate ket)
+  const int* fam_tasks;
+  const long long* fam_coff;
+  unsigned char* cmask;
 };
 
 // Screening record of a sorted pair position, 16 bytes read in list order (coalesced):
@@ -388,57 +393,98 @@ __device__ __forceinline__ long long slot(const ListArgs& a, long long t, int g,
   return t0 * NBUCKET + (long long)bucket * nt + (t - t0);
 }
 
+// Bra-family members a family task can hold (the largest fam_cap_l); the member
+// mask of a list entry is one byte.
+constexpr int FAM_LIST_MAX = 4;
+static_assert(fam_cap_l(0, 0, 0, 0) <= FAM_LIST_MAX && fam_cap_l(2, 0, 0, 0) <= FAM_LIST_MAX,
+              "family capacity beyond the list pass");
+
 // One warp per bra task.  MODE 0: screen every candidate ket and count the
 // survivors per bucket (and record the screening when a.cand is set); MODE 1:
 // screen again and write the survivors; MODE 2: write the survivors from the
 // recorded screening.  Lanes are grouped by bucket with one warp match per 32
-// candidates; per-warp bucket counters live in shared memory.
+// candidates; per-warp bucket counters live in shared memory.  FAM = false takes
+// the tasks [t_base, n_tasks) and skips family tasks; FAM = true takes the family
+// tasks a.fam_tasks[t_base .. n_tasks) (a bra family: every surviving ket carries
+// the mask of the members whose quartet with it passes the screen, recorded in
+// MODE 0 beside the bucket at cmask[fam_coff[w] + j]).
 constexpr int LIST_THREADS = 256;
 
 // (six resident blocks per SM: the pass waits on dependent L1 loads, so warps in
 // flight matter more than registers; measured 0.5 ms faster per (H2O)32 build
-// than four blocks, eight spill)
-template <int MODE>
-__global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long long* __restrict__ counts,
+// than four blocks, eight spill.  The family instantiation holds its members'
+// screening data in registers and runs four: 0.45 ms faster than six, which
+// spill.  Loading the next 32 candidates' records one chunk ahead measured
+// 0.2 ms slower.)
+template <int MODE, bool FAM>
+__global__ void __launch_bounds__(LIST_THREADS, FAM ? 4 : 6) k_quartets(ListArgs a, long long* __restrict__ counts,
                                                            const long long* __restrict__ offsets,
                                                            int2* __restrict__ out) {
   __shared__ int scnt[LIST_THREADS / 32][NBUCKET];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long t = a.t_base + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (t >= a.n_tasks) return;                    // uniform over the warp
+  const long long w = a.t_base + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (w >= a.n_tasks) return;                    // uniform over the warp
   if (MODE != 0 && a.list_total && *a.list_total - a.out_base > a.out_cap) return;
-  for (int k = lane; k < NBUCKET; k += 32) scnt[warp][k] = 0;
-  __syncwarp();
+  const long long t = FAM ? (long long)a.fam_tasks[w] : w;
   const int2 task = a.tasks[t];
   const CPUnit cp = a.units[task.x];
+  if (!FAM && cp.fam) return;                    // the family instantiation's task
+  for (int k = lane; k < NBUCKET; k += 32) scnt[warp][k] = 0;
+  __syncwarp();
   const int g = a.unit_group[task.x];
   const int i = task.y;
   // a family task: the family's first member stands for the bra; its members sit at
   // xs .. xs + nm - 1 of the bra class's list
-  const int bra = cp.fam ? a.csorted[cp.bra_off + i] : a.sorted[cp.bra_off + i];
-  const int xs = cp.fam ? a.cxstart[cp.bra_off + i] : 0;
-  const int nm = cp.fam ? a.cn[cp.bra_off + i] : 1;
-  const int jend = (a.bad && *a.bad) ? 0 : ((cp.p1 == cp.p2) ? (cp.fam ? xs + nm : i + 1) : cp.n_ket);
+  const int bra = FAM ? a.csorted[cp.bra_off + i] : a.sorted[cp.bra_off + i];
+  const int xs = FAM ? a.cxstart[cp.bra_off + i] : 0;
+  const int nm = FAM ? a.cn[cp.bra_off + i] : 1;
+  const int jend = (a.bad && *a.bad) ? 0 : ((cp.p1 == cp.p2) ? (FAM ? xs + nm : i + 1) : cp.n_ket);
   const long long coff = a.cand ? a.cand_off[t] : 0;
+  const long long foff = FAM && a.cand ? a.fam_coff[w] : 0;
   const int len = MODE == 2 ? a.task_len[t] : jend;
   double Ib = 0.0, pg = 0.0;
   int4 b = make_int4(0, 0, 0, 0);
   MolInfo mi{};
-  if (MODE != 2 || cp.fam) {
-    Ib = cp.fam ? a.cimax[cp.bra_off + i] : a.sorted_imax[cp.bra_off + i];
-    b = cp.fam ? a.srec[cp.bra_xoff + xs] : a.srec[cp.bra_off + i];
+  if (MODE != 2) {
+    Ib = FAM ? a.cimax[cp.bra_off + i] : a.sorted_imax[cp.bra_off + i];
+    b = FAM ? a.srec[cp.bra_xoff + xs] : a.srec[cp.bra_off + i];
     mi = a.mols[cp.mol];
     pg = __longlong_as_double((long long)a.pglob[cp.mol]);
   }
+  // the members' shells, Schwarz factors and bra density maxima, read once per task
+  int mshell[FAM_LIST_MAX];
+  double mib[FAM_LIST_MAX], mpab[FAM_LIST_MAX];
+  if (FAM && MODE != 2) {
+    const double* pm = a.pmax + mi.pmax;
+#pragma unroll
+    for (int m = 0; m < FAM_LIST_MAX; ++m) {
+      mshell[m] = 0; mib[m] = 0.0; mpab[m] = 0.0;
+      if (m < nm) {
+        mshell[m] = a.srec[cp.bra_xoff + xs + m].x;
+        mib[m] = a.sorted_imax[cp.bra_xoff + xs + m];
+        mpab[m] = pm[lo16(mshell[m]) * mi.n_shell + hi16(mshell[m])];
+      }
+    }
+  }
   // members of the bra family whose quartet with ket position j passes the screen
-  // (inside the family's own block, p1 == p2, only members at or after the ket)
+  // (inside the family's own block, p1 == p2, only members at or after the ket):
+  // quartet_bound member by member, the ket's own density maximum read once
   auto family_mask = [&](int j, const int4 k, double Ik, double& maxb) {
+    const double* pm = a.pmax + mi.pmax;
+    const int ns = mi.n_shell;
+    const int sc = lo16(k.x), sd = hi16(k.x);
+    const double pcd = pm[sc * ns + sd];
     unsigned m_ok = 0;
     maxb = 0.0;
-    for (int m = 0; m < nm; ++m) {
-      if (cp.p1 == cp.p2 && j - xs > m) continue;
-      const int4 bm = a.srec[cp.bra_xoff + xs + m];
-      const double bound = quartet_bound(a, mi, bm, k, a.sorted_imax[cp.bra_xoff + xs + m], Ik);
+#pragma unroll
+    for (int m = 0; m < FAM_LIST_MAX; ++m) {
+      if (m >= nm || (cp.p1 == cp.p2 && j - xs > m)) continue;
+      const int sa = lo16(mshell[m]), sb = hi16(mshell[m]);
+      double p = fmax(mpab[m], pcd);
+      p = fmax(p, fmax(pm[sa * ns + sc], pm[sa * ns + sd]));
+      p = fmax(p, fmax(pm[sb * ns + sc], pm[sb * ns + sd]));
+      if (p < 1.0e-20) continue;                  // TOL(20): skipped
+      const double bound = p * mib[m] * Ik;
       if (bound > a.cutoff) { m_ok |= 1u << m; maxb = fmax(maxb, bound); }
     }
     return m_ok;
@@ -455,20 +501,17 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
         if (cb != 0xff) {
           bucket = cb;
           ket = a.sorted[cp.ket_off + j];
-          if (cp.fam) {
-            double maxb;
-            fmask = family_mask(j, a.srec[cp.ket_off + j], a.sorted_imax[cp.ket_off + j], maxb);
-          }
+          if (FAM) fmask = a.cmask[foff + j];
         }
       }
     } else if (j < jend) {
       const double Ik = a.sorted_imax[cp.ket_off + j];
+      const int4 k = a.srec[cp.ket_off + j];
       if (!(Ib * a.sorted_bmax[cp.ket_off + j] * pg > a.cutoff)) {
         beyond = true;                           // bands are in decreasing I_max: nothing further survives
       } else if (Ib * Ik * pg > a.cutoff) {
-        const int4 k = a.srec[cp.ket_off + j];
         ket = k.w;
-        if (cp.fam) {
+        if (FAM) {
           double maxb;
           fmask = family_mask(j, k, Ik, maxb);
           if (fmask) bucket = cost_bucket(b, k) + (maxb < a.fp32_cut ? NCOST : 0);
@@ -477,7 +520,10 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
           if (bound > a.cutoff) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
         }
       }
-      if (MODE == 0 && a.cand) a.cand[coff + j] = bucket >= 0 ? (unsigned char)bucket : (unsigned char)0xff;
+      if (MODE == 0 && a.cand) {
+        a.cand[coff + j] = bucket >= 0 ? (unsigned char)bucket : (unsigned char)0xff;
+        if (FAM && bucket >= 0) a.cmask[foff + j] = (unsigned char)fmask;
+      }
     }
     const unsigned peers = __match_any_sync(0xffffffffu, bucket);
     const int rank = __popc(peers & ((1u << lane) - 1u));
@@ -489,7 +535,7 @@ __global__ void __launch_bounds__(LIST_THREADS, 6) k_quartets(ListArgs a, long l
       const long long pos = offsets[slot(a, t, g, bucket)] - a.out_base + base + rank;
       if (pos < a.out_cap) {
         out[pos] = make_int2(bra, ket);
-        if (cp.fam) a.qmask[pos] = (unsigned char)fmask;
+        if (FAM) a.qmask[pos] = (unsigned char)fmask;
       }
     }
     scanned = j0 + 32;
@@ -1491,6 +1537,7 @@ struct tf_ctx {
   std::vector<int> group_fam;                            // bra-family capacity of each group's kernel (1: none)
   tf::PairFamilies fams;                                 // shell-pair families (host)
   long long n_tasks = 0;
+  std::vector<int> fam_tasks;                            // family tasks, ascending
   long long list_budget = 1LL << 30;                     // quartets per list chunk (8 B each)
   // screening record: one byte per candidate (bra task, ket) pair, when it fits
   bool use_cand = false;
@@ -1517,6 +1564,9 @@ struct tf_ctx {
   tf::DBuf<tf::CPUnit> d_units;
   tf::DBuf<int> d_unit_group, d_group_task0, d_task_len;
   tf::DBuf<unsigned char> d_cand;
+  tf::DBuf<int> d_fam_tasks;                             // family tasks (k_quartets<.., true>)
+  tf::DBuf<long long> d_fam_coff;                        // their member masks in d_cmask
+  tf::DBuf<unsigned char> d_cmask;                       // recorded member mask per candidate ket
   tf::DBuf<int4> d_srec, d_jkrec;
   tf::DBuf<double2> d_pairR;
   tf::DBuf<long long> d_task_cand_off;
@@ -1910,11 +1960,28 @@ static int build_tasks(tf_ctx* c) {
                          : u.fam ? c->lists.cxstart[u.bra_off + i] + c->lists.cn[u.bra_off + i] : i + 1;
     cand_off[t + 1] = cand_off[t] + nk;
   }
+  // family tasks, and where their member masks start in the screening record
+  c->fam_tasks.clear();
+  std::vector<long long> fam_coff(1, 0);
+  for (size_t t = 0; t < tasks.size(); ++t)
+    if (c->units[tasks[t].x].fam) {
+      c->fam_tasks.push_back((int)t);
+      fam_coff.push_back(fam_coff.back() + (cand_off[t + 1] - cand_off[t]));
+    }
+  TF_CUDA(c->d_fam_tasks.reserve(std::max<size_t>(c->fam_tasks.size(), 1)));
+  if (!c->fam_tasks.empty())
+    TF_CUDA(cudaMemcpyAsync(c->d_fam_tasks.p, c->fam_tasks.data(), c->fam_tasks.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, c->stream));
   c->use_cand = false;
-  if (cand_off.back() <= c->cand_budget && c->d_cand.reserve(std::max<long long>(cand_off.back(), 1)) == cudaSuccess &&
+  if (cand_off.back() + fam_coff.back() <= c->cand_budget &&
+      c->d_cand.reserve(std::max<long long>(cand_off.back(), 1)) == cudaSuccess &&
+      c->d_cmask.reserve(std::max<long long>(fam_coff.back(), 1)) == cudaSuccess &&
+      c->d_fam_coff.reserve(fam_coff.size()) == cudaSuccess &&
       c->d_task_cand_off.reserve(cand_off.size()) == cudaSuccess &&
       c->d_task_len.reserve(std::max<size_t>(tasks.size(), 1)) == cudaSuccess) {
     TF_CUDA(cudaMemcpyAsync(c->d_task_cand_off.p, cand_off.data(), cand_off.size() * sizeof(long long),
+                            cudaMemcpyHostToDevice, c->stream));
+    TF_CUDA(cudaMemcpyAsync(c->d_fam_coff.p, fam_coff.data(), fam_coff.size() * sizeof(long long),
                             cudaMemcpyHostToDevice, c->stream));
     c->use_cand = true;
   }
@@ -2264,6 +2331,29 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
   return npq * per_prim + nq * per_q;
 }
 
+// The list pass MODE over tasks [t0, t1): the plain tasks, then the family tasks
+// among them (their own instantiation, over the family task list).
+template <int MODE>
+static void launch_list(tf_ctx* c, ListArgs a, long long t0, long long t1, long long* counts,
+                        const long long* offsets, int2* out, cudaStream_t s, int& kernels) {
+  const long long thr = LIST_THREADS;
+  a.t_base = t0;
+  a.n_tasks = t1;
+  k_quartets<MODE, false><<<(unsigned)std::max<long long>(1, ((t1 - t0) * 32 + thr - 1) / thr), (unsigned)thr, 0, s>>>(
+      a, counts, offsets, out);
+  kernels++;
+  const auto& ft = c->fam_tasks;
+  const long long f0 = std::lower_bound(ft.begin(), ft.end(), (int)t0) - ft.begin();
+  const long long f1 = std::lower_bound(ft.begin(), ft.end(), (int)t1) - ft.begin();
+  if (f1 > f0) {
+    a.t_base = f0;
+    a.n_tasks = f1;
+    k_quartets<MODE, true><<<(unsigned)(((f1 - f0) * 32 + thr - 1) / thr), (unsigned)thr, 0, s>>>(a, counts, offsets,
+                                                                                                  out);
+    kernels++;
+  }
+}
+
 // Density transform, pair maxima, quartet counts, their scan and the per-group
 // (start, FP32 start, end) offsets on the device: the part of a build shared by
 // the dynamic and the graph paths.
@@ -2296,11 +2386,11 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   la.cxstart = c->d_cxstart.p;
   la.cn = c->d_cn.p;
   la.qmask = c->d_qmask.p;
-  const long long thr_list = LIST_THREADS;
-  const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
+  la.fam_tasks = c->d_fam_tasks.p;
+  la.fam_coff = c->d_fam_coff.p;
+  la.cmask = c->d_cmask.p;
   const long long nslots = c->n_tasks * NBUCKET;
-  k_quartets<0><<<grid_list, (unsigned)thr_list, 0, s>>>(la, c->d_counts.p, nullptr, nullptr);
-  kernels++;
+  launch_list<0>(c, la, 0, c->n_tasks, c->d_counts.p, nullptr, nullptr, s, kernels);
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
   if (tmp_bytes > c->d_scan_tmp.n) { set_error("scan scratch not sized"); return TF_ESTATE; }
@@ -2355,11 +2445,8 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
   ListArgs lw = la;
   lw.out_cap = c->graph_cap;
   lw.list_total = c->d_offsets.p + c->n_tasks * NBUCKET;     // an overflowing list is not written
-  const long long thr_list = LIST_THREADS;
-  const unsigned grid_list = (unsigned)std::max<long long>(1, (c->n_tasks * 32 + thr_list - 1) / thr_list);
-  if (c->use_cand) k_quartets<2><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
-  else k_quartets<1><<<grid_list, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
-  kernels++;
+  if (c->use_cand) launch_list<2>(c, lw, 0, c->n_tasks, nullptr, c->d_offsets.p, c->d_quartets.p, s, kernels);
+  else launch_list<1>(c, lw, 0, c->n_tasks, nullptr, c->d_offsets.p, c->d_quartets.p, s, kernels);
   const int ng = (int)c->group_cls.size();
   // class schedule: the class launches are spread over sched_streams branches of
   // the graph (the autotuner's choice), so that one class's tail overlaps another
@@ -2596,23 +2683,19 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
     drop_graph(c);
     c->graph_cap = 0;
   }
-  const long long thr_list = LIST_THREADS;
   for (size_t ci = 0; ci + 1 < chunk.size(); ++ci) {
     const int g0 = chunk[ci], g1 = chunk[ci + 1];
     const long long base = goff[3 * g0], nq = goff[3 * (g1 - 1) + 2] - base;
     if (nq > 0) {
       ListArgs lw = la;
-      lw.t_base = c->group_task0[g0];
-      lw.n_tasks = c->group_task0[g1];
       lw.out_base = base;
       lw.qmask = c->d_qmask.p;
-      const unsigned grid_w =
-          (unsigned)std::max<long long>(1, ((lw.n_tasks - lw.t_base) * 32 + thr_list - 1) / thr_list);
       if (c->use_cand)
-        k_quartets<2><<<grid_w, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
+        launch_list<2>(c, lw, c->group_task0[g0], c->group_task0[g1], nullptr, c->d_offsets.p, c->d_quartets.p, s,
+                       kernels);
       else
-        k_quartets<1><<<grid_w, (unsigned)thr_list, 0, s>>>(lw, nullptr, c->d_offsets.p, c->d_quartets.p);
-      kernels++;
+        launch_list<1>(c, lw, c->group_task0[g0], c->group_task0[g1], nullptr, c->d_offsets.p, c->d_quartets.p, s,
+                       kernels);
     }
     for (int g = g0; g < g1; ++g) {
       int l1h, l1l, l2h, l2l;
