@@ -46,6 +46,7 @@ def parse():
                     help="clusters of the batch time-to-SCF measurement (0: skip; 256: the full batch)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the oracle build (CPU baseline, parity, FLOP counts)")
     ap.add_argument("--no-alkane", action="store_true", help="skip the C40H82 mixed-precision measurement")
+    ap.add_argument("--no-det", action="store_true", help="skip the deterministic-build measurement")
     ap.add_argument("--waters", type=int, default=N_WATER,
                     help="cluster size (default 32: the benchmark workload; smaller sizes for profiling)")
     return ap.parse_args()
@@ -444,6 +445,39 @@ def main():
                  "max_abs_dJ_vs_fp64": float((J - J64).abs().max()), "max_abs_dK_vs_fp64": float((K - K64).abs().max())}
         fb.make_r_JK_device(P, J, K)
         torch.cuda.synchronize(dev)
+    # the same builds with deterministic accumulation (two fixed-point words per
+    # element, integer atomics), device-timed alike, in a context of their own
+    det = None
+    if world == 1 and not args.no_det:
+        J64, K64 = J.clone(), K.clone()
+        fd = FockBuilder(mol, schwarz_cutoff=SCHWARZ, device=local, deterministic=True)
+        Jd, Kd = torch.empty_like(J), torch.empty_like(K)
+        fd.autotune(P, Jd, Kd, max_streams=4)
+        for _ in range(max(3, args.warmup)):
+            fd.make_r_JK_device(P, Jd, Kd)
+        torch.cuda.synchronize(dev)
+        first = (Jd.clone(), Kd.clone())
+        dev_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+        same = True
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            dev_ev[k][0].record(stream)
+            fd.make_r_JK_device(P, Jd, Kd)
+            dev_ev[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+            same = same and torch.equal(Jd, first[0]) and torch.equal(Kd, first[1])
+        fd.set_graph(False)                       # class by class, another path to the same bits
+        fd.make_r_JK_device(P, Jd, Kd)
+        torch.cuda.synchronize(dev)
+        same_path = torch.equal(Jd, first[0]) and torch.equal(Kd, first[1])
+        fd.close()
+        d_ms = sum(a.elapsed_time(b) for a, b in dev_ev) / args.steps
+        det = {"value": 1e3 / d_ms, "unit": "builds/s", "ms_per_step": d_ms,
+               "bitwise_equal_over_timed_builds": bool(same), "bitwise_equal_graph_vs_class_by_class": bool(same_path),
+               "max_abs_dJ_vs_fp64": float((first[0] - J64).abs().max()),
+               "max_abs_dK_vs_fp64": float((first[1] - K64).abs().max())}
+        del Jd, Kd, first
     # per-class device times: builds launched class by class (events between the
     # launches), outside the timed region
     cls_acc = {}
@@ -525,6 +559,7 @@ def main():
             "class_schedule": {"graph_branches": tune["streams"], "non_default_kernel_variants": tune["variant_classes"],
                                "autotune_ms": [round(v, 3) for v in tune["ms"]]},
             "mixed_precision_builds": mixed,
+            "deterministic_builds": det,
             "build": {"quartets": st["quartets"], "prim_quartets": st["prim_quartets"],
                       "graph": graph_builds, "direct_build_ms": st_direct["build_ms"],
                       "direct_eri_ms": st_direct["eri_ms"]},

@@ -87,8 +87,16 @@ typedef struct tf_options {
   double eri_primitive_pair_cutoff;  /* SHELL1QUARTET pair_cutoff (Tonto default 1e-6, macros.in:695) */
   double mixed_fp32_cut;             /* TF_JK_MIXED: Schwarz x density bound below which FP32 is used */
   int device;                        /* CUDA device ordinal */
-  int deterministic;                 /* reserved, set 0: J and K accumulate with FP64 atomics
-                                        (reproducible to rounding, not bitwise) */
+  int deterministic;                 /* 0: J and K accumulate with FP64 atomics (reproducible to
+                                        rounding, not bitwise).  1: bitwise-reproducible builds:
+                                        every contribution is added as two 64-bit fixed-point
+                                        words (2^-32 and 2^-60 units) with integer atomics, whose
+                                        sums do not depend on the order of the additions, so a
+                                        build gives the same bits whatever the launch schedule,
+                                        graph or not, kernel variants and list chunking (for a
+                                        fixed shard plan); elements and contributions must stay
+                                        below 2^31 in magnitude.  Costs twice the accumulator
+                                        memory and about one more atomic per contribution */
 } tf_options;
 
 typedef struct tf_stats {

@@ -93,7 +93,8 @@ def test_null_arrays_are_refused(mol):
 
 @pytest.mark.parametrize("field,value", [("eri_schwarz_cutoff", 0.0), ("eri_schwarz_cutoff", -1e-9),
                                          ("eri_schwarz_cutoff", math.nan), ("eri_primitive_pair_cutoff", -1.0),
-                                         ("mixed_fp32_cut", math.nan), ("device", -1)])
+                                         ("mixed_fp32_cut", math.nan), ("device", -1), ("deterministic", 2),
+                                         ("deterministic", -1)])
 def test_bad_options_are_refused(mol, field, value):
     from tonto_b200.fock import default_options
     opt = default_options()

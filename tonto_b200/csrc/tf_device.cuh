@@ -62,6 +62,38 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
 }
 
 // ---------------------------------------------------------------------------
+// Fock accumulation.  FX = false: an FP64 atomic add.  Deterministic builds
+// (FX = true, a kernel instantiation of its own so that the default kernels carry
+// none of this code): the contribution v is split into two 64-bit fixed-point words,
+// hi = round(v 2^32) and lo = round((v - hi 2^-32) 2^60), added with integer
+// atomics to the element's hi word (the accumulator itself, read as an integer)
+// and to its lo word, fx_lo elements further on.  v - hi 2^-32 is exact (the two
+// are within a factor of two of each other, or hi = 0), so each contribution is
+// kept to 2^-61; integer sums are exact and wrap modulo 2^64, so the totals do
+// not depend on the order of the additions, and k_finalize reads them as
+// hi 2^-32 + lo 2^-60.  Contributions and totals below 2^31 in magnitude.
+// ---------------------------------------------------------------------------
+template <bool FX>
+__device__ __forceinline__ void fock_add(double* addr, double v, long long fx_lo) {
+  if constexpr (!FX) {
+    atomicAdd(addr, v);
+  } else {
+    const double h = rint(v * 0x1p32);
+    const long long hi = (long long)h;
+    const long long lo = __double2ll_rn((v - h * 0x1p-32) * 0x1p60);
+    atomicAdd(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)hi);
+    atomicAdd(reinterpret_cast<unsigned long long*>(addr + fx_lo), (unsigned long long)lo);
+  }
+}
+
+// The value of a Fock accumulator element (see fock_add).
+__device__ __forceinline__ double fock_value(const double* m, size_t i, long long fx_lo) {
+  if (fx_lo == 0) return m[i];
+  const long long* q = reinterpret_cast<const long long*>(m);
+  return (double)q[i] * 0x1p-32 + (double)q[i + fx_lo] * 0x1p-60;
+}
+
+// ---------------------------------------------------------------------------
 // compile-time helpers
 // ---------------------------------------------------------------------------
 template <int... Is, class F>

@@ -234,6 +234,7 @@ struct GroupArgs {
   double* K2;
   int want;                     // bit 0 J, bit 1 K
   unsigned long long* qcount;   // quartets counted per class (the launch's FP64 or FP32 half), or null
+  long long fx_lo;              // deterministic builds: offset of the lo words (fock_add), else 0
 };
 
 // Rys nodes and weights of a lane group's primitive quartet: the 2 N polynomial
@@ -280,7 +281,7 @@ __device__ __forceinline__ void group_rys(double x, int gl, int gbase, double (&
 __constant__ unsigned char c_gcomp[3][NCOMP_ALL];
 __constant__ unsigned char c_gidx[(LCOMP + 1) * (LCOMP + 1) * (LCOMP + 1)];
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, bool FX>
 __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
   using C = GroupCfg<LA, LB, LC, LD>;
   using Q = typename C::Q;
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
           for (int c = 0; c < NC; ++c)
 #pragma unroll
             for (int d = 0; d < ND; ++d) s += I[e * NCD + c * ND + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
-          atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ibb, f * s);
+          fock_add<FX>(Jm + (size_t)(oa + ia) * n + ob + ibb, f * s, a.fx_lo);
         }
         for (int e = gl; e < NCD; e += G) {                // J(cd) = sum_ab I P(ab)
           const int c = e / ND, d = e - c * ND;
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
 #pragma unroll
             for (int ibb = 0; ibb < NB; ++ibb)
               s += I[(ia * NB + ibb) * NCD + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ibb);
-          atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+          fock_add<FX>(Jm + (size_t)(oc + c) * n + od + d, f * s, a.fx_lo);
         }
       };
       if (a.want & 1) {
@@ -454,7 +455,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
 #pragma unroll
             for (int d = 0; d < ND; ++d)
               s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + od + d);
-          atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
+          fock_add<FX>(Km + (size_t)(oa + ia) * n + oc + c, f * s, a.fx_lo);
         }
         for (int e = gl; e < NA * ND; e += G) {            // K(ad) = sum_bc I P(bc)
           const int ia = e / ND, d = e - ia * ND;
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
 #pragma unroll
             for (int c = 0; c < NC; ++c)
               s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ibb) * n + oc + c);
-          atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
+          fock_add<FX>(Km + (size_t)(oa + ia) * n + od + d, f * s, a.fx_lo);
         }
         for (int e = gl; e < NB * NC; e += G) {            // K(bc) = sum_ad I P(ad)
           const int ibb = e / NC, c = e - ibb * NC;
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
 #pragma unroll
             for (int d = 0; d < ND; ++d)
               s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
-          atomicAdd(Km + (size_t)(ob + ibb) * n + oc + c, f * s);
+          fock_add<FX>(Km + (size_t)(ob + ibb) * n + oc + c, f * s, a.fx_lo);
         }
         for (int e = gl; e < NB * ND; e += G) {            // K(bd) = sum_ac I P(ac)
           const int ibb = e / ND, d = e - ibb * ND;
@@ -484,7 +485,7 @@ __global__ void __launch_bounds__(128) k_jk_group(GroupArgs a) {
 #pragma unroll
             for (int c = 0; c < NC; ++c)
               s += I[(ia * NB + ibb) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
-          atomicAdd(Km + (size_t)(ob + ibb) * n + od + d, f * s);
+          fock_add<FX>(Km + (size_t)(ob + ibb) * n + od + d, f * s, a.fx_lo);
         }
       };
       if (a.want & 2) {

@@ -583,6 +583,7 @@ struct JKArgs {
   unsigned long long* qcount;
   int fam;                      // bra-family capacity of the launch's kernel (1: none)
   int bucket32;                 // 1: the launch covers the FP32 buckets
+  long long fx_lo;              // deterministic builds: offset of the lo words (fock_add), else 0
 };
 
 
@@ -601,7 +602,8 @@ constexpr int jk_min_blocks() {
   return Quartet<LA, LB, LC, LD>::NROOT == 1 ? ((V & 1) ? 6 : TF_JK_MINB_N1) : ((V & 1) ? 4 : TF_JK_MINB);
 }
 // Variant bits: 1 = more resident warps (see above); 2 = K atomics of lanes that hit
-// the same element summed first (segmented warp sums over lanes of one bra).
+// the same element summed first (segmented warp sums over lanes of one bra); 4 =
+// deterministic accumulation (fock_add), set by the context, not by the autotuner.
 constexpr int JK_VARIANTS = 4;
 // Threads per block: the resident warps of an SM form one block, so the SM holds
 // one copy of the shared Rys/Boys grid and leaves the rest of its shared storage to
@@ -635,6 +637,7 @@ __device__ __forceinline__ void digest_jk(const JKArgs& a, const MolInfo& mi,
                                           const double (&I)[ncart(LA)][ncart(LB)][ncart(LC) * ncart(LD)], double f,
                                           int bid, int oa, int ob, int oc, int od) {
   using Q = Quartet<LA, LB, LC, LD>;
+  constexpr bool FX = (V & 4) != 0;
   const int lane = threadIdx.x & 31;
   const bool live = f != 0.0;
   const int n = mi.n_cart;
@@ -665,14 +668,14 @@ __device__ __forceinline__ void digest_jk(const JKArgs& a, const MolInfo& mi,
         if (uni) {
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          if (lane == 0 && s != 0.0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+          if (lane == 0 && s != 0.0) fock_add<FX>(Jm + (size_t)(oa + ia) * n + ob + ib, s, a.fx_lo);
         } else {                       // idle lanes join the last run with s = 0
 #pragma unroll
           for (int o = 1; o < 32; o <<= 1) {
             const double t = __shfl_up_sync(0xffffffffu, s, o);
             if (lane - o >= sega) s += t;
           }
-          if (taila && s != 0.0) atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, s);
+          if (taila && s != 0.0) fock_add<FX>(Jm + (size_t)(oa + ia) * n + ob + ib, s, a.fx_lo);
         }
       }
     if (live) {
@@ -690,7 +693,7 @@ __device__ __forceinline__ void digest_jk(const JKArgs& a, const MolInfo& mi,
           for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
             for (int ib = 0; ib < Q::NB; ++ib) s += I[ia][ib][c * Q::ND + d] * Pab[ia][ib];
-          atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+          fock_add<FX>(Jm + (size_t)(oc + c) * n + od + d, f * s, a.fx_lo);
         }
     }
   };
@@ -718,9 +721,9 @@ __device__ __forceinline__ void digest_jk(const JKArgs& a, const MolInfo& mi,
         const double t = __shfl_up_sync(0xffffffffu, v, o);
         if (lane - o >= seg) v += t;
       }
-      if (tail && v != 0.0) atomicAdd(addr, v);
+      if (tail && v != 0.0) fock_add<FX>(addr, v, a.fx_lo);
     } else {
-      atomicAdd(addr, v);
+      fock_add<FX>(addr, v, a.fx_lo);
     }
   };
 #define TF_KADD_C(addr, v) kadd((addr), (v), segc, tailc)
@@ -955,6 +958,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_schwarz_warp(const int
 // gscr: WF_SCRATCH doubles of global memory per warp of the grid.  Used for the
 // FP64 and the FP32 buckets alike (f classes are always evaluated in FP64).
 // ---------------------------------------------------------------------------
+template <bool FX>
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int la, int lb, int lc, int ld,
                                                                  double* __restrict__ gscr) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -996,14 +1000,14 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
           double s = 0.0;
           for (int c = 0; c < NC; ++c)
             for (int d = 0; d < ND; ++d) s += I[e * NCD + c * ND + d] * __ldg(P + (size_t)(oc + c) * n + od + d);
-          atomicAdd(Jm + (size_t)(oa + ia) * n + ob + ib, f * s);
+          fock_add<FX>(Jm + (size_t)(oa + ia) * n + ob + ib, f * s, a.fx_lo);
         }
         for (int e = lane; e < NCD; e += 32) {                 // J(cd) = sum_ab I P(ab)
           const int c = e / ND, d = e - c * ND;
           double s = 0.0;
           for (int ia = 0; ia < NA; ++ia)
             for (int ib = 0; ib < NB; ++ib) s += I[(ia * NB + ib) * NCD + e] * __ldg(P + (size_t)(oa + ia) * n + ob + ib);
-          atomicAdd(Jm + (size_t)(oc + c) * n + od + d, f * s);
+          fock_add<FX>(Jm + (size_t)(oc + c) * n + od + d, f * s, a.fx_lo);
         }
       }
       if (a.want & 2) {
@@ -1013,7 +1017,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
           for (int ib = 0; ib < NB; ++ib)
             for (int d = 0; d < ND; ++d)
               s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ib) * n + od + d);
-          atomicAdd(Km + (size_t)(oa + ia) * n + oc + c, f * s);
+          fock_add<FX>(Km + (size_t)(oa + ia) * n + oc + c, f * s, a.fx_lo);
         }
         for (int e = lane; e < NA * ND; e += 32) {             // K(ad) = sum_bc I P(bc)
           const int ia = e / ND, d = e - ia * ND;
@@ -1021,7 +1025,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
           for (int ib = 0; ib < NB; ++ib)
             for (int c = 0; c < NC; ++c)
               s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(ob + ib) * n + oc + c);
-          atomicAdd(Km + (size_t)(oa + ia) * n + od + d, f * s);
+          fock_add<FX>(Km + (size_t)(oa + ia) * n + od + d, f * s, a.fx_lo);
         }
         for (int e = lane; e < NB * NC; e += 32) {             // K(bc) = sum_ad I P(ad)
           const int ib = e / NC, c = e - ib * NC;
@@ -1029,7 +1033,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
           for (int ia = 0; ia < NA; ++ia)
             for (int d = 0; d < ND; ++d)
               s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + od + d);
-          atomicAdd(Km + (size_t)(ob + ib) * n + oc + c, f * s);
+          fock_add<FX>(Km + (size_t)(ob + ib) * n + oc + c, f * s, a.fx_lo);
         }
         for (int e = lane; e < NB * ND; e += 32) {             // K(bd) = sum_ac I P(ac)
           const int ib = e / ND, d = e - ib * ND;
@@ -1037,7 +1041,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
           for (int ia = 0; ia < NA; ++ia)
             for (int c = 0; c < NC; ++c)
               s += I[(ia * NB + ib) * NCD + c * ND + d] * __ldg(P + (size_t)(oa + ia) * n + oc + c);
-          atomicAdd(Km + (size_t)(ob + ib) * n + od + d, f * s);
+          fock_add<FX>(Km + (size_t)(ob + ib) * n + od + d, f * s, a.fx_lo);
         }
       }
     };
@@ -1058,7 +1062,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_jk_warp(JKArgs a, int 
 // J = 2 (J + J^T), K = K + K^T in the Cartesian basis, then to the Tonto basis
 // (column-major), for every molecule of the batch.
 __global__ void k_finalize(BatchArgs bt, const double* __restrict__ Jc, const double* __restrict__ Kc,
-                           double* __restrict__ J, double* __restrict__ K) {
+                           double* __restrict__ J, double* __restrict__ K, long long fx_lo) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= bt.bmat_off[bt.n_mol]) return;
   const int m = find_mol(bt.bmat_off, bt.n_mol, t);
@@ -1084,8 +1088,8 @@ __global__ void k_finalize(BatchArgs bt, const double* __restrict__ Jc, const do
       if (uq == 0.0) continue;
       const int cq = tj ? cj + q : cj + mj;
       const double w = up * uq;
-      sJ += w * (Jm[(size_t)cp * nc + cq] + Jm[(size_t)cq * nc + cp]);
-      sK += w * (Km[(size_t)cp * nc + cq] + Km[(size_t)cq * nc + cp]);
+      sJ += w * (fock_value(Jm, (size_t)cp * nc + cq, fx_lo) + fock_value(Jm, (size_t)cq * nc + cp, fx_lo));
+      sK += w * (fock_value(Km, (size_t)cp * nc + cq, fx_lo) + fock_value(Km, (size_t)cq * nc + cp, fx_lo));
     }
   }
   J[t] = 2.0 * sJ;
@@ -2222,10 +2226,12 @@ static void launch_jk_v(const JKArgs& a, cudaStream_t s, bool fp32) {
 
 template <int LA, int LB, int LC, int LD, int MB>
 static void launch_jk_m(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
-  switch (variant & 3) {
+  switch (variant & 7) {
     case 1: launch_jk_v<LA, LB, LC, LD, 1, MB>(a, s, fp32); break;
     case 2: launch_jk_v<LA, LB, LC, LD, 2, MB>(a, s, fp32); break;
     case 3: launch_jk_v<LA, LB, LC, LD, 3, MB>(a, s, fp32); break;
+    case 4: case 6: launch_jk_v<LA, LB, LC, LD, 4, MB>(a, s, fp32); break;   // deterministic: no bit 2
+    case 5: case 7: launch_jk_v<LA, LB, LC, LD, 5, MB>(a, s, fp32); break;
     default: launch_jk_v<LA, LB, LC, LD, 0, MB>(a, s, fp32); break;
   }
 }
@@ -2250,8 +2256,10 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   constexpr size_t smem = group_smem_bytes<LA, LB, LC, LD>(GROUP_WPB);
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_jk_group<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
+    if (cudaFuncSetAttribute(k_jk_group<LA, LB, LC, LD, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_jk_group<LA, LB, LC, LD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
       set_error("shared memory attribute");
       return TF_ECUDA;
     }
@@ -2263,8 +2271,8 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   constexpr int QPB = GroupCfg<LA, LB, LC, LD>::QPW * GROUP_WPB;
   static int group_blocks_per_sm = -1;
   if (group_blocks_per_sm < 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group_blocks_per_sm, k_jk_group<LA, LB, LC, LD>, 32 * GROUP_WPB,
-                                                  smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group_blocks_per_sm, k_jk_group<LA, LB, LC, LD, false>,
+                                                  32 * GROUP_WPB, smem);
     if (group_blocks_per_sm < 1) group_blocks_per_sm = 1;
   }
   if (a.n <= 0 && !a.range) return TF_OK;
@@ -2272,8 +2280,9 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   const long long blocks = a.range ? full : std::min<long long>((a.n + QPB - 1) / QPB, (long long)nsm * 32);
   GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count,
               a.range, a.base, a.cap, a.jkrec, a.pairR, a.P2, a.J2, a.K2, a.want,
-              a.qcount ? a.qcount + (a.bucket32 ? NQCLS : 0) : nullptr};
-  k_jk_group<LA, LB, LC, LD><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
+              a.qcount ? a.qcount + (a.bucket32 ? NQCLS : 0) : nullptr, a.fx_lo};
+  if (a.fx_lo) k_jk_group<LA, LB, LC, LD, true><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
+  else k_jk_group<LA, LB, LC, LD, false><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
   return TF_OK;
 }
 
@@ -2284,7 +2293,8 @@ static int launch_warp_jk(const JKArgs& a, cudaStream_t s, int la, int lb, int l
   if (!a.wscratch || a.wscratch_warps < WARPS_PER_BLOCK) { set_error("no scratch for the f-shell kernel"); return TF_ESTATE; }
   const long long full = a.wscratch_warps / WARPS_PER_BLOCK;
   const long long blocks = a.range ? full : std::min<long long>((a.n + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK, full);
-  k_jk_warp<<<(unsigned)blocks, 32 * WARPS_PER_BLOCK, 0, s>>>(a, la, lb, lc, ld, a.wscratch);
+  if (a.fx_lo) k_jk_warp<true><<<(unsigned)blocks, 32 * WARPS_PER_BLOCK, 0, s>>>(a, la, lb, lc, ld, a.wscratch);
+  else k_jk_warp<false><<<(unsigned)blocks, 32 * WARPS_PER_BLOCK, 0, s>>>(a, la, lb, lc, ld, a.wscratch);
   return TF_OK;
 }
 
@@ -2329,6 +2339,18 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
   for (int k = 1; k <= lb; ++k) hrr += 2.0 * nc * nd * (ncart_upto(la + lb - k) - ncart_upto(la - 1)) * ncart(k);
   const double per_q = hrr + 12.0 * nint;
   return npq * per_prim + nq * per_q;
+}
+
+// Deterministic builds (tf_options.deterministic): the Fock accumulators hold two
+// fixed-point words per element (fock_add), the lo words after all the hi words,
+// the kernels are their deterministic instantiations (variant bit 4, fock_add),
+// and the variants that sum K contributions across lanes in FP64 first (bit 2)
+// are not used, so that what is added to each element does not depend on the
+// autotuner's choice.
+static long long fx_offset(const tf_ctx* c) { return c->opt.deterministic ? c->cmat_off[c->n_mol] : 0; }
+static long long acc_elems(const tf_ctx* c) { return (c->opt.deterministic ? 2 : 1) * c->cmat_off[c->n_mol]; }
+static int jk_variant(const tf_ctx* c, int g) {
+  return c->opt.deterministic ? ((c->cls_variant[g] & ~2) | 4) : c->cls_variant[g];
 }
 
 // The list pass MODE over tasks [t0, t1): the plain tasks, then the family tasks
@@ -2400,12 +2422,12 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   const int ng = (int)c->group_cls.size();
   k_group_offsets<<<(ng + 63) / 64, 64, 0, s>>>(ng, c->d_group_task0.p, c->d_offsets.p, cap, c->d_group_offsets.p);
   kernels += 3;
-  const long long nc = c->cmat_off[c->n_mol];
-  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nc * sizeof(double), s));
-  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nc * sizeof(double), s));
+  const long long nacc = acc_elems(c);
+  TF_CUDA(cudaMemsetAsync(c->d_Jc.p, 0, nacc * sizeof(double), s));
+  TF_CUDA(cudaMemsetAsync(c->d_Kc.p, 0, nacc * sizeof(double), s));
   if (dPb) {
-    TF_CUDA(cudaMemsetAsync(c->d_JcB.p, 0, nc * sizeof(double), s));
-    TF_CUDA(cudaMemsetAsync(c->d_KcB.p, 0, nc * sizeof(double), s));
+    TF_CUDA(cudaMemsetAsync(c->d_JcB.p, 0, nacc * sizeof(double), s));
+    TF_CUDA(cudaMemsetAsync(c->d_KcB.p, 0, nacc * sizeof(double), s));
   }
   return TF_OK;
 }
@@ -2415,10 +2437,10 @@ static int enqueue_finalize(tf_ctx* c, double* dJ, double* dK, double* dJb, doub
   const BatchArgs bt = batch_args(c);
   const long long nb2 = c->bmat_off[c->n_mol];
   const unsigned gb = (unsigned)std::max<long long>(1, (nb2 + 255) / 256);
-  k_finalize<<<gb, 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK);
+  k_finalize<<<gb, 256, 0, s>>>(bt, c->d_Jc.p, c->d_Kc.p, dJ, dK, fx_offset(c));
   kernels++;
   if (dKb) {                                   // unrestricted: the beta J and K
-    k_finalize<<<gb, 256, 0, s>>>(bt, c->d_JcB.p, c->d_KcB.p, dJb, dKb);
+    k_finalize<<<gb, 256, 0, s>>>(bt, c->d_JcB.p, c->d_KcB.p, dJb, dKb, fx_offset(c));
     kernels++;
   }
   TF_CUDA(cudaGetLastError());
@@ -2473,14 +2495,15 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
     a.qcount = c->d_prim_count.p + NQCLS + 1;
     a.fam = c->group_fam[g];
     a.bucket32 = 0;
+    a.fx_lo = fx_offset(c);
     JKArgs a32 = a;
     a32.range = c->d_group_offsets.p + 3 * g + 1;
     a32.bucket32 = 1;
-    rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false, c->cls_variant[g]);
+    rc = dispatch_jk(l1h, l1l, l2h, l2l, a, sg, false, jk_variant(c, g));
     if (rc != TF_OK) return rc;
     kernels++;
     if (mixed) {
-      rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, sg, true, c->cls_variant[g]);
+      rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, sg, true, jk_variant(c, g));
       if (rc != TF_OK) return rc;
       kernels++;
     }
@@ -2559,8 +2582,8 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   const bool mixed = (flags & TF_JK_MIXED) != 0;
   if (dPb) {                                    // unrestricted: per-spin Cartesian densities and exchange
     const long long nc = c->cmat_off[c->n_mol];
-    if (!dJb || !dKb || c->d_PcB.reserve(nc) != cudaSuccess || c->d_JcB.reserve(nc) != cudaSuccess ||
-        c->d_KcB.reserve(nc) != cudaSuccess) {
+    if (!dJb || !dKb || c->d_PcB.reserve(nc) != cudaSuccess || c->d_JcB.reserve(acc_elems(c)) != cudaSuccess ||
+        c->d_KcB.reserve(acc_elems(c)) != cudaSuccess) {
       cudaGetLastError();
       set_error("device allocation");
       return TF_ENOMEM;
@@ -2601,7 +2624,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
         JKArgs none{};
         none.fam = c->group_fam[g];
         for (int fp32 = 0; fp32 < 2; ++fp32) {
-          const int rc = dispatch_jk(l1h, l1l, l2h, l2l, none, s, fp32 != 0, c->cls_variant[g]);
+          const int rc = dispatch_jk(l1h, l1l, l2h, l2l, none, s, fp32 != 0, jk_variant(c, g));
           if (rc != TF_OK) return rc;
         }
       }
@@ -2713,18 +2736,19 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       a.qcount = c->d_prim_count.p + NQCLS + 1;
       a.fam = c->group_fam[g];
       a.bucket32 = 0;
+      a.fx_lo = fx_offset(c);
       JKArgs a32 = a;
       a32.quartets = c->d_quartets.p + (goff[3 * g + 1] - base);
       a32.qmask = c->d_qmask.p + (goff[3 * g + 1] - base);
       a32.n = goff[3 * g + 2] - goff[3 * g + 1];
       a32.bucket32 = 1;
       if (a.n > 0) {
-        rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false, c->cls_variant[g]);
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a, s, false, jk_variant(c, g));
         if (rc != TF_OK) return rc;
         kernels++;
       }
       if (a32.n > 0) {
-        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true, c->cls_variant[g]);
+        rc = dispatch_jk(l1h, l1l, l2h, l2l, a32, s, true, jk_variant(c, g));
         if (rc != TF_OK) return rc;
         kernels++;
       }
@@ -2784,7 +2808,8 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
     }
   }
   if (opt && (!(opt->eri_schwarz_cutoff > 0.0) || !(opt->eri_primitive_pair_cutoff >= 0.0) ||
-              !(opt->mixed_fp32_cut >= 0.0) || opt->device < 0)) {
+              !(opt->mixed_fp32_cut >= 0.0) || opt->device < 0 ||
+              (opt->deterministic != 0 && opt->deterministic != 1))) {
     set_error("bad options"); return TF_EINVAL;
   }
   int ndev = 0;
@@ -2906,7 +2931,8 @@ static int create_impl(const tf_basis* bases, int n_mol, const tf_options* opt, 
   TF_TRY(up(c->d_bf_local, bf_local));
   const size_t nb2 = (size_t)c->bmat_off[n_mol], nc2 = (size_t)c->cmat_off[n_mol];
   if (c->d_P.reserve(nb2) || c->d_J.reserve(nb2) || c->d_K.reserve(nb2) || c->d_H.reserve(nb2) ||
-      c->d_Pc.reserve(nc2) || c->d_Jc.reserve(nc2) || c->d_Kc.reserve(nc2) ||
+      c->d_Pc.reserve(nc2) || c->d_Jc.reserve(c->opt.deterministic ? 2 * nc2 : nc2) ||
+      c->d_Kc.reserve(c->opt.deterministic ? 2 * nc2 : nc2) ||
       c->d_pmax.reserve((size_t)c->pmax_off[n_mol]) || c->d_pglob.reserve(n_mol) ||
       c->d_prim_count.reserve(BUILD_COUNTERS)) {
     tf_ctx_destroy(c); set_error("device allocation"); return TF_ENOMEM;

@@ -331,7 +331,7 @@ class BatchFockBuilder(FockBuilder):
     context).  Device arrays hold the molecules' n_bf x n_bf blocks concatenated."""
 
     def __init__(self, mols, schwarz_cutoff: float = 1e-9, pair_cutoff: float = 1e-6, device: int = 0,
-                 mixed_fp32_cut: float = 1e-6):
+                 mixed_fp32_cut: float = 1e-6, deterministic: bool = False):
         L = load_library()
         self.mols = list(mols)
         self.mol = self.mols[0]
@@ -339,7 +339,8 @@ class BatchFockBuilder(FockBuilder):
         arr = (_Basis * len(self.mols))(*[_basis_struct(m, self._arrays) for m in self.mols])
         self._basis = arr
         self.options = default_options(eri_schwarz_cutoff=schwarz_cutoff, eri_primitive_pair_cutoff=pair_cutoff,
-                                       device=device, mixed_fp32_cut=mixed_fp32_cut)
+                                       device=device, mixed_fp32_cut=mixed_fp32_cut,
+                                       deterministic=int(deterministic))
         h = ctypes.c_void_p()
         _check(L.tf_ctx_create_batch(arr, len(self.mols), ctypes.byref(self.options), ctypes.byref(h)))
         self.h = h
