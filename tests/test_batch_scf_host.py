@@ -3,6 +3,8 @@ on CPU tensors, with the oracle's J/K standing in for the batched CUDA builder: 
 molecule converges to the oracle's own SCF energy, with or without the incremental and
 mixed-precision schedule."""
 
+import types
+
 import numpy as np
 import pytest
 import torch
@@ -16,16 +18,30 @@ class OracleBatchBuilder:
     concatenated (row-major blocks; P, J, K are symmetric), J and K from the oracle."""
 
     def __init__(self, oracle_mod, mols):
-        self.orcs = [oracle_mod.Oracle(m, schwarz_cutoff=1e-12) for m in mols]
+        self.mod, self.mols = oracle_mod, mols
+        self.by_cut = {}
+        self.orcs = self._oracles(1e-12)
+        self.options = types.SimpleNamespace(eri_schwarz_cutoff=1e-12)
+        self.cuts = []
         self.n = [m.n_bf for m in mols]
         self.offsets = np.concatenate([[0], np.cumsum([n * n for n in self.n])]).astype(np.int64)
+
+    def _oracles(self, cut):
+        if cut not in self.by_cut:
+            self.by_cut[cut] = [self.mod.Oracle(m, schwarz_cutoff=cut) for m in self.mols]
+        return self.by_cut[cut]
+
+    def set_schwarz_cutoff(self, cut):
+        self.options.eri_schwarz_cutoff = cut
 
     def one_electron(self):
         S, T, V = zip(*(o.one_electron() for o in self.orcs))
         return list(S), list(T), list(V)
 
     def make_r_JK_device(self, P, J, K, flags=0):
-        for o, n, a in zip(self.orcs, self.n, self.offsets):
+        self.cuts.append(self.options.eri_schwarz_cutoff)
+        orcs = self._oracles(self.options.eri_schwarz_cutoff)
+        for o, n, a in zip(orcs, self.n, self.offsets):
             Jn, Kn = o.jk(P[a:a + n * n].reshape(n, n).numpy())
             J[a:a + n * n] = torch.from_numpy(np.ascontiguousarray(Jn)).reshape(-1)
             K[a:a + n * n] = torch.from_numpy(np.ascontiguousarray(Kn)).reshape(-1)
@@ -68,3 +84,31 @@ def test_batched_fallback_replaces_one_molecules_guess(oracle_mod, clusters):
     assert res[1].fell_back and not res[0].fell_back and not res[2].fell_back
     for r, e in zip(res, refs):
         assert r.converged and abs(r.energy - e) < 1e-9
+
+
+def test_batched_loosened_cheap_cycles_keep_the_energies(oracle_mod, clusters):
+    """The batch's cheap cycles use loosen x (least DIIS error of the active molecules)
+    as the Schwarz cutoff, clamped to [tight, loose_max]; once any molecule is in its
+    final full FP64 builds the build is at the tight cutoff, so every energy is still
+    the oracle's."""
+    mols, refs = clusters
+    fb = OracleBatchBuilder(oracle_mod, mols)
+    b = BatchRHF(mols, device=torch.device("cpu"), n_buckets=2, builder=fb)
+    res = b.run(conv=1e-9, diis_tol=1e-6, mixed=True, incremental=True, loosen=1e-4, loose_max=1e-8)
+    for r, e in zip(res, refs):
+        assert r.converged and abs(r.energy - e) < 1e-9
+    assert fb.cuts[0] == 1e-8 and any(1e-12 < c < 1e-8 for c in fb.cuts) and fb.cuts[-1] == 1e-12
+    assert all(1e-12 <= c <= 1e-8 for c in fb.cuts)
+    assert fb.options.eri_schwarz_cutoff == 1e-12
+    # a build in which some molecule makes a full (non-incremental) build after its
+    # first is a final FP64 build: always at the tight cutoff
+    n_full = [0] * len(mols)
+    for k, cut in enumerate(fb.cuts):
+        finals = []
+        for i, r in enumerate(res):
+            if k < len(r.history) and not r.history[k][4].endswith("+delta"):
+                n_full[i] += 1
+                if n_full[i] > 1:
+                    finals.append(i)
+        if finals:
+            assert cut == 1e-12

@@ -81,6 +81,47 @@ def test_fallback_replaces_a_guess_that_does_not_converge(oracle_mod, water2):
     assert r.converged and abs(r.energy - ref["E"]) < 1e-9
 
 
+class CutoffOracleBuilder(OracleBuilder):
+    """OracleBuilder whose builds honour the Schwarz cutoff set last (one oracle per
+    cutoff value), recording the cutoff of every build."""
+
+    def __init__(self, oracle_mod, mol):
+        super().__init__(oracle_mod, mol)
+        self.mod, self.mol = oracle_mod, mol
+        self.by_cut = {1e-12: self.o}
+        self.cuts = []
+
+    def set_schwarz_cutoff(self, cut):
+        self.options.eri_schwarz_cutoff = cut
+
+    def make_r_JK_device(self, P, J, K, flags=0):
+        cut = self.options.eri_schwarz_cutoff
+        if cut not in self.by_cut:
+            self.by_cut[cut] = self.mod.Oracle(self.mol, schwarz_cutoff=cut)
+        self.o = self.by_cut[cut]
+        self.cuts.append(cut)
+        super().make_r_JK_device(P, J, K, flags)
+
+
+def test_loosened_cheap_cycles_keep_the_converged_energy(oracle_mod, water2):
+    """Cheap cycles with a Schwarz cutoff that follows the DIIS error (loosen x error,
+    clamped to [tight, loose_max]); the final full builds at the tight cutoff decide the
+    energy, which stays the oracle's."""
+    mol, ref = water2
+    fb = CutoffOracleBuilder(oracle_mod, mol)
+    r = RHF(mol, device=torch.device("cpu"), builder=fb).run(conv=1e-9, diis_tol=1e-6, incremental=True,
+                                                            loosen=1e-4, loose_max=1e-8)
+    assert r.converged and abs(r.energy - ref["E"]) < 1e-9
+    kinds = [h[4] for h in r.history]
+    assert fb.cuts[0] == 1e-8                                   # first build: the loosest cutoff
+    for cut, kind, h_prev in zip(fb.cuts[1:], kinds[1:], r.history[:-1]):
+        if kind.endswith("+delta"):
+            assert cut == min(1e-8, max(1e-12, 1e-4 * h_prev[3]))
+    assert fb.cuts[-2:] == [1e-12, 1e-12] and kinds[-2:] == ["fp64", "fp64"]
+    assert any(c > 1e-12 for c in fb.cuts[1:-2])
+    assert fb.options.eri_schwarz_cutoff == 1e-12               # restored after the run
+
+
 class OracleUBuilder(OracleBuilder):
     """Adds the unrestricted build (make_u_JK_direct) from the oracle."""
 

@@ -144,11 +144,12 @@ class BatchRHF:
             max_iter: int = 100, incremental: bool = True, mixed: bool = False, rebuild_every: int = 16,
             mixed_until: float = 1e-6, fp64_final: int = 2, final_at: float = 10.0,
             fallback: Optional[Callable[[int], torch.Tensor]] = None, fallback_after: int = 3,
-            diis_keep: int = 8) -> List[SCFResult]:
+            diis_keep: int = 8, loosen: Optional[float] = None, loose_max: float = 1e-10) -> List[SCFResult]:
         nm = len(self.mols)
         dev = self.dev
         _sync(dev)
         t0 = time.perf_counter()
+        tight = self.fb.options.eri_schwarz_cutoff
         bk = self.buckets
         for b in bk:
             if P0 is None:
@@ -194,6 +195,17 @@ class BatchRHF:
                 D = torch.where(dm, b.P - b.P_prev, b.P) * mask(b, live)[:, None, None]
                 self._to_cat(b, D, self.Xin)
             flags = (TF_JK_MIXED if use_mixed else TF_JK_FULL) | TF_JK_DELTA
+            if loosen is not None:
+                # cheap cycles: a Schwarz x density cutoff that follows the least DIIS
+                # error of the active molecules (the Fock error it admits stays far
+                # below it); the context's own cutoff once any molecule is in its final
+                # full FP64 builds, whose Fock matrices are then exact
+                cut = tight
+                if not any_final:
+                    errs = [hist[i][-1][3] for i in active if hist[i]]
+                    cut = loose_max if len(errs) < len(active) else min(loose_max, max(tight, loosen * min(errs)))
+                if cut != self.fb.options.eri_schwarz_cutoff:
+                    self.fb.set_schwarz_cutoff(cut)
             self.fb.make_r_JK_device(self.Xin, self.J, self.K, flags)
             builds += 1
             scal = []
@@ -255,6 +267,8 @@ class BatchRHF:
                 b.P[k, :n, :n] = fallback(i).to(dev, torch.float64)
                 b.count[k] = 0
             it += 1
+        if self.fb.options.eri_schwarz_cutoff != tight:
+            self.fb.set_schwarz_cutoff(tight)
         _sync(dev)
         secs = time.perf_counter() - t0
         out = []

@@ -142,7 +142,7 @@ class RHF:
             max_iter: int = 100, mixed: bool = False, fp64_final: int = 2, incremental: bool = False,
             rebuild_every: int = 16, guess_name: str = "core", mixed_until: float = 1e-6,
             fallback: Optional[Callable[[], torch.Tensor]] = None, fallback_after: int = 3,
-            shrink: Optional[float] = None, loose_max: float = 1e-9, final_at: float = 10.0,
+            loosen: Optional[float] = None, loose_max: float = 1e-10, final_at: float = 10.0,
             verbose: bool = False) -> SCFResult:
         """Converge from P0 (default: core guess).
 
@@ -159,11 +159,12 @@ class RHF:
         ``fallback``: a callable giving a replacement density; used (once) if the DIIS
         error after ``fallback_after`` cycles is not below the first cycle's.
 
-        ``shrink``: in the cheap state, the Schwarz x density cutoff of each build is
-        ``shrink`` times the square of the previous DIIS error, clamped to [the
-        context's cutoff, ``loose_max``], so the bound tightens as the SCF converges
-        while the Fock error it admits stays well below the current error; the final
-        full FP64 builds always use the context's own cutoff.
+        ``loosen``: in the cheap state, the Schwarz x density cutoff of each build is
+        ``loosen`` times the previous DIIS error, clamped to [the context's cutoff,
+        ``loose_max``] (``loose_max`` for the first build), so the bound tightens as the
+        SCF converges while the Fock error it admits stays far below the current error;
+        the final full FP64 builds always use the context's own cutoff, so the result
+        does not depend on it.
         """
         _sync(self.dev)
         t0 = time.perf_counter()
@@ -190,13 +191,14 @@ class RHF:
             else:
                 use_mixed = use_delta = False
             flags = TF_JK_MIXED if use_mixed else TF_JK_FULL
-            if shrink is not None:
+            if loosen is not None:
                 cut = tight
                 if state == "cheap" and hist:
-                    cut = min(loose_max, max(tight, shrink * hist[-1][3] ** 2))
+                    cut = min(loose_max, max(tight, loosen * hist[-1][3]))
                 elif state == "cheap":
                     cut = loose_max
-                self.fb.set_schwarz_cutoff(cut)
+                if cut != self.fb.options.eri_schwarz_cutoff:
+                    self.fb.set_schwarz_cutoff(cut)
             tb = time.perf_counter()
             if use_delta:
                 J, K = self.jk((P - P_prev).contiguous(), flags | TF_JK_DELTA)
@@ -243,7 +245,7 @@ class RHF:
             Fx = diis.extrapolate(F, err)
             P, _, _ = self.density(Fx)
             it += 1
-        if shrink is not None:
+        if self.fb.options.eri_schwarz_cutoff != tight:
             self.fb.set_schwarz_cutoff(tight)
         _sync(self.dev)
         return SCFResult(energy=E, converged=converged, iterations=it, builds=builds,
