@@ -56,9 +56,12 @@ def test_adam_reduces_loss(cuda_ok):
 
 @pytest.mark.gpu
 def test_trained_guess_cuts_scf_cycles_not_the_answer(cuda_ok):
-    """The committed network (tonto_b200/data/guess_mlp.npz) against the core guess on
-    held-out clusters (seeds outside the training range): fewer SCF cycles, the same
-    converged energy."""
+    """The committed network (tonto_b200/data/guess_mlp.npz) on held-out clusters (seeds
+    outside the training range), against the core guess and against the superposition of
+    isolated-water densities it falls back to: a density closer to the converged one
+    than the superposition's (smaller largest element error, smaller DIIS error of the
+    first cycle), no more SCF cycles than from the superposition, far fewer than from
+    the core guess, and the same converged energy."""
     import torch
     from tonto_b200 import guess as G
     from tonto_b200 import learned_guess as LG
@@ -73,6 +76,11 @@ def test_trained_guess_cuts_scf_cycles_not_the_answer(cuda_ok):
         P_sup = torch.tensor(G.superposition_guess(mol, P_mono), device=rhf.dev)
         P0 = torch.tensor(LG.learned_density(mol, model, P_mono), device=rhf.dev)
         learned = rhf.run(P0=P0, conv=1e-8, diis_tol=1e-5, fallback=lambda: P_sup)
-        assert core.converged and learned.converged
+        sup = rhf.run(P0=P_sup, conv=1e-8, diis_tol=1e-5)
+        assert core.converged and learned.converged and sup.converged and not learned.fell_back
         assert learned.iterations <= 0.7 * core.iterations, (learned.iterations, core.iterations)
-        assert abs(learned.energy - core.energy) < 1e-8
+        assert learned.iterations <= sup.iterations, (learned.iterations, sup.iterations)
+        err_l, err_s = float((P0 - core.P).abs().max()), float((P_sup - core.P).abs().max())
+        assert err_l < 0.8 * err_s, (err_l, err_s)
+        assert learned.history[0][3] < 0.8 * sup.history[0][3], (learned.history[0][3], sup.history[0][3])
+        assert abs(learned.energy - core.energy) < 1e-8 and abs(sup.energy - core.energy) < 1e-8
