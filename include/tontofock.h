@@ -166,6 +166,15 @@ int tf_set_geometry(tf_ctx* ctx, const double* xyz);
  * (the reference keeps it fixed). */
 int tf_set_schwarz_cutoff(tf_ctx* ctx, double cutoff);
 
+/* Per-molecule Schwarz x density cutoffs of a batched context: the quartets of
+ * molecule m are screened against cutoffs[m] (host array of one value per molecule,
+ * each > 0) in place of the context's cutoff, so that the molecules of one batched
+ * build can be at different stages of their SCFs (a loose cutoff for early cycles,
+ * the tight one for the final full builds).  NULL returns every molecule to the
+ * context's cutoff.  No reference counterpart (the reference builds one molecule
+ * at a time with one cutoff). */
+int tf_set_molecule_cutoffs(tf_ctx* ctx, const double* cutoffs);
+
 /* Device memory for the screened quartet lists: a build writes and consumes them
  * in chunks of whole (la lb|lc ld) class pairs of at most `quartets` entries
  * (8 bytes each; default 2^30, 8 GiB).  A class pair larger than the budget is

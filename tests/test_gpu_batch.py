@@ -48,3 +48,44 @@ def test_batched_scf_matches_single_scf(cuda_ok):
     for m, r in zip(mols, res):
         ref = RHF(m, schwarz_cutoff=1e-12).run(conv=1e-9, diis_tol=1e-6)
         assert r.converged and abs(r.energy - ref.energy) < 1e-8
+
+
+@pytest.mark.gpu
+def test_per_molecule_cutoffs_screen_each_molecule_on_its_own(cuda_ok, oracle_mod):
+    """tf_set_molecule_cutoffs: each molecule of a batched build is screened with its
+    own Schwarz x density cutoff, exactly as a single-molecule context with that cutoff
+    (the same quartets, J and K against the oracle at that cutoff), class by class and
+    in replayed graph builds whose cutoffs change between replays."""
+    from tonto_b200.fock import BatchFockBuilder, FockBuilder
+    mols = [water_cluster(n, seed=60 + n) for n in (3, 2, 4)]
+    rng = np.random.default_rng(9)
+    Ps = []
+    for m in mols:
+        A = rng.normal(size=(m.n_bf, m.n_bf)) * 0.05
+        Ps.append(A + A.T)
+    bb = BatchFockBuilder(mols, schwarz_cutoff=1e-12)
+    for graph in (False, True):
+        bb.set_graph(graph)
+        for cuts in ([1e-12, 1e-8, 1e-10], [1e-9, 1e-12, 1e-7]):
+            bb.set_molecule_cutoffs(cuts)
+            for _ in range(2 if graph else 1):              # capture, then replay
+                Js, Ks = bb.make_r_JK_batched(Ps)
+            quartets = 0
+            for m, P, J, K, c in zip(mols, Ps, Js, Ks, cuts):
+                Jr, Kr = oracle_mod.Oracle(m, schwarz_cutoff=c).jk(P)
+                assert np.max(np.abs(J - Jr)) < 1e-11 and np.max(np.abs(K - Kr)) < 1e-11
+                f = FockBuilder(m, schwarz_cutoff=c)
+                f.make_r_JK(P)
+                quartets += int(f.stats()["quartets"])
+                f.close()
+            assert int(bb.stats()["quartets"]) == quartets
+    bb.set_molecule_cutoffs(None)                            # back to the context's cutoff
+    Js, Ks = bb.make_r_JK_batched(Ps)
+    for m, P, J, K in zip(mols, Ps, Js, Ks):
+        Jr, Kr = oracle_mod.Oracle(m, schwarz_cutoff=1e-12).jk(P)
+        assert np.max(np.abs(J - Jr)) < 1e-11 and np.max(np.abs(K - Kr)) < 1e-11
+    with pytest.raises(Exception):
+        bb.set_molecule_cutoffs([1e-12, -1.0, 1e-12])
+    with pytest.raises(ValueError):
+        bb.set_molecule_cutoffs([1e-12, 1e-12])
+    bb.close()

@@ -150,6 +150,7 @@ class BatchRHF:
         _sync(dev)
         t0 = time.perf_counter()
         tight = self.fb.options.eri_schwarz_cutoff
+        per_mol = loosen is not None and hasattr(self.fb, "set_molecule_cutoffs")
         bk = self.buckets
         for b in bk:
             if P0 is None:
@@ -196,16 +197,21 @@ class BatchRHF:
                 self._to_cat(b, D, self.Xin)
             flags = (TF_JK_MIXED if use_mixed else TF_JK_FULL) | TF_JK_DELTA
             if loosen is not None:
-                # cheap cycles: a Schwarz x density cutoff that follows the least DIIS
-                # error of the active molecules (the Fock error it admits stays far
-                # below it); the context's own cutoff once any molecule is in its final
-                # full FP64 builds, whose Fock matrices are then exact
-                cut = tight
-                if not any_final:
-                    errs = [hist[i][-1][3] for i in active if hist[i]]
-                    cut = loose_max if len(errs) < len(active) else min(loose_max, max(tight, loosen * min(errs)))
-                if cut != self.fb.options.eri_schwarz_cutoff:
-                    self.fb.set_schwarz_cutoff(cut)
+                # cheap cycles: a Schwarz x density cutoff that follows the DIIS error
+                # (the Fock error it admits stays far below it), loose_max before the
+                # first error is known; the context's own cutoff for the final full FP64
+                # builds, whose Fock matrices are then exact.  Per molecule when the
+                # builder takes per-molecule cutoffs, else one cutoff for the build: the
+                # least error of the active molecules, the tight one once any is final.
+                def cheap_cut(i):
+                    return loose_max if not hist[i] else min(loose_max, max(tight, loosen * hist[i][-1][3]))
+                if per_mol:
+                    self.fb.set_molecule_cutoffs([tight if (done[i] or state[i] == "final") else cheap_cut(i)
+                                                  for i in range(nm)])
+                else:
+                    cut = tight if any_final else min(cheap_cut(i) for i in active)
+                    if cut != self.fb.options.eri_schwarz_cutoff:
+                        self.fb.set_schwarz_cutoff(cut)
             self.fb.make_r_JK_device(self.Xin, self.J, self.K, flags)
             builds += 1
             scal = []
@@ -267,6 +273,8 @@ class BatchRHF:
                 b.P[k, :n, :n] = fallback(i).to(dev, torch.float64)
                 b.count[k] = 0
             it += 1
+        if per_mol:
+            self.fb.set_molecule_cutoffs(None)
         if self.fb.options.eri_schwarz_cutoff != tight:
             self.fb.set_schwarz_cutoff(tight)
         _sync(dev)

@@ -328,6 +328,7 @@ struct ListArgs {
   const double* pmax;           // per-molecule n_shell x n_shell blocks
   const unsigned long long* pglob;   // per molecule
   double cutoff;
+  const double* mol_cut;        // per-molecule cutoffs in place of `cutoff` (tf_set_molecule_cutoffs), or null
   double fp32_cut;              // 0: no FP32 quartets
   long long out_base;           // list index of out[0] (chunked list writes)
   long long out_cap;            // entries of out (writes beyond are dropped; the host sees the count)
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(LIST_THREADS, FAM ? 4 : 6) k_quartets(ListArgs
   const long long coff = a.cand ? a.cand_off[t] : 0;
   const long long foff = FAM && a.cand ? a.fam_coff[w] : 0;
   const int len = MODE == 2 ? a.task_len[t] : jend;
-  double Ib = 0.0, pg = 0.0;
+  double Ib = 0.0, pg = 0.0, cut = a.cutoff;
   int4 b = make_int4(0, 0, 0, 0);
   MolInfo mi{};
   if (MODE != 2) {
@@ -450,6 +451,7 @@ __global__ void __launch_bounds__(LIST_THREADS, FAM ? 4 : 6) k_quartets(ListArgs
     b = FAM ? a.srec[cp.bra_xoff + xs] : a.srec[cp.bra_off + i];
     mi = a.mols[cp.mol];
     pg = __longlong_as_double((long long)a.pglob[cp.mol]);
+    if (a.mol_cut) cut = a.mol_cut[cp.mol];
   }
   // the members' shells, Schwarz factors and bra density maxima, read once per task
   int mshell[FAM_LIST_MAX];
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(LIST_THREADS, FAM ? 4 : 6) k_quartets(ListArgs
       p = fmax(p, fmax(pm[sb * ns + sc], pm[sb * ns + sd]));
       if (p < 1.0e-20) continue;                  // TOL(20): skipped
       const double bound = p * mib[m] * Ik;
-      if (bound > a.cutoff) { m_ok |= 1u << m; maxb = fmax(maxb, bound); }
+      if (bound > cut) { m_ok |= 1u << m; maxb = fmax(maxb, bound); }
     }
     return m_ok;
   };
@@ -507,9 +509,9 @@ __global__ void __launch_bounds__(LIST_THREADS, FAM ? 4 : 6) k_quartets(ListArgs
     } else if (j < jend) {
       const double Ik = a.sorted_imax[cp.ket_off + j];
       const int4 k = a.srec[cp.ket_off + j];
-      if (!(Ib * a.sorted_bmax[cp.ket_off + j] * pg > a.cutoff)) {
+      if (!(Ib * a.sorted_bmax[cp.ket_off + j] * pg > cut)) {
         beyond = true;                           // bands are in decreasing I_max: nothing further survives
-      } else if (Ib * Ik * pg > a.cutoff) {
+      } else if (Ib * Ik * pg > cut) {
         ket = k.w;
         if (FAM) {
           double maxb;
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(LIST_THREADS, FAM ? 4 : 6) k_quartets(ListArgs
           if (fmask) bucket = cost_bucket(b, k) + (maxb < a.fp32_cut ? NCOST : 0);
         } else {
           const double bound = quartet_bound(a, mi, b, k, Ib, Ik);
-          if (bound > a.cutoff) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
+          if (bound > cut) bucket = cost_bucket(b, k) + (bound < a.fp32_cut ? NCOST : 0);
         }
       }
       if (MODE == 0 && a.cand) {
@@ -1575,6 +1577,8 @@ struct tf_ctx {
   tf::DBuf<double2> d_pairR;
   tf::DBuf<long long> d_task_cand_off;
   tf::DBuf<long long> d_counts, d_offsets, d_group_offsets;
+  tf::DBuf<double> d_mol_cut;                            // per-molecule cutoffs (tf_set_molecule_cutoffs)
+  bool use_mol_cut = false;
   tf::DBuf<unsigned long long> d_pglob, d_prim_count;
   tf::DBuf<unsigned char> d_scan_tmp;
   std::vector<cudaEvent_t> cls_ev;                       // start and end of each group's launches
@@ -1591,6 +1595,7 @@ struct tf_ctx {
   bool graph_key_mixed = false;
   int graph_key_want = 3;
   double graph_key_cutoff = 0.0;
+  bool graph_key_mol_cut = false;             // the captured list passes read per-molecule cutoffs
   int graph_kernels = 0;
   // class schedule (autotuned): graph branches and the branch of each class pair
   int sched_streams = 1;
@@ -2400,7 +2405,8 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   la = ListArgs{c->d_tasks.p,    0,           c->n_tasks,    c->d_units.p, c->d_unit_group.p, c->d_group_task0.p,
                 c->d_sorted.p,   c->d_sorted_imax.p, c->d_sorted_bmax.p, c->d_srec.p, c->d_pairs.p,  c->d_mols.p,
                 c->d_pmax.p,
-                c->d_pglob.p,    c->opt.eri_schwarz_cutoff, mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX,
+                c->d_pglob.p,    c->opt.eri_schwarz_cutoff, c->use_mol_cut ? c->d_mol_cut.p : nullptr,
+                mixed ? c->opt.mixed_fp32_cut : 0.0, 0, LLONG_MAX,
                 c->use_cand ? c->d_cand.p : nullptr, c->d_task_cand_off.p, c->d_task_len.p};
   la.bad = c->d_prim_count.p + NQCLS;
   la.csorted = c->d_csorted.p;
@@ -2614,7 +2620,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
   if (c->use_graph && c->graph_cap > 0 && !dPb) {
     const bool same = c->graph_exec && c->graph_key_P == dP && c->graph_key_J == dJ && c->graph_key_K == dK &&
                       c->graph_key_mixed == mixed && c->graph_key_cutoff == c->opt.eri_schwarz_cutoff &&
-                      c->graph_key_want == want;
+                      c->graph_key_want == want && c->graph_key_mol_cut == c->use_mol_cut;
     if (!same) {
       drop_graph(c);
       for (int g = 0; g < ng; ++g) {         // launch set-up of every class, outside the capture
@@ -2642,6 +2648,7 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       c->graph_key_mixed = mixed;
       c->graph_key_cutoff = c->opt.eri_schwarz_cutoff;
       c->graph_key_want = want;
+      c->graph_key_mol_cut = c->use_mol_cut;
       c->graph_kernels = kernels;
     }
     TF_CUDA(cudaEventRecord(c->ev0, s));
@@ -2989,6 +2996,25 @@ int tf_set_geometry(tf_ctx* c, const double* xyz) {
 int tf_set_schwarz_cutoff(tf_ctx* c, double cutoff) {
   if (!c || !(cutoff > 0.0)) { tf::set_error("bad cutoff"); return TF_EINVAL; }
   c->opt.eri_schwarz_cutoff = cutoff;
+  return TF_OK;
+}
+
+int tf_set_molecule_cutoffs(tf_ctx* c, const double* cutoffs) {
+  using namespace tf;
+  if (!c) { set_error("null context"); return TF_EINVAL; }
+  if (!cutoffs) {
+    c->use_mol_cut = false;
+    return TF_OK;
+  }
+  for (int m = 0; m < c->n_mol; ++m)
+    if (!(cutoffs[m] > 0.0) || !std::isfinite(cutoffs[m])) { set_error("bad molecule cutoff"); return TF_EINVAL; }
+  int rc = set_device(c);
+  if (rc) return rc;
+  if (c->d_mol_cut.reserve(c->n_mol) != cudaSuccess) { cudaGetLastError(); set_error("device allocation"); return TF_ENOMEM; }
+  // builds are synchronous, so no captured or running build reads the array now; a
+  // captured graph reads the new values at its next replay
+  TF_CUDA(cudaMemcpy(c->d_mol_cut.p, cutoffs, c->n_mol * sizeof(double), cudaMemcpyHostToDevice));
+  c->use_mol_cut = true;
   return TF_OK;
 }
 

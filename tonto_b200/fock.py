@@ -93,6 +93,7 @@ def load_library(path: Optional[str] = None):
     L.tf_build_jk.argtypes = [vp, P(d), P(d), P(d), i]
     L.tf_set_shard.argtypes = [vp, i, i]
     L.tf_set_schwarz_cutoff.argtypes = [vp, d]
+    L.tf_set_molecule_cutoffs.argtypes = [vp, P(d)]
     L.tf_set_list_budget.argtypes = [vp, ctypes.c_longlong]
     L.tf_set_kernel_variant.argtypes = [vp, ctypes.c_int]
     L.tf_set_screen_record_budget.argtypes = [vp, ctypes.c_longlong]
@@ -189,6 +190,20 @@ class FockBuilder:
         """Schwarz x density cutoff of the following builds."""
         _check(load_library().tf_set_schwarz_cutoff(self.h, float(cutoff)))
         self.options.eri_schwarz_cutoff = float(cutoff)
+
+    def set_molecule_cutoffs(self, cutoffs):
+        """Per-molecule Schwarz x density cutoffs of the following builds (one value per
+        molecule of the context, in place of the context's cutoff); None returns every
+        molecule to the context's cutoff."""
+        L = load_library()
+        if cutoffs is None:
+            _check(L.tf_set_molecule_cutoffs(self.h, None))
+            return
+        c = np.ascontiguousarray(cutoffs, dtype=np.float64)
+        n = len(getattr(self, "mols", [self.mol]))
+        if c.shape != (n,):
+            raise ValueError(f"{n} cutoffs expected")
+        _check(L.tf_set_molecule_cutoffs(self.h, _dp(c)))
 
     def set_list_budget(self, quartets: int):
         """Largest quartet-list chunk (entries of 8 bytes) a build keeps on the device."""
