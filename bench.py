@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-det", action="store_true", help="skip the deterministic-build measurement")
     ap.add_argument("--waters", type=int, default=N_WATER,
                     help="cluster size (default 32: the benchmark workload; smaller sizes for profiling)")
+    ap.add_argument("--profile-build", action="store_true",
+                    help="one class-by-class build with the default kernel variants and nothing else "
+                         "(a short launch sequence for per-kernel profiling), then its class times")
     return ap.parse_args()
 
 
@@ -409,6 +412,13 @@ def main():
     n = mol.n_bf
     J = torch.empty((n, n), dtype=torch.float64, device=dev)
     K = torch.empty((n, n), dtype=torch.float64, device=dev)
+    if args.profile_build:
+        fb.set_graph(False)
+        fb.make_r_JK_device(P, J, K)
+        torch.cuda.synchronize(dev)
+        print(json.dumps({"profile_build": f"(H2O){args.waters}", "build_ms": fb.stats()["build_ms"],
+                          "classes": {c["class"]: round(c["ms"], 3) for c in fb.class_stats()}}), flush=True)
+        return
     peak = fp64_peak(local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
     stream = torch.cuda.current_stream(dev)
