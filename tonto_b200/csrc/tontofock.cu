@@ -2235,8 +2235,8 @@ static void launch_jk_m(const JKArgs& a, cudaStream_t s, bool fp32, int variant)
     case 1: launch_jk_v<LA, LB, LC, LD, 1, MB>(a, s, fp32); break;
     case 2: launch_jk_v<LA, LB, LC, LD, 2, MB>(a, s, fp32); break;
     case 3: launch_jk_v<LA, LB, LC, LD, 3, MB>(a, s, fp32); break;
-    case 4: case 6: launch_jk_v<LA, LB, LC, LD, 4, MB>(a, s, fp32); break;   // deterministic: no bit 2
-    case 5: case 7: launch_jk_v<LA, LB, LC, LD, 5, MB>(a, s, fp32); break;
+    case 4: case 6: launch_jk_v<LA, LB, LC, LD, 6, MB>(a, s, fp32); break;   // deterministic: always bit 2
+    case 5: case 7: launch_jk_v<LA, LB, LC, LD, 7, MB>(a, s, fp32); break;
     default: launch_jk_v<LA, LB, LC, LD, 0, MB>(a, s, fp32); break;
   }
 }
@@ -2348,14 +2348,17 @@ double class_flops(int la, int lb, int lc, int ld, double nq, double npq) {
 
 // Deterministic builds (tf_options.deterministic): the Fock accumulators hold two
 // fixed-point words per element (fock_add), the lo words after all the hi words,
-// the kernels are their deterministic instantiations (variant bit 4, fock_add),
-// and the variants that sum K contributions across lanes in FP64 first (bit 2)
-// are not used, so that what is added to each element does not depend on the
-// autotuner's choice.
+// and the kernels are their deterministic instantiations (variant bit 4, fock_add)
+// with the K contributions of neighbouring lanes that hit the same element always
+// summed in FP64 first (bit 2, whatever the autotuner chose): which lanes are
+// summed, and in which order, follows from an entry's position in its class pair's
+// list (lane = position mod 32), which neither the launch shape, the graph nor the
+// list chunking changes, so every path adds the same values.  (Each contribution
+// costs two integer atomics here, so the merged ones pay twice.)
 static long long fx_offset(const tf_ctx* c) { return c->opt.deterministic ? c->cmat_off[c->n_mol] : 0; }
 static long long acc_elems(const tf_ctx* c) { return (c->opt.deterministic ? 2 : 1) * c->cmat_off[c->n_mol]; }
 static int jk_variant(const tf_ctx* c, int g) {
-  return c->opt.deterministic ? ((c->cls_variant[g] & ~2) | 4) : c->cls_variant[g];
+  return c->opt.deterministic ? (c->cls_variant[g] | 6) : c->cls_variant[g];
 }
 
 // The list pass MODE over tasks [t0, t1): the plain tasks, then the family tasks
