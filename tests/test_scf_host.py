@@ -90,12 +90,13 @@ class CutoffOracleBuilder(OracleBuilder):
         self.mod, self.mol = oracle_mod, mol
         self.by_cut = {1e-12: self.o}
         self.cuts = []
+        self.mol_cut = None
 
     def set_schwarz_cutoff(self, cut):
         self.options.eri_schwarz_cutoff = cut
 
     def make_r_JK_device(self, P, J, K, flags=0):
-        cut = self.options.eri_schwarz_cutoff
+        cut = self.mol_cut if self.mol_cut is not None else self.options.eri_schwarz_cutoff
         if cut not in self.by_cut:
             self.by_cut[cut] = self.mod.Oracle(self.mol, schwarz_cutoff=cut)
         self.o = self.by_cut[cut]
@@ -103,12 +104,21 @@ class CutoffOracleBuilder(OracleBuilder):
         super().make_r_JK_device(P, J, K, flags)
 
 
-def test_loosened_cheap_cycles_keep_the_converged_energy(oracle_mod, water2):
+class MolCutoffOracleBuilder(CutoffOracleBuilder):
+    """The same with a per-molecule cutoff (one molecule), as the CUDA builder offers."""
+
+    def set_molecule_cutoffs(self, cuts):
+        self.mol_cut = None if cuts is None else float(cuts[0])
+
+
+@pytest.mark.parametrize("builder", [CutoffOracleBuilder, MolCutoffOracleBuilder])
+def test_loosened_cheap_cycles_keep_the_converged_energy(oracle_mod, water2, builder):
     """Cheap cycles with a Schwarz cutoff that follows the DIIS error (loosen x error,
-    clamped to [tight, loose_max]); the final full builds at the tight cutoff decide the
-    energy, which stays the oracle's."""
+    clamped to [tight, loose_max]), set as the context cutoff or as the molecule's own
+    cutoff; the final full builds at the tight cutoff decide the energy, which stays the
+    oracle's."""
     mol, ref = water2
-    fb = CutoffOracleBuilder(oracle_mod, mol)
+    fb = builder(oracle_mod, mol)
     r = RHF(mol, device=torch.device("cpu"), builder=fb).run(conv=1e-9, diis_tol=1e-6, incremental=True,
                                                             loosen=1e-4, loose_max=1e-8)
     assert r.converged and abs(r.energy - ref["E"]) < 1e-9
@@ -119,7 +129,7 @@ def test_loosened_cheap_cycles_keep_the_converged_energy(oracle_mod, water2):
             assert cut == min(1e-8, max(1e-12, 1e-4 * h_prev[3]))
     assert fb.cuts[-2:] == [1e-12, 1e-12] and kinds[-2:] == ["fp64", "fp64"]
     assert any(c > 1e-12 for c in fb.cuts[1:-2])
-    assert fb.options.eri_schwarz_cutoff == 1e-12               # restored after the run
+    assert fb.options.eri_schwarz_cutoff == 1e-12 and fb.mol_cut is None   # restored after the run
 
 
 class OracleUBuilder(OracleBuilder):

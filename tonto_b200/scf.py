@@ -164,11 +164,14 @@ class RHF:
         ``loose_max``] (``loose_max`` for the first build), so the bound tightens as the
         SCF converges while the Fock error it admits stays far below the current error;
         the final full FP64 builds always use the context's own cutoff, so the result
-        does not depend on it.
+        does not depend on it.  With a builder that takes per-molecule cutoffs the cutoff
+        is set that way (a device value that a replayed graph build reads, so changing it
+        every cycle costs no graph re-capture).
         """
         _sync(self.dev)
         t0 = time.perf_counter()
         tight = self.fb.options.eri_schwarz_cutoff
+        per_mol = loosen is not None and hasattr(self.fb, "set_molecule_cutoffs")
         P = self.core_guess() if P0 is None else P0.to(self.dev, torch.float64).contiguous()
         diis = DIIS(self.diis_keep)
         hist = []
@@ -197,7 +200,9 @@ class RHF:
                     cut = min(loose_max, max(tight, loosen * hist[-1][3]))
                 elif state == "cheap":
                     cut = loose_max
-                if cut != self.fb.options.eri_schwarz_cutoff:
+                if per_mol:
+                    self.fb.set_molecule_cutoffs([cut])
+                elif cut != self.fb.options.eri_schwarz_cutoff:
                     self.fb.set_schwarz_cutoff(cut)
             tb = time.perf_counter()
             if use_delta:
@@ -245,6 +250,8 @@ class RHF:
             Fx = diis.extrapolate(F, err)
             P, _, _ = self.density(Fx)
             it += 1
+        if per_mol:
+            self.fb.set_molecule_cutoffs(None)
         if self.fb.options.eri_schwarz_cutoff != tight:
             self.fb.set_schwarz_cutoff(tight)
         _sync(self.dev)
