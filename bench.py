@@ -123,20 +123,24 @@ def fp64_peak(device: int):
 
 
 def traffic_from_profile():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the dominant kernel and its FP64 pipe utilisation (of
+    active cycles) from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "eri_jk_w32.md")
     if not os.path.exists(path):
-        return None, None
-    kern, val = None, None
+        return None, None, None
+    kern, val, pipe = None, None, None
     for ln in open(path):
-        if ln.startswith("dominant_kernel:"):
-            kern = ln.split(":", 1)[1].strip()
-        if ln.startswith("dram_bytes_per_launch_full_size:"):
-            try:
-                val = float(ln.split(":", 1)[1].strip())
-            except ValueError:
-                pass
-    return kern, val
+        key, _, rest = ln.partition(":")
+        try:
+            if key == "dominant_kernel":
+                kern = rest.strip()
+            elif key == "dram_bytes_per_launch_full_size":
+                val = float(rest.strip())
+            elif key == "fp64_pipe_active_fraction":
+                pipe = float(rest.strip())
+        except ValueError:
+            pass
+    return kern, val, pipe
 
 
 def core_density_torch(mol, fb, dev):
@@ -537,11 +541,14 @@ def main():
     # dominant kernel by device time
     dom_cls, (dom_ms, dom_model, dom_n, _, _) = max(cls_acc.items(), key=lambda kv: kv[1][0])
     dom_ms, dom_model = dom_ms / dom_n, dom_model / dom_n          # per launch (one build)
-    tkern, traffic = traffic_from_profile()
+    tkern, traffic, pipe = traffic_from_profile()
     if tkern != dom_cls:
-        traffic = None          # the committed capture is of another kernel
+        traffic = pipe = None   # the committed capture is of another kernel
     roofline = {"bound": "fp64_pipe", "kernel": f"k_jk {dom_cls}", "peak": peak, "unit": "TFLOP/s",
-                "traffic": traffic, "peak_source": "measured on this GPU: FP64 FMA loop (tf_peak_fma), of measured"}
+                "traffic": traffic, "peak_source": "measured on this GPU: FP64 FMA loop (tf_peak_fma), of measured",
+                "fp64_pipe_active_ncu": pipe,
+                "fp64_pipe_active_ncu_source": "sm__pipe_fp64_cycles_active (of active cycles) of the same kernel "
+                                               "in the committed ncu summary ((H2O)16 capture)"}
     if orc_res is not None and dom_cls in orc_res["classes"]:
         fl = gpu_flops(orc_res["classes"][dom_cls])
         achieved = fl / (dom_ms * 1e-3) / 1e12
