@@ -2255,10 +2255,21 @@ static void launch_jk(const JKArgs& a, cudaStream_t s, bool fp32, int variant) {
 }
 
 constexpr int GROUP_WPB = 4;
+// Warps per block of a lane-group kernel: four, or one where a warp's several groups
+// need more than 16 KB of shared memory ((dd|ps), (dd|pp), (dd|ds), (dd|dp): 25-31 KB per
+// warp), so that an SM holds as many warps as its shared memory fits (seven) instead of
+// one four-warp block.  Measured on (H2O)32: (dd|ps) 2.09 -> 1.65 ms, (dd|ds) 0.86 -> 0.69,
+// (dd|dp) 1.07 -> 1.02; (dd|dd), one group per warp, ran 13 % slower and keeps four.
+template <int LA, int LB, int LC, int LD>
+constexpr int group_wpb() {
+  using C = GroupCfg<LA, LB, LC, LD>;
+  return C::PER_WARP * sizeof(double) > 16384 && C::QPW > 1 ? 1 : GROUP_WPB;
+}
 
 template <int LA, int LB, int LC, int LD>
 static int launch_group(const JKArgs& a, cudaStream_t s) {
-  constexpr size_t smem = group_smem_bytes<LA, LB, LC, LD>(GROUP_WPB);
+  constexpr int WPB = group_wpb<LA, LB, LC, LD>();
+  constexpr size_t smem = group_smem_bytes<LA, LB, LC, LD>(WPB);
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_jk_group<LA, LB, LC, LD, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2273,11 +2284,11 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  constexpr int QPB = GroupCfg<LA, LB, LC, LD>::QPW * GROUP_WPB;
+  constexpr int QPB = GroupCfg<LA, LB, LC, LD>::QPW * WPB;
   static int group_blocks_per_sm = -1;
   if (group_blocks_per_sm < 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group_blocks_per_sm, k_jk_group<LA, LB, LC, LD, false>,
-                                                  32 * GROUP_WPB, smem);
+                                                  32 * WPB, smem);
     if (group_blocks_per_sm < 1) group_blocks_per_sm = 1;
   }
   if (a.n <= 0 && !a.range) return TF_OK;
@@ -2286,8 +2297,8 @@ static int launch_group(const JKArgs& a, cudaStream_t s) {
   GroupArgs g{a.quartets, a.n, a.pairs, a.prim_full, a.prim_skip, a.P, a.J, a.K, a.mols, a.prim_count,
               a.range, a.base, a.cap, a.jkrec, a.pairR, a.P2, a.J2, a.K2, a.want,
               a.qcount ? a.qcount + (a.bucket32 ? NQCLS : 0) : nullptr, a.fx_lo};
-  if (a.fx_lo) k_jk_group<LA, LB, LC, LD, true><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
-  else k_jk_group<LA, LB, LC, LD, false><<<(unsigned)blocks, 32 * GROUP_WPB, smem, s>>>(g);
+  if (a.fx_lo) k_jk_group<LA, LB, LC, LD, true><<<(unsigned)blocks, 32 * WPB, smem, s>>>(g);
+  else k_jk_group<LA, LB, LC, LD, false><<<(unsigned)blocks, 32 * WPB, smem, s>>>(g);
   return TF_OK;
 }
 
