@@ -11,9 +11,9 @@ no dataset is involved.
 Prints one JSON line (rank 0).  ``value`` is whole-job builds/s from CUDA-event
 device time with inputs resident in HBM; ``e2e`` is the same metric through the C
 ABI (tf_build_jk) with host buffers, copies included.  With --gpus N > 1 (torchrun,
-one process per GPU) each rank builds its round-robin share of the bra shell pairs
-(Tonto's parallel do) and the partial J, K are summed with one NCCL all-reduce:
-strong scaling of one molecule's build.
+one process per GPU) each rank builds its share of the bra tasks (Tonto's parallel do
+over the bra shell pairs, here dealt by estimated cost: tf_plan_shards) and the partial
+J, K are summed with one NCCL all-reduce: strong scaling of one molecule's build.
 """
 
 from __future__ import annotations
@@ -331,7 +331,7 @@ def config_dict(n_bf: int, world: int) -> dict:
     """The workload description both arms print (identical for the same N)."""
     return {"workload": WORKLOAD, "n_bf": n_bf, "schwarz_cutoff": SCHWARZ,
             "l2": "GPU arm: flushed (256 MB write) between timed builds",
-            "parallelism": f"round-robin bra pairs x{world} + NCCL all-reduce" if world > 1 else "single GPU"}
+            "parallelism": f"cost-balanced bra tasks x{world} + NCCL all-reduce" if world > 1 else "single GPU"}
 
 
 def host_cpu_model() -> str:

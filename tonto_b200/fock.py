@@ -234,8 +234,8 @@ class FockBuilder:
         return res.as_dict()
 
     def set_shard(self, index: int, count: int):
-        """Build only shard ``index`` of ``count`` (round-robin bra tasks); the shards'
-        J and K sum to the full build."""
+        """Build only shard ``index`` of ``count`` (the bra tasks tf_plan_shards deals to
+        it by estimated cost); the shards' J and K sum to the full build."""
         _check(load_library().tf_set_shard(self.h, int(index), int(count)))
 
     @property
