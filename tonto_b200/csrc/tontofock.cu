@@ -70,6 +70,13 @@ __constant__ double c_U[4][10 * 7];               // Cartesian -> spherical, l =
     }                                                                     \
   } while (0)
 
+// Returns from the calling function with the status of a call that failed.
+#define TF_TRY_RC(call)              \
+  do {                               \
+    const int rc__ = (call);         \
+    if (rc__ != TF_OK) return rc__;  \
+  } while (0)
+
 thread_local std::string g_last_error;
 void set_error(const std::string& s) { g_last_error = s; }
 
@@ -1604,6 +1611,7 @@ struct tf_ctx {
   std::vector<cudaStream_t> side;                        // branch streams besides the context stream
   cudaEvent_t fork_ev = nullptr;
   std::vector<cudaEvent_t> join_ev;
+  cudaEvent_t list_fork_ev = nullptr, list_join_ev = nullptr;   // family list pass on side[0]
   tf_tune tune{};                                        // last autotuner result
   tf::PinnedStage pin_obj;
   tf::PinnedStage* pin = &pin_obj;
@@ -2373,26 +2381,40 @@ static int jk_variant(const tf_ctx* c, int g) {
 }
 
 // The list pass MODE over tasks [t0, t1): the plain tasks, then the family tasks
-// among them (their own instantiation, over the family task list).
+// among them (their own instantiation, over the family task list).  The two passes
+// touch disjoint tasks (their counts, records and list positions), so when the
+// context has a branch stream (tf_autotune creates them) the family pass runs on it,
+// beside the plain pass, and the context stream waits for both.
 template <int MODE>
-static void launch_list(tf_ctx* c, ListArgs a, long long t0, long long t1, long long* counts,
-                        const long long* offsets, int2* out, cudaStream_t s, int& kernels) {
+static int launch_list(tf_ctx* c, ListArgs a, long long t0, long long t1, long long* counts,
+                       const long long* offsets, int2* out, cudaStream_t s, int& kernels) {
   const long long thr = LIST_THREADS;
+  const auto& ft = c->fam_tasks;
+  const long long f0 = std::lower_bound(ft.begin(), ft.end(), (int)t0) - ft.begin();
+  const long long f1 = std::lower_bound(ft.begin(), ft.end(), (int)t1) - ft.begin();
+  const bool side = f1 > f0 && !c->side.empty() && c->list_fork_ev && c->list_join_ev;
+  if (f1 > f0) {
+    cudaStream_t sf = s;
+    if (side) {
+      TF_CUDA(cudaEventRecord(c->list_fork_ev, s));
+      TF_CUDA(cudaStreamWaitEvent(c->side[0], c->list_fork_ev, 0));
+      sf = c->side[0];
+    }
+    ListArgs af = a;
+    af.t_base = f0;
+    af.n_tasks = f1;
+    k_quartets<MODE, true><<<(unsigned)(((f1 - f0) * 32 + thr - 1) / thr), (unsigned)thr, 0, sf>>>(af, counts, offsets,
+                                                                                                   out);
+    kernels++;
+    if (side) TF_CUDA(cudaEventRecord(c->list_join_ev, sf));
+  }
   a.t_base = t0;
   a.n_tasks = t1;
   k_quartets<MODE, false><<<(unsigned)std::max<long long>(1, ((t1 - t0) * 32 + thr - 1) / thr), (unsigned)thr, 0, s>>>(
       a, counts, offsets, out);
   kernels++;
-  const auto& ft = c->fam_tasks;
-  const long long f0 = std::lower_bound(ft.begin(), ft.end(), (int)t0) - ft.begin();
-  const long long f1 = std::lower_bound(ft.begin(), ft.end(), (int)t1) - ft.begin();
-  if (f1 > f0) {
-    a.t_base = f0;
-    a.n_tasks = f1;
-    k_quartets<MODE, true><<<(unsigned)(((f1 - f0) * 32 + thr - 1) / thr), (unsigned)thr, 0, s>>>(a, counts, offsets,
-                                                                                                  out);
-    kernels++;
-  }
+  if (side) TF_CUDA(cudaStreamWaitEvent(s, c->list_join_ev, 0));
+  return TF_OK;
 }
 
 // Density transform, pair maxima, quartet counts, their scan and the per-group
@@ -2432,7 +2454,7 @@ static int enqueue_counts(tf_ctx* c, const double* dP, const double* dPb, bool m
   la.fam_coff = c->d_fam_coff.p;
   la.cmask = c->d_cmask.p;
   const long long nslots = c->n_tasks * NBUCKET;
-  launch_list<0>(c, la, 0, c->n_tasks, c->d_counts.p, nullptr, nullptr, s, kernels);
+  TF_TRY_RC(launch_list<0>(c, la, 0, c->n_tasks, c->d_counts.p, nullptr, nullptr, s, kernels));
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, c->d_counts.p, c->d_offsets.p, (int)(nslots + 1), s);
   if (tmp_bytes > c->d_scan_tmp.n) { set_error("scan scratch not sized"); return TF_ESTATE; }
@@ -2487,8 +2509,8 @@ static int enqueue_graph_body(tf_ctx* c, const double* dP, double* dJ, double* d
   ListArgs lw = la;
   lw.out_cap = c->graph_cap;
   lw.list_total = c->d_offsets.p + c->n_tasks * NBUCKET;     // an overflowing list is not written
-  if (c->use_cand) launch_list<2>(c, lw, 0, c->n_tasks, nullptr, c->d_offsets.p, c->d_quartets.p, s, kernels);
-  else launch_list<1>(c, lw, 0, c->n_tasks, nullptr, c->d_offsets.p, c->d_quartets.p, s, kernels);
+  if (c->use_cand) TF_TRY_RC(launch_list<2>(c, lw, 0, c->n_tasks, nullptr, c->d_offsets.p, c->d_quartets.p, s, kernels));
+  else TF_TRY_RC(launch_list<1>(c, lw, 0, c->n_tasks, nullptr, c->d_offsets.p, c->d_quartets.p, s, kernels));
   const int ng = (int)c->group_cls.size();
   // class schedule: the class launches are spread over sched_streams branches of
   // the graph (the autotuner's choice), so that one class's tail overlaps another
@@ -2735,11 +2757,12 @@ static int build_jk_device(tf_ctx* c, const double* dP, double* dJ, double* dK, 
       lw.out_base = base;
       lw.qmask = c->d_qmask.p;
       if (c->use_cand)
-        launch_list<2>(c, lw, c->group_task0[g0], c->group_task0[g1], nullptr, c->d_offsets.p, c->d_quartets.p, s,
-                       kernels);
+        rc = launch_list<2>(c, lw, c->group_task0[g0], c->group_task0[g1], nullptr, c->d_offsets.p,
+                            c->d_quartets.p, s, kernels);
       else
-        launch_list<1>(c, lw, c->group_task0[g0], c->group_task0[g1], nullptr, c->d_offsets.p, c->d_quartets.p, s,
-                       kernels);
+        rc = launch_list<1>(c, lw, c->group_task0[g0], c->group_task0[g1], nullptr, c->d_offsets.p,
+                            c->d_quartets.p, s, kernels);
+      if (rc) return rc;
     }
     for (int g = g0; g < g1; ++g) {
       int l1h, l1l, l2h, l2l;
@@ -3080,6 +3103,8 @@ int tf_autotune(tf_ctx* c, const double* dP, double* dJ, double* dK, int flags, 
     c->join_ev.push_back(e);
   }
   if (!c->fork_ev) TF_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+  if (!c->list_fork_ev) TF_CUDA(cudaEventCreateWithFlags(&c->list_fork_ev, cudaEventDisableTiming));
+  if (!c->list_join_ev) TF_CUDA(cudaEventCreateWithFlags(&c->list_join_ev, cudaEventDisableTiming));
   const bool use_graph = c->use_graph;
   tf_tune res{};
   const int ng = (int)c->group_cls.size();
@@ -3619,6 +3644,8 @@ void tf_ctx_destroy(tf_ctx* c) {
   for (cudaStream_t x : c->side) cudaStreamDestroy(x);
   for (cudaEvent_t x : c->join_ev) cudaEventDestroy(x);
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->list_fork_ev) cudaEventDestroy(c->list_fork_ev);
+  if (c->list_join_ev) cudaEventDestroy(c->list_join_ev);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
