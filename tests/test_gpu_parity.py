@@ -146,3 +146,29 @@ def test_delta_build_is_linear(cuda_ok, oracle_mod):
     dJ, dK = fb.make_r_JK(P1 - P0, TF_JK_DELTA)
     J1r, K1r = orc.jk(P1)
     assert np.max(np.abs(J0 + dJ - J1r)) < 1e-10 and np.max(np.abs(K0 + dK - K1r)) < 1e-10
+
+
+@pytest.mark.gpu
+def test_host_build_into_caller_arrays(cuda_ok, oracle_mod):
+    """make_r_JK(P, out=(J, K)) writes into the caller's Fortran-ordered arrays (here
+    views of page-locked buffers, as the end-to-end measurement uses): the same J and K
+    as new arrays, within the bar of the oracle."""
+    import torch
+    from tonto_b200.fock import FockBuilder
+    mol = water_cluster(2, seed=7)
+    orc = oracle_mod.Oracle(mol, schwarz_cutoff=1e-12)
+    P = core_density(orc, oracle_mod, mol)
+    fb = FockBuilder(mol, schwarz_cutoff=1e-12)
+    n = mol.n_bf
+    pin = [torch.empty((n, n), dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    pin[0].copy_(torch.from_numpy(np.ascontiguousarray(P.T)))
+    out = (pin[1].numpy().T, pin[2].numpy().T)
+    J, K = fb.make_r_JK(pin[0].numpy().T, out=out)
+    assert J is out[0] and K is out[1]
+    J2, K2 = fb.make_r_JK(P)
+    assert np.max(np.abs(J - J2)) <= 1e-13 and np.max(np.abs(K - K2)) <= 1e-13     # atomics: same to rounding
+    Jr, Kr = orc.jk(P)
+    assert np.max(np.abs(J - Jr)) <= TOL and np.max(np.abs(K - Kr)) <= TOL
+    with pytest.raises(ValueError):
+        fb.make_r_JK(P, out=(np.empty((n, n)), np.empty((n, n))))       # C-ordered: refused
+    fb.close()

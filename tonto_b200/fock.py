@@ -245,14 +245,23 @@ class FockBuilder:
         _check(load_library().tf_schwarz(self.h, _dp(out)))
         return out
 
-    def make_r_JK(self, P: np.ndarray, flags: int = TF_JK_FULL) -> Tuple[np.ndarray, np.ndarray]:
-        """J, K for the symmetric density P (host arrays; Fortran-ordered results)."""
+    def make_r_JK(self, P: np.ndarray, flags: int = TF_JK_FULL, out=None) -> Tuple[np.ndarray, np.ndarray]:
+        """J, K for the symmetric density P (host arrays; Fortran-ordered results).
+        ``out``: a pair of Fortran-contiguous float64 (n_bf, n_bf) arrays to write J and K
+        into (for instance views of page-locked buffers, which the copies back reach
+        faster), else new arrays."""
         n = self.n_bf
         Pf = np.asfortranarray(P, dtype=np.float64)
         if Pf.shape != (n, n):
             raise ValueError(f"P must be {n}x{n}")
-        J = np.empty((n, n), order="F")
-        K = np.empty((n, n), order="F")
+        if out is None:
+            J = np.empty((n, n), order="F")
+            K = np.empty((n, n), order="F")
+        else:
+            J, K = out
+            for a in (J, K):
+                if a.shape != (n, n) or a.dtype != np.float64 or not a.flags.f_contiguous or not a.flags.writeable:
+                    raise ValueError(f"out arrays must be writeable Fortran-contiguous float64 {n}x{n}")
         _check(load_library().tf_build_jk(self.h, _dp(Pf), _dp(J), _dp(K), int(flags)))
         return J, K
 
