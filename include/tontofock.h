@@ -224,8 +224,10 @@ int tf_autotune(tf_ctx* ctx, const double* dP, double* dJ, double* dK, int flags
 
 /* Run every class pair's thread kernel in one variant (0 .. 3, as tf_autotune
  * numbers them: bit 0 more resident warps, bit 1 exchange atomics summed over lanes
- * first) until the next tf_autotune or tf_set_kernel_variant.
- * Results do not depend on it beyond summation order.  No reference counterpart. */
+ * first) until the next tf_autotune or tf_set_kernel_variant.  A deterministic
+ * context always sums over lanes first (bit 1), whatever the variant.
+ * Results do not depend on it beyond summation order (deterministic contexts: not at
+ * all).  No reference counterpart. */
 int tf_set_kernel_variant(tf_ctx* ctx, int variant);
 
 /* Restrict this context's builds to shard `index` of `count`: the bra shell-pair
