@@ -1803,12 +1803,29 @@ static void make_class_lists(const std::vector<PairRec>& pairs, const std::vecto
   L.sorted.reserve(n_pairs);
   L.simax.reserve(n_pairs);
   L.sbmax.reserve(n_pairs);
+  L.csorted.reserve(n_pairs);
+  L.cimax.reserve(n_pairs);
+  L.cxstart.reserve(n_pairs);
+  L.cn.reserve(n_pairs);
+  std::vector<int> cnt, tmp;
   for (size_t q = 0; q < lists.size(); ++q) {
     auto& v = lists[q];
-    std::sort(v.begin(), v.end(), [&](int x, int y) {
-      const int bx = band_of[x], by = band_of[y];
-      return bx != by ? bx > by : x < y;
-    });
+    // bands in decreasing order, pair ids increasing inside a band: the lists were
+    // filled in increasing pair id, so a stable counting sort over the few bands of
+    // the list gives that order (families without a bound, band -1000000, last)
+    if (v.size() > 1) {
+      int bhi = -1000000, blo = 1000000;
+      for (int x : v)
+        if (band_of[x] != -1000000) { bhi = std::max(bhi, band_of[x]); blo = std::min(blo, band_of[x]); }
+      const int nb = bhi >= blo ? bhi - blo + 2 : 1;      // the last slot holds the unbounded ones
+      auto slot = [&](int x) { return band_of[x] == -1000000 ? nb - 1 : bhi - band_of[x]; };
+      cnt.assign(nb + 1, 0);
+      for (int x : v) ++cnt[slot(x) + 1];
+      for (int k = 0; k < nb; ++k) cnt[k + 1] += cnt[k];
+      tmp.resize(v.size());
+      for (int x : v) tmp[cnt[slot(x)]++] = x;
+      v.swap(tmp);
+    }
     L.cls_off[q] = (int)L.sorted.size();
     L.cls_coff[q] = (int)L.csorted.size();
     L.cls_cn[q] = (int)v.size();
